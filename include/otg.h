@@ -1,0 +1,184 @@
+/*
+ * otg.h -- C ABI of the B200-native RC-net timing and levelization library
+ * (libotg.so).  Plain pointers and sizes only; every device entry point is
+ * asynchronous on the caller's stream and allocates nothing -- the caller
+ * passes a workspace whose size comes from the matching *_workspace_size
+ * query (the cuBLAS/cuDNN workspace pattern).
+ *
+ * Layout conventions follow OpenTimer's flat RC storage (FlatRctStorage,
+ * ot/timer/net.hpp:149-166, and RctEdgeArrayCUDA, ot/cuda/rct.cuh:20-42):
+ *   corner c = split*2 + tran  (MIN=0,MAX=1; RISE=0,FALL=1;
+ *                               ot/headerdef.hpp:79-91,172-177)
+ *   nodes_start[N+1]  node offsets; net i owns nodes [ns[i], ns[i+1])
+ *   edges[E]          E = V - N; net i owns edges [ns[i]-i, ns[i+1]-i-1),
+ *                     local node ids, SPEF *RES order
+ *   per-node arrays   [V][4] floats, corner-interleaved (16 B per node)
+ */
+#ifndef OTG_H_
+#define OTG_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st* otg_stream_t; /* == cudaStream_t */
+
+typedef enum otg_status {
+  OTG_OK = 0,
+  OTG_ERR_INVALID = 1,     /* bad argument, or an edge/root id out of range   */
+  OTG_ERR_CUDA = 2,        /* a CUDA runtime call failed                      */
+  OTG_ERR_OOM = 3,         /* device or host allocation failed                */
+  OTG_ERR_NOT_TREE = 4,    /* an RC net is not a tree spanning its nodes      */
+  OTG_ERR_CYCLE = 5,       /* levelization left pins unemitted (a cycle)      */
+  OTG_ERR_TIMEOUT = 6,     /* a bounded device wait gave up                   */
+  OTG_ERR_TOO_LARGE = 7,   /* a net exceeds the size the workspace was sized for */
+  OTG_ERR_WORKSPACE = 8,   /* workspace smaller than the query returned       */
+  OTG_ERR_ADMISSION = 9,   /* a request does not fit the device memory budget */
+} otg_status;
+
+/* One RC edge; same layout as RctEdgeCUDA {int s; int t;} (ot/cuda/rct.cuh:15-18). */
+typedef struct otg_rc_edge {
+  int32_t s;
+  int32_t t;
+} otg_rc_edge;
+
+/*
+ * A batch of RC nets on the DEVICE (all pointers are device pointers).
+ * Replaces the device half of RctEdgeArrayCUDA (ot/cuda/rct.cuh:20-42).
+ *
+ * inputs : nodes_start, edges (undirected), roots (local id of the driver),
+ *          edges_res [E], nodes_cap [V][4] (original order, pin caps of
+ *          non-root pins already added as in Net::_make_flat_rct,
+ *          ot/timer/net.cpp:425-446)
+ * outputs: edges rewritten in place to (parent, child)
+ *          node2bfs[V]  BFS slot of each local id (net-relative)
+ *          pid[V]       BFS order; parent of slot i is i - pid[i]; root 0
+ *          load/delay/ldelay/impulse [V][4] in BFS order
+ * optional sink-slew epilogue (all four NULL to skip):
+ *          sinks_start[N+1], sink_nodes[S] (local ids),
+ *          driver_slew[N][4] in, sink_slew[S][4] out:
+ *          slew = sign(si) * sqrt(si^2 + impulse)  (ot/timer/net.cpp:30-32)
+ * BFS order is the reference's: distance from the root ascending, ties by
+ * local id DESCENDING (ot/cuda/rct.cu:120-245, ot/cuda/sort.cuh:102-121).
+ */
+typedef struct otg_rc_forest {
+  int32_t num_nets;
+  int32_t total_nodes;
+  const int32_t* nodes_start;
+  otg_rc_edge* edges;
+  const int32_t* roots;
+  const float* edges_res;
+  const float* nodes_cap;
+  int32_t* node2bfs;
+  int32_t* pid;
+  float* load;
+  float* delay;
+  float* ldelay;
+  float* impulse;
+  const int32_t* sinks_start;
+  const int32_t* sink_nodes;
+  const float* driver_slew;
+  float* sink_slew;
+} otg_rc_forest;
+
+/* Workspace bytes for otg_rc_timing over num_nets nets none of which has
+ * more than max_net_nodes nodes. */
+otg_status otg_rc_workspace_size(int32_t num_nets, int32_t max_net_nodes, size_t* bytes);
+
+/*
+ * otg_rc_timing -- RC-tree BFS flattening + Elmore load/delay/ldelay/impulse
+ * for 2 splits x 2 transitions, fused in one pass over HBM.  Replaces
+ * compute_net_bfs + prepare_res_cap + compute_net_timing
+ * (ot/cuda/rct.cu:11-59,120-245,314-359) and the CPU Rct::update_rc_timing
+ * (ot/timer/net.cpp:101-193).  Asynchronous on `stream`; device-detected
+ * errors (bad ids, non-tree nets, oversize nets) are recorded in the
+ * workspace and returned by otg_rc_status().
+ */
+otg_status otg_rc_timing(const otg_rc_forest* forest, int32_t max_net_nodes, void* workspace,
+                         size_t workspace_bytes, otg_stream_t stream);
+
+/* Synchronizes `stream` and returns the first device-side error recorded in
+ * `workspace` by the last otg_rc_timing call (OTG_OK if none); *bad_net (if
+ * non-NULL) gets the offending net index or -1. */
+otg_status otg_rc_status(const void* workspace, otg_stream_t stream, int32_t* bad_net);
+
+/*
+ * Levelization of the timing graph -- replaces toposort_advance /
+ * toposort_compute_cuda (ot/cuda/toposort.cu:4-72).  Device pointers.
+ *   fanin_start[n+1], fanin[E]: fanin CSR over pins (LOOP_BREAKER arcs and
+ *   non-candidates already excluded, ot/timer/timer.cpp:1005-1048)
+ *   out_deg[n]: candidate fanout count per pin (read only; copied)
+ *   frontier0[first_size]: the seed level (candidates with no fanout)
+ * Outputs:
+ *   order[n]        pins concatenated level by level (level 0 = seed order,
+ *                   every later level in ascending pin index)
+ *   level[n]        level of each pin, -1 if never emitted
+ *   level_ends[n+2] level_ends[0]=0, level_ends[k+1] = end of level k
+ *   counts[2]       counts[0] = number of levels, counts[1] = pins emitted
+ * level(v) = 1 + max over candidate fanouts (longest path to a sink).  All
+ * levels run inside one cooperative launch (no host round trip per level);
+ * its grid barrier is bounded and reports OTG_ERR_TIMEOUT instead of hanging.
+ */
+otg_status otg_levelize_workspace_size(int32_t n, int32_t num_edges, size_t* bytes);
+otg_status otg_levelize(int32_t n, int32_t num_edges, const int32_t* fanin_start,
+                        const int32_t* fanin, const int32_t* out_deg, const int32_t* frontier0,
+                        int32_t first_size, int32_t* order, int32_t* level, int32_t* level_ends,
+                        int32_t* counts, void* workspace, size_t workspace_bytes,
+                        otg_stream_t stream);
+/* Synchronizes and returns the levelization status (OTG_ERR_TIMEOUT if the
+ * bounded grid barrier gave up). */
+otg_status otg_levelize_status(const void* workspace, otg_stream_t stream);
+
+/*
+ * Host-buffer entry points (end-to-end: host->device copies, compute,
+ * device->host copies inside the call).  They keep a per-device context
+ * with cached device buffers (grown, never shrunk) and pinned staging, and
+ * stream large batches in chunks so transfers overlap compute.  Blocking.
+ * Arrays as in otg_rc_forest but host pointers.
+ */
+otg_status otg_rc_timing_host(const otg_rc_forest* host_forest);
+otg_status otg_levelize_host(int32_t n, int32_t num_edges, const int32_t* fanin_start,
+                             const int32_t* fanin, const int32_t* out_deg,
+                             const int32_t* frontier0, int32_t first_size, int32_t* order,
+                             int32_t* level, int32_t* level_ends, int32_t* counts);
+/* Frees the host-path context of the current device. */
+void otg_release_host_context(void);
+
+/* Human-readable name of a status code. */
+const char* otg_status_string(otg_status s);
+
+/* Number of kernel launches issued by this library since load (a counter
+ * for measurement harnesses). */
+uint64_t otg_kernel_launches(void);
+
+/*
+ * Seeded synthetic RC forest (the batched-Elmore workload): net sizes are
+ * given (nodes_start), 70% random recursive trees / 30% chains with side
+ * branches, shuffled edges with random orientation, local ids by first
+ * appearance over the edges, R ~ U(0.1,50), C ~ U(0.05,5) plus a per-corner
+ * pin cap on leaves, driver slews U(5,200).  Device pointers; writes edges,
+ * roots, res, cap, driver_slew and sink_count[N] (leaves per net).  The
+ * sinks themselves come from otg_synth_rc_sinks once sinks_start (the
+ * exclusive scan of sink_count) is known.  scratch: V int32 (device).
+ */
+otg_status otg_synth_rc_forest(uint64_t seed, int32_t num_nets, const int32_t* nodes_start,
+                               otg_rc_edge* edges, int32_t* roots, float* res, float* cap,
+                               float* driver_slew, int32_t* sink_count, int32_t* scratch,
+                               otg_stream_t stream);
+otg_status otg_synth_rc_sinks(int32_t num_nets, const int32_t* nodes_start,
+                              const otg_rc_edge* edges, const int32_t* roots,
+                              const int32_t* sinks_start, int32_t* sink_nodes, int32_t* scratch,
+                              otg_stream_t stream);
+/* The same generator on the host (no GPU needed); host pointers. */
+otg_status otg_synth_rc_forest_host(uint64_t seed, int32_t num_nets, const int32_t* nodes_start,
+                                    otg_rc_edge* edges, int32_t* roots, float* res, float* cap,
+                                    float* driver_slew, int32_t* sink_count);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* OTG_H_ */

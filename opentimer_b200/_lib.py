@@ -1,0 +1,96 @@
+"""ctypes binding of libotg.so (the C ABI declared in include/otg.h).
+
+The library must be built in-tree (opentimer_b200/libotg.so); importing
+without it raises -- there is no fallback path.
+"""
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libotg.so")
+
+OK = 0
+STATUS = {
+    0: "OTG_OK", 1: "OTG_ERR_INVALID", 2: "OTG_ERR_CUDA", 3: "OTG_ERR_OOM",
+    4: "OTG_ERR_NOT_TREE", 5: "OTG_ERR_CYCLE", 6: "OTG_ERR_TIMEOUT", 7: "OTG_ERR_TOO_LARGE",
+    8: "OTG_ERR_WORKSPACE", 9: "OTG_ERR_ADMISSION",
+}
+
+# Every symbol include/otg.h declares (checked by the CPU test suite).
+C_SYMBOLS = [
+    "otg_rc_workspace_size", "otg_rc_timing", "otg_rc_status",
+    "otg_levelize_workspace_size", "otg_levelize", "otg_levelize_status",
+    "otg_rc_timing_host", "otg_levelize_host", "otg_release_host_context",
+    "otg_status_string", "otg_kernel_launches",
+    "otg_synth_rc_forest", "otg_synth_rc_sinks", "otg_synth_rc_forest_host",
+]
+# The reference-compatible C++ entry points (include/otg_compat.hpp), by
+# their Itanium-mangled names.
+CXX_SYMBOLS = {
+    "rct_bfs_and_compute_cuda": "_Z24rct_bfs_and_compute_cuda16RctEdgeArrayCUDA",
+    "rct_compute_cuda": "_Z16rct_compute_cuda7RctCUDA",
+    "toposort_compute_cuda": "_Z21toposort_compute_cudaiiiPiS_S_S_RSt6vectorIiSaIiEE",
+}
+
+
+class OtgError(RuntimeError):
+    def __init__(self, where, code):
+        super().__init__(f"{where}: {STATUS.get(code, code)}")
+        self.code = code
+
+
+class RcForest(ctypes.Structure):
+    _fields_ = [
+        ("num_nets", ctypes.c_int32), ("total_nodes", ctypes.c_int32),
+        ("nodes_start", ctypes.c_void_p), ("edges", ctypes.c_void_p),
+        ("roots", ctypes.c_void_p), ("edges_res", ctypes.c_void_p),
+        ("nodes_cap", ctypes.c_void_p), ("node2bfs", ctypes.c_void_p),
+        ("pid", ctypes.c_void_p), ("load", ctypes.c_void_p), ("delay", ctypes.c_void_p),
+        ("ldelay", ctypes.c_void_p), ("impulse", ctypes.c_void_p),
+        ("sinks_start", ctypes.c_void_p), ("sink_nodes", ctypes.c_void_p),
+        ("driver_slew", ctypes.c_void_p), ("sink_slew", ctypes.c_void_p),
+    ]
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(
+                f"{LIB_PATH} is missing: build it with `python -m opentimer_b200.build` "
+                "(there is no CPU fallback)")
+        L = ctypes.CDLL(LIB_PATH)
+        I32, P, S, U64 = ctypes.c_int32, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_uint64
+        PS = ctypes.POINTER(ctypes.c_size_t)
+        L.otg_rc_workspace_size.argtypes = [I32, I32, PS]
+        L.otg_rc_timing.argtypes = [ctypes.POINTER(RcForest), I32, P, S, P]
+        L.otg_rc_status.argtypes = [P, P, ctypes.POINTER(I32)]
+        L.otg_levelize_workspace_size.argtypes = [I32, I32, PS]
+        L.otg_levelize.argtypes = [I32, I32, P, P, P, P, I32, P, P, P, P, P, S, P]
+        L.otg_levelize_status.argtypes = [P, P]
+        L.otg_rc_timing_host.argtypes = [ctypes.POINTER(RcForest)]
+        L.otg_levelize_host.argtypes = [I32, I32, P, P, P, P, I32, P, P, P, P]
+        L.otg_release_host_context.argtypes = []
+        L.otg_release_host_context.restype = None
+        L.otg_status_string.argtypes = [ctypes.c_int]
+        L.otg_status_string.restype = ctypes.c_char_p
+        L.otg_kernel_launches.argtypes = []
+        L.otg_kernel_launches.restype = U64
+        L.otg_synth_rc_forest.argtypes = [U64, I32, P, P, P, P, P, P, P, P, P]
+        L.otg_synth_rc_sinks.argtypes = [I32, P, P, P, P, P, P, P]
+        L.otg_synth_rc_forest_host.argtypes = [U64, I32, P, P, P, P, P, P, P]
+        for name in ["otg_rc_workspace_size", "otg_rc_timing", "otg_rc_status",
+                     "otg_levelize_workspace_size", "otg_levelize", "otg_levelize_status",
+                     "otg_rc_timing_host", "otg_levelize_host", "otg_synth_rc_forest",
+                     "otg_synth_rc_sinks", "otg_synth_rc_forest_host"]:
+            getattr(L, name).restype = ctypes.c_int
+        _lib = L
+    return _lib
+
+
+def check(where, code):
+    if code != OK:
+        raise OtgError(where, code)

@@ -1,0 +1,351 @@
+// otg_levelize.cu -- timing-graph levelization (frontier Kahn) on B200.
+//
+// Replaces toposort_advance + toposort_compute_cuda (ot/cuda/toposort.cu:4-72)
+// which launch one kernel per level and copy the frontier size back to the
+// host after each one.  Here every level runs inside ONE cooperative launch:
+//
+//   level 0      = the caller's seed (pins without candidate fanout)
+//   expand(k)    every pin of level k decrements the fanout counter of each
+//                of its fanins (warp-aggregated atomics: lanes that hit the
+//                same pin combine into one atomicSub); the pin whose counter
+//                reaches zero sets its bit in the "ready" bitmap
+//   compact(k+1) the ready bitmap is split into per-CTA word ranges; each CTA
+//                counts its bits, and after a grid barrier writes its pins in
+//                ascending index order at its offset -- so every level after
+//                the seed comes out sorted by pin index, deterministically --
+//                then expands them into the other bitmap.
+//
+// Two grid barriers per level.  The barrier is a sense-counting barrier on
+// global memory whose waits are bounded by %globaltimer: a wait that runs
+// past the limit raises an abort flag that every other wait also watches,
+// so the kernel always returns and the host sees OTG_ERR_TIMEOUT.
+#include <cooperative_groups.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <algorithm>
+
+#include "../../include/otg.h"
+#include "otg_internal.cuh"
+
+namespace otg {
+namespace {
+
+constexpr unsigned FULL = 0xffffffffu;
+constexpr int LT = 512;                              // threads per CTA
+constexpr unsigned long long kWaitNs = 2000000000ull;  // 2 s per barrier wait
+
+struct LvCtl {
+  unsigned count;   // barrier arrivals
+  unsigned gen;     // barrier generation
+  int abort;        // set by a wait that timed out
+  int status;       // OTG_* status of the launch
+};
+
+__device__ __forceinline__ unsigned long long gtime() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Returns false if the barrier was abandoned (timeout somewhere).
+__device__ bool grid_barrier(LvCtl* c) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile LvCtl* vc = c;
+    int ok = 1;
+    const unsigned gen = vc->gen;
+    __threadfence();
+    const unsigned arrived = atomicAdd(&c->count, 1u);
+    if (arrived == gridDim.x - 1) {
+      c->count = 0;
+      __threadfence();
+      atomicAdd(&c->gen, 1u);
+    } else {
+      const unsigned long long t0 = gtime();
+      while (vc->gen == gen) {
+        if (vc->abort) { ok = 0; break; }
+        if (gtime() - t0 > kWaitNs) {
+          atomicExch(&c->abort, 1);
+          atomicCAS(&c->status, 0, (int)OTG_ERR_TIMEOUT);
+          ok = 0;
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+    if (vc->abort) ok = 0;
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+// Decrement the fanout counters of u's fanins; pins that become ready set
+// their bit in `bm`.  Lanes of a warp that target the same pin combine.
+__device__ __forceinline__ void expand_pin(int u, bool active, const int* fanin_start,
+                                           const int* fanin, int* cnt, unsigned* bm, int n,
+                                           const int* level) {
+  int e = active ? fanin_start[u] : 0;
+  const int e1 = active ? fanin_start[u + 1] : 0;
+  while (__any_sync(FULL, e < e1)) {
+    const bool has = e < e1;
+    const int v = has ? fanin[e] : -1;
+    const bool ok = has && (unsigned)v < (unsigned)n;
+    const unsigned peers = __match_any_sync(FULL, ok ? v : -2 - (int)(threadIdx.x & 31));
+    const int lane = threadIdx.x & 31;
+    if (ok && (__ffs(peers) - 1 == lane)) {
+      const int k = __popc(peers);
+      const int old = atomicSub(&cnt[v], k);
+      // a seed pin (level 0) is never emitted twice, even if the caller's
+      // out_deg disagrees with the fanin lists
+      if (old > 0 && old - k <= 0 && level[v] < 0) atomicOr(&bm[v >> 5], 1u << (v & 31));
+    }
+    e += has ? 1 : 0;
+  }
+}
+
+__global__ void __launch_bounds__(LT) levelize_kernel(int n, const int* fanin_start,
+                                                      const int* fanin, const int* out_deg,
+                                                      const int* frontier0, int first_size,
+                                                      int* order, int* level, int* level_ends,
+                                                      int* counts, LvCtl* ctl, int* cnt,
+                                                      unsigned* bm0, unsigned* bm1, int* blk) {
+  __shared__ int wsum[LT / 32];
+  __shared__ int s_total, s_off;
+  const int G = gridDim.x, b = blockIdx.x, tid = threadIdx.x;
+  const int gtid = b * LT + tid, gstride = G * LT;
+  const int nw = (n + 31) >> 5;
+  const int lane = tid & 31, w = tid >> 5;
+
+  for (int v = gtid; v < n; v += gstride) {
+    cnt[v] = out_deg[v];
+    level[v] = -1;
+  }
+  for (int i = gtid; i < nw; i += gstride) bm0[i] = bm1[i] = 0u;
+  if (!grid_barrier(ctl)) return;
+  for (int k = gtid; k < first_size; k += gstride) {
+    const int v = frontier0[k];
+    order[k] = v;
+    if ((unsigned)v < (unsigned)n) level[v] = 0;
+    else atomicCAS(&ctl->status, 0, (int)OTG_ERR_INVALID);
+  }
+  if (gtid == 0) {
+    level_ends[0] = 0;
+    if (first_size > 0) level_ends[1] = first_size;
+  }
+  if (first_size == 0) {
+    if (gtid == 0) { counts[0] = 0; counts[1] = 0; }
+    return;
+  }
+  if (!grid_barrier(ctl)) return;
+  // expand the seed
+  for (int k0 = b * LT; k0 < first_size; k0 += gstride) {
+    const int k = k0 + tid;
+    const bool act = k < first_size && (unsigned)order[k] < (unsigned)n;
+    expand_pin(act ? order[k] : 0, act, fanin_start, fanin, cnt, bm0, n, level);
+  }
+  unsigned* cur = bm0;
+  unsigned* nxt = bm1;
+  int emitted = first_size;
+  int L = 1;
+  const int w0 = (int)((long long)nw * b / G), w1 = (int)((long long)nw * (b + 1) / G);
+  while (true) {
+    if (!grid_barrier(ctl)) return;
+    // phase 1: count own ready bits
+    int c = 0;
+    for (int i = w0 + tid; i < w1; i += LT) c += __popc(cur[i]);
+    for (int d = 16; d >= 1; d >>= 1) c += __shfl_xor_sync(FULL, c, d);
+    if (lane == 0) wsum[w] = c;
+    __syncthreads();
+    if (tid == 0) {
+      int s = 0;
+      for (int i = 0; i < LT / 32; ++i) s += wsum[i];
+      blk[b] = s;
+    }
+    if (!grid_barrier(ctl)) return;
+    // phase 2: offset of this CTA, level total
+    if (tid < 32) {
+      int before = 0, total = 0;
+      for (int i = lane; i < G; i += 32) {
+        const int x = blk[i];
+        total += x;
+        if (i < b) before += x;
+      }
+      for (int d = 16; d >= 1; d >>= 1) {
+        total += __shfl_xor_sync(FULL, total, d);
+        before += __shfl_xor_sync(FULL, before, d);
+      }
+      if (lane == 0) { s_total = total; s_off = before; }
+    }
+    __syncthreads();
+    const int total = s_total;
+    if (total == 0) break;
+    int run = emitted + s_off;
+    // write own pins in ascending order, tile by tile, and expand them
+    for (int t0 = w0; t0 < w1; t0 += LT) {
+      const int i = t0 + tid;
+      const unsigned word = i < w1 ? cur[i] : 0u;
+      const int pc = __popc(word);
+      // block exclusive scan of pc
+      int x = pc;
+      for (int d = 1; d < 32; d <<= 1) {
+        const int y = __shfl_up_sync(FULL, x, d);
+        if (lane >= d) x += y;
+      }
+      if (lane == 31) wsum[w] = x;
+      __syncthreads();
+      int wb = 0, tt = 0;
+      for (int u = 0; u < LT / 32; ++u) {
+        if (u < w) wb += wsum[u];
+        tt += wsum[u];
+      }
+      __syncthreads();
+      int pos = run + wb + x - pc;
+      unsigned bits = word;
+      int pins[32];
+      int np = 0;
+      while (bits) {
+        const int bit = __ffs(bits) - 1;
+        bits &= bits - 1;
+        const int v = (i << 5) + bit;
+        if (pos < n) {
+          order[pos] = v;
+        } else {
+          atomicCAS(&ctl->status, 0, (int)OTG_ERR_INVALID);  // duplicate seeds
+        }
+        ++pos;
+        level[v] = L;
+        pins[np++] = v;
+      }
+      if (i < w1) cur[i] = 0u;  // ready for reuse two levels on
+      // expand: one pin per lane per step
+      int maxp = np;
+      for (int d = 16; d >= 1; d >>= 1) maxp = max(maxp, __shfl_xor_sync(FULL, maxp, d));
+      for (int k = 0; k < maxp; ++k) {
+        const bool act = k < np;
+        int u = 0;
+#pragma unroll
+        for (int q = 0; q < 32; ++q)
+          if (q == k) u = pins[q];
+        expand_pin(act ? u : 0, act, fanin_start, fanin, cnt, nxt, n, level);
+      }
+      run += tt;
+    }
+    emitted += total;
+    if (emitted > n) {  // only reachable with duplicate seeds; stop cleanly
+      if (gtid == 0) atomicCAS(&ctl->status, 0, (int)OTG_ERR_INVALID);
+      emitted = n;
+      break;
+    }
+    if (gtid == 0) level_ends[L + 1] = emitted;
+    ++L;
+    unsigned* t = cur;
+    cur = nxt;
+    nxt = t;
+  }
+  if (gtid == 0) {
+    counts[0] = L;
+    counts[1] = emitted;
+  }
+}
+
+struct LvDev {
+  int sms = 0;
+  int occ = 0;
+  bool init = false;
+};
+LvDev g_lv[64];
+
+LvDev& lv_dev() {
+  int d = 0;
+  cudaGetDevice(&d);
+  LvDev& x = g_lv[d & 63];
+  if (!x.init) {
+    cudaDeviceGetAttribute(&x.sms, cudaDevAttrMultiProcessorCount, d);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&x.occ, levelize_kernel, LT, 0);
+    x.occ = std::max(1, std::min(x.occ, 2));
+    x.init = true;
+  }
+  return x;
+}
+
+size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+struct LvWs {
+  size_t ctl, cnt, bm0, bm1, blk, total;
+};
+LvWs lv_ws(int n, int G) {
+  LvWs l;
+  size_t o = 0;
+  l.ctl = o; o = align256(o + sizeof(LvCtl));
+  l.cnt = o; o = align256(o + 4 * (size_t)std::max(n, 1));
+  const size_t nw = ((size_t)n + 31) / 32 + 1;
+  l.bm0 = o; o = align256(o + 4 * nw);
+  l.bm1 = o; o = align256(o + 4 * nw);
+  l.blk = o; o = align256(o + 4 * (size_t)G);
+  l.total = o;
+  return l;
+}
+
+}  // namespace
+}  // namespace otg
+
+extern "C" {
+
+otg_status otg_levelize_workspace_size(int32_t n, int32_t num_edges, size_t* bytes) {
+  (void)num_edges;
+  if (!bytes || n < 0) return OTG_ERR_INVALID;
+  otg::LvDev& d = otg::lv_dev();
+  if (d.sms <= 0) return OTG_ERR_CUDA;
+  *bytes = otg::lv_ws(n, d.sms * d.occ).total;
+  return OTG_OK;
+}
+
+otg_status otg_levelize(int32_t n, int32_t num_edges, const int32_t* fanin_start,
+                        const int32_t* fanin, const int32_t* out_deg, const int32_t* frontier0,
+                        int32_t first_size, int32_t* order, int32_t* level, int32_t* level_ends,
+                        int32_t* counts, void* workspace, size_t workspace_bytes,
+                        otg_stream_t stream) {
+  if (n < 0 || num_edges < 0 || first_size < 0 || first_size > n || !workspace || !counts ||
+      !level_ends)
+    return OTG_ERR_INVALID;
+  if (n > 0 && (!fanin_start || !out_deg || !order || !level || (first_size && !frontier0) ||
+                (num_edges && !fanin)))
+    return OTG_ERR_INVALID;
+  otg::LvDev& d = otg::lv_dev();
+  int G = d.sms * d.occ;
+  const otg::LvWs l = otg::lv_ws(n, G);
+  if (workspace_bytes < l.total) return OTG_ERR_WORKSPACE;
+  const int nw = (n + 31) / 32;
+  // small graphs need fewer CTAs (each CTA owns at least one bitmap word)
+  G = std::max(1, std::min(G, std::max(nw, 1)));
+  char* ws = (char*)workspace;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (cudaMemsetAsync(ws + l.ctl, 0, sizeof(otg::LvCtl), s) != cudaSuccess) return OTG_ERR_CUDA;
+  otg::LvCtl* ctl = (otg::LvCtl*)(ws + l.ctl);
+  int* cnt = (int*)(ws + l.cnt);
+  unsigned* bm0 = (unsigned*)(ws + l.bm0);
+  unsigned* bm1 = (unsigned*)(ws + l.bm1);
+  int* blk = (int*)(ws + l.blk);
+  void* args[] = {&n,     (void*)&fanin_start, (void*)&fanin, (void*)&out_deg, (void*)&frontier0,
+                  &first_size, &order, &level, &level_ends, &counts, &ctl, &cnt, &bm0, &bm1, &blk};
+  cudaError_t e = cudaLaunchCooperativeKernel((const void*)otg::levelize_kernel, dim3(G),
+                                              dim3(otg::LT), args, 0, s);
+  otg::count_launch();
+  return e == cudaSuccess ? OTG_OK : OTG_ERR_CUDA;
+}
+
+otg_status otg_levelize_status(const void* workspace, otg_stream_t stream) {
+  if (!workspace) return OTG_ERR_INVALID;
+  otg::LvCtl h;
+  if (cudaMemcpyAsync(&h, workspace, sizeof(h), cudaMemcpyDeviceToHost, (cudaStream_t)stream) !=
+          cudaSuccess ||
+      cudaStreamSynchronize((cudaStream_t)stream) != cudaSuccess)
+    return OTG_ERR_CUDA;
+  return (otg_status)h.status;
+}
+
+}  // extern "C"
