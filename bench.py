@@ -235,15 +235,15 @@ def run_ours(args, world, rank, local):
     stream = torch.cuda.current_stream(dev)
 
     # ---- workload (per rank: its own 1M nets -> weak scaling)
-    ns_np = workloads.net_sizes(SEED + rank, NUM_NETS)
+    ns_np = workloads.net_sizes(SEED + rank, args.nets, args.min_nodes, args.max_nodes)
     ns = torch.from_numpy(ns_np).to(dev)
     g = otg.synth_forest(SEED + rank, ns)
     torch.cuda.synchronize()
-    N, V = NUM_NETS, int(ns_np[-1])
+    N, V = args.nets, int(ns_np[-1])
     S = int(g["sink_nodes"].numel())
     batch = otg.RcBatch(ns, g["edges"], g["roots"], g["res"], g["cap"],
                         sinks_start=g["sinks_start"], sink_nodes=g["sink_nodes"],
-                        driver_slew=g["driver_slew"], max_net_nodes=4096)
+                        driver_slew=g["driver_slew"], max_net_nodes=args.max_nodes)
     for _ in range(args.warmup):
         batch.run(stream)
     batch.check(stream)
@@ -283,8 +283,9 @@ def run_ours(args, world, rank, local):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded, generated on the device)",
-        "config": {"workload": "batched Elmore: 1M RC nets/GPU, log-uniform 2..4096 nodes, "
-                               "70% random recursive trees / 30% chains, 4 corners, sink slews",
+        "config": {"workload": f"batched Elmore: {N} RC nets/GPU, log-uniform "
+                               f"{args.min_nodes}..{args.max_nodes} nodes, 70% random recursive "
+                               "trees / 30% chains, 4 corners, sink slews",
                    "num_nets_per_gpu": N, "total_nodes_per_gpu": V, "sinks_per_gpu": S,
                    "l2": "inputs and outputs (>60 GB) far exceed L2; no flush needed",
                    "parallelism": f"replicas x{world} (nets shard with no collective)"},
@@ -309,7 +310,10 @@ def run_e2e(args, world, g, ns_np, N, V, S, dev):
     compute -> host outputs, all inside the timed region."""
     import torch
     import opentimer_b200 as otg
-    pin = lambda t: t.cpu().pin_memory()  # noqa: E731
+    def pin(t):
+        h = torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
+        h.copy_(t)
+        return h
     h_ns = torch.from_numpy(ns_np).pin_memory()
     h_edges = pin(g["edges"])
     h_roots, h_res, h_cap = pin(g["roots"]), pin(g["res"]), pin(g["cap"])
@@ -395,6 +399,10 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-levelize", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    # smaller cases (profiling); the defaults are the benchmark workload
+    ap.add_argument("--nets", type=int, default=NUM_NETS)
+    ap.add_argument("--min-nodes", type=int, default=2)
+    ap.add_argument("--max-nodes", type=int, default=4096)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
     world, rank, local = dist_setup(args)

@@ -11,73 +11,100 @@ namespace otg {
 void count_launch();
 
 // Per-net workspace of the block path, in bytes from the slice base.  The
-// slice is shared memory for nets that fit, a per-CTA slice of the caller's
-// workspace otherwise.  Three regions:
+// slice is shared memory for nets that fit (16-bit indices), a per-CTA
+// slice of the caller's workspace otherwise (32-bit indices).  Regions:
 //   I  (whole net)  pre[n] (by local id), nap[n] (preorder -> local id),
 //                   size[n] (subtree size by preorder), nas[n] (BFS slot ->
-//                   local id), tour[2m] (adjacency, then Euler tour codes)
-//   A  (topology)   posin[2m], lr[2m] (int2: next, rank; also the radix
-//                   ping-pong), es[m], et[m], start[n+1], depth[n],
-//                   parent[n], pedge[n], slot[n], hist[256*W]
-//   B  (Elmore)     pres[n], cap[n] f4, X[n] f4, Y[n] f4, L[n] f4,
-//                   Bh[c] f4, Bl[c] f4 (c = chunks of 4 preorder slots)
-// B overlays A once the topology outputs are written; pres (first in B)
-// only overlaps posin, which is dead by then.
+//                   local id), tour[2m] (adjacency, then the Euler tour,
+//                   then signed tour codes), pres[n] f32 (by preorder)
+//   A  (topology)   es[m], et[m], then one of
+//                     A-a  ends[n] i32, posin[2m] (+ radix buffers 2x2m)
+//                     A-b  sub[2m], off[2m], spl[2m], splarc[S], sl[S] u64
+//                     A-c  depth[n], parent[n], pedge[n], slot[n]
+//                   then succ[2m] / radix buffers 2n, hist[256*W] i32
+//   B  (Elmore, one corner pair at a time; overlays A)
+//                   X[n] f2, Y[n] f2, L[n] f2, Bh[c] f2, Bl[c] f2
+//                   (c = ceil(n/K) thread chunks of K preorder slots)
 struct RcLayout {
-  uint32_t pre, nap, size, nas, tour;
-  uint32_t posin, lr, es, et, start, depth, parent, pedge, slot, hist;
-  uint32_t pres, cap, X, Y, L, Bh, Bl;
+  uint32_t pre, nap, size, nas, tour, pres;
+  uint32_t es, et, ends, posin, rb, sub, off, spl, splarc, sl, depth, parent, pedge, slot;
+  uint32_t r2, hist;
+  uint32_t X, Y, L, Bh, Bl;
   uint32_t total;
+  uint32_t ns_cap;  // capacity of the splitter arrays
 };
 
-__host__ __device__ inline RcLayout rc_layout(int n, int T) {
+// Sublist splitters of the Euler-tour ranking: about one arc in kSplit.
+constexpr int kSplit = 16;
+
+__host__ __device__ inline uint32_t rc_max3(uint32_t a, uint32_t b, uint32_t c) {
+  return a > b ? (a > c ? a : c) : (b > c ? b : c);
+}
+
+__host__ __device__ inline RcLayout rc_layout(int n, int T, int K, int ib) {
   RcLayout l;
   const uint32_t N = (uint32_t)n, M = n > 0 ? (uint32_t)(n - 1) : 0u, A = 2u * M;
-  const uint32_t W = (uint32_t)T / 32u, NCH = (N + 3u) / 4u + 1u;
+  const uint32_t W = (uint32_t)T / 32u, NCH = (N + (uint32_t)K - 1u) / (uint32_t)K + 1u;
+  const uint32_t I = (uint32_t)ib;
+  l.ns_cap = 2u * (A / (uint32_t)kSplit) + 64u;
   uint32_t o = 0;
-#define OTG_TAKE(f, bytes)             \
-  do {                                 \
-    l.f = o;                           \
-    o = (o + (bytes) + 15u) & ~15u;    \
+#define OTG_AL(x) (((x) + 15u) & ~15u)
+#define OTG_TAKE(f, bytes)      \
+  do {                          \
+    l.f = o;                    \
+    o = OTG_AL(o + (bytes));    \
   } while (0)
-  OTG_TAKE(pre, 4u * N);
-  OTG_TAKE(nap, 4u * N);
-  OTG_TAKE(size, 4u * N);
-  OTG_TAKE(nas, 4u * N);
-  OTG_TAKE(tour, 4u * A);
-  const uint32_t r0 = o;
-  OTG_TAKE(posin, 4u * A);
-  OTG_TAKE(lr, 8u * A);
-  OTG_TAKE(es, 4u * M);
-  OTG_TAKE(et, 4u * M);
-  OTG_TAKE(start, 4u * (N + 1u));
-  OTG_TAKE(depth, 4u * N);
-  OTG_TAKE(parent, 4u * N);
-  OTG_TAKE(pedge, 4u * N);
-  OTG_TAKE(slot, 4u * N);
+  OTG_TAKE(pre, I * N);
+  OTG_TAKE(nap, I * N);
+  OTG_TAKE(size, I * N);
+  OTG_TAKE(nas, I * N);
+  OTG_TAKE(tour, I * A);
+  OTG_TAKE(pres, 4u * N);
+  const uint32_t rA = o;
+  OTG_TAKE(es, I * M);
+  OTG_TAKE(et, I * M);
+  const uint32_t r1 = o;
+  // A-a
+  OTG_TAKE(ends, 4u * N);
+  OTG_TAKE(posin, I * A);
+  l.rb = l.posin;  // adjacency radix fallback: 2 x A indices from here
+  const uint32_t end_a = OTG_AL(l.posin + 2u * I * A);
+  // A-b
+  o = r1;
+  OTG_TAKE(sub, I * A);
+  OTG_TAKE(off, I * A);
+  OTG_TAKE(spl, I * A);
+  OTG_TAKE(splarc, I * l.ns_cap);
+  OTG_TAKE(sl, 8u * l.ns_cap);
+  const uint32_t end_b = o;
+  // A-c
+  o = r1;
+  OTG_TAKE(depth, I * N);
+  OTG_TAKE(parent, I * N);
+  OTG_TAKE(pedge, I * N);
+  OTG_TAKE(slot, I * N);
+  const uint32_t end_c = o;
+  o = rc_max3(end_a, end_b, end_c);
+  OTG_TAKE(r2, I * (A > 2u * N ? A : 2u * N));
   OTG_TAKE(hist, 4u * 256u * W);
   const uint32_t endA = o;
-  o = r0;
-  OTG_TAKE(pres, 4u * N);
-  OTG_TAKE(cap, 16u * N);
-  OTG_TAKE(X, 16u * N);
-  OTG_TAKE(Y, 16u * N);
-  OTG_TAKE(L, 16u * N);
-  OTG_TAKE(Bh, 16u * NCH);
-  OTG_TAKE(Bl, 16u * NCH);
+  o = rA;
+  OTG_TAKE(X, 8u * N);
+  OTG_TAKE(Y, 8u * N);
+  OTG_TAKE(L, 8u * N);
+  OTG_TAKE(Bh, 8u * NCH);
+  OTG_TAKE(Bl, 8u * NCH);
 #undef OTG_TAKE
+#undef OTG_AL
   l.total = endA > o ? endA : o;
   return l;
 }
 
 // Net-size classes: class c takes nets with nmax[c-1] < n <= nmax[c].
 struct RcClasses {
-  static constexpr int kMax = 7;
+  static constexpr int kMax = 8;
   int num;
   int nmax[kMax];
 };
-
-RcClasses rc_classes(int smem_budget);
-int rc_smem_nmax(int T, int smem_budget);
 
 }  // namespace otg

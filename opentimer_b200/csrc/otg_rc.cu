@@ -270,9 +270,63 @@ __global__ void __launch_bounds__(256) rc_warp_kernel(RcArgs a, const int* list,
   }
 }
 
+// Optional per-phase cycle accounting (build with -DOTG_PHASE_TIMING; the
+// product build compiles it out).  Thread 0 of each CTA adds the clock64()
+// delta of every phase of the block path into otg_phase_cycles[].
+#ifdef OTG_PHASE_TIMING
+}  // namespace
+__device__ unsigned long long otg_phase_cycles[32];
+namespace {
+#define PHASE_BEGIN() long long _ph_t = clock64()
+#define PHASE(k)                                                              \
+  do {                                                                        \
+    if (threadIdx.x == 0) {                                                   \
+      const long long _t = clock64();                                         \
+      atomicAdd(&otg_phase_cycles[k], (unsigned long long)(_t - _ph_t));      \
+      _ph_t = _t;                                                             \
+    }                                                                         \
+  } while (0)
+#else
+#define PHASE_BEGIN() \
+  do {                \
+  } while (0)
+#define PHASE(k) \
+  do {           \
+  } while (0)
+#endif
+
 // =====================================================================
-// Block path.
+// Block path: one CTA per net, 16-bit indices in shared memory (32-bit in
+// the global-workspace slices).  Phases:
+//   A1-A2  edges -> degrees -> adjacency offsets (validates ids, degrees)
+//   A3     adjacency: atomic fill, then each list sorted by arc id so the
+//          Euler tour is deterministic (a stable radix sort by source
+//          replaces this when some node has degree > 32)
+//   A4     Euler-tour successor of every arc; the tour starts at the
+//          root's first arc
+//   A5     tour ranking: hashed splitter arcs cut the tour into short
+//          sublists, one thread walks each sublist, pointer jumping ranks
+//          the splitters; every arc lands at its tour position
+//   A6     one scan over the tour: down arcs give preorder, depth,
+//          parent, parent edge and subtree size of every node
+//   A7     BFS slots: stable radix sort by depth of the ids in descending
+//          order (the reference's (dist asc, id desc) rule)
+//   A8     topology outputs (node2bfs, pid, directed edges) and the
+//          parent resistance by preorder
+//   B      Elmore, one corner pair at a time: load and ldelay as
+//          compensated range sums over the preorder, delay and beta as
+//          compensated prefix sums over the signed tour.
 // =====================================================================
+
+template <class Ix> struct IxT;
+template <> struct IxT<uint16_t> {
+  using S = int16_t;
+  static constexpr unsigned NONE = 0xFFFFu;
+};
+template <> struct IxT<int> {
+  using S = int;
+  static constexpr unsigned NONE = 0xFFFFFFFFu;
+};
 
 // Block-wide exclusive scan of one int per thread.
 template <int T>
@@ -304,7 +358,7 @@ __device__ __forceinline__ int block_excl_scan(int v, int& total, int* wsum) {
 }
 
 // Exclusive scan over `count` items: val(i) gives item i, out(i, prefix, v)
-// receives it.  K consecutive items per thread per tile.
+// receives it.  K consecutive items per thread per tile.  Returns the total.
 template <int T, int K, class ValF, class OutF>
 __device__ int block_scan_items(int count, ValF val, OutF out, int* wsum) {
   int carry = 0;
@@ -329,54 +383,54 @@ __device__ int block_scan_items(int count, ValF val, OutF out, int* wsum) {
   return carry;
 }
 
-// Stable LSD radix sort of the items 0..N-1 by key(i) (nbits bits, 8 bits
-// per pass).  The final order lands in `out` (out[rank] = item); b0/b1 are
-// ping-pong buffers of N ints; hist has 256*(T/32) ints.  Each warp owns a
-// contiguous range of the current sequence, so ranks inside a warp follow
-// sequence order (match_any + popc) and the digit-major scan of per-warp
-// counts keeps the sort stable.
-template <int T, class KeyF>
-__device__ void block_radix_sort(int N, int nbits, KeyF key, int* b0, int* b1, int* out,
-                                 int* hist, int* wsum) {
+// Stable LSD radix sort of the items 0..N-1 by key(i) (nbits bits, up to 8
+// bits per pass).  The final order lands in `out` (out[rank] = item); b0/b1
+// are ping-pong buffers of N entries; hist holds 256*(T/32) ints.  Each
+// warp owns a contiguous range of the current sequence, so ranks inside a
+// warp follow sequence order (match_any + popc) and the digit-major scan of
+// the per-warp counts keeps the sort stable.
+template <int T, class Ix, class KeyF>
+__device__ void block_radix_sort(int N, int nbits, KeyF key, Ix* b0, Ix* b1, Ix* out, int* hist,
+                                 int* wsum) {
   constexpr int W = T / 32;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const unsigned lt = (1u << lane) - 1u;
   const int per = ((N + W - 1) / W + 31) & ~31;
-  const int passes = nbits <= 0 ? 1 : (nbits + 7) / 8;
+  if (nbits < 1) nbits = 1;
+  const int passes = (nbits + 7) / 8;
   for (int p = 0; p < passes; ++p) {
     const int shift = 8 * p;
-    const int* src = (p == 0) ? nullptr : ((p - 1) % 2 == 0 ? b0 : b1);
-    int* dst = (p == passes - 1) ? out : (p % 2 == 0 ? b0 : b1);
-    for (int i = threadIdx.x; i < 256 * W; i += T) hist[i] = 0;
+    const int db = min(8, nbits - shift);
+    const int nb = 1 << db;
+    const unsigned mask = (unsigned)nb - 1u;
+    const Ix* src = (p == 0) ? nullptr : ((p - 1) % 2 == 0 ? b0 : b1);
+    Ix* dst = (p == passes - 1) ? out : (p % 2 == 0 ? b0 : b1);
+    for (int i = threadIdx.x; i < nb * W; i += T) hist[i] = 0;
     __syncthreads();
-    // sweep 1: per-warp digit counts
     for (int j = 0; j < per; j += 32) {
       const int idx = w * per + j + lane;
       const bool valid = idx < N;
-      const int item = valid ? (src ? src[idx] : idx) : 0;
-      const int d = valid ? ((key(item) >> shift) & 255) : (256 + lane);
+      const int item = valid ? (src ? (int)src[idx] : idx) : 0;
+      const int d = valid ? (int)(((unsigned)key(item) >> shift) & mask) : (256 + lane);
       const unsigned peers = __match_any_sync(FULL, d);
-      const bool leader = valid && (__ffs(peers) - 1 == lane);
-      if (leader) hist[d * W + w] += __popc(peers);
+      if (valid && (__ffs(peers) - 1 == lane)) hist[d * W + w] += __popc(peers);
       __syncwarp();
     }
     __syncthreads();
-    // digit-major exclusive scan of the per-warp counts
     block_scan_items<T, 4>(
-        256 * W, [&](int i) { return hist[i]; }, [&](int i, int pre, int) { hist[i] = pre; },
+        nb * W, [&](int i) { return hist[i]; }, [&](int i, int pre, int) { hist[i] = pre; },
         wsum);
     __syncthreads();
-    // sweep 2: place
     for (int j = 0; j < per; j += 32) {
       const int idx = w * per + j + lane;
       const bool valid = idx < N;
-      const int item = valid ? (src ? src[idx] : idx) : 0;
-      const int d = valid ? ((key(item) >> shift) & 255) : (256 + lane);
+      const int item = valid ? (src ? (int)src[idx] : idx) : 0;
+      const int d = valid ? (int)(((unsigned)key(item) >> shift) & mask) : (256 + lane);
       const unsigned peers = __match_any_sync(FULL, d);
-      int base = valid ? hist[d * W + w] : 0;
+      const int base = valid ? hist[d * W + w] : 0;
       __syncwarp();
       if (valid) {
-        dst[base + __popc(peers & lt)] = item;
+        dst[base + __popc(peers & lt)] = (Ix)item;
         if (__ffs(peers) - 1 == lane) hist[d * W + w] = base + __popc(peers);
       }
       __syncwarp();
@@ -385,225 +439,255 @@ __device__ void block_radix_sort(int N, int nbits, KeyF key, int* b0, int* b1, i
   }
 }
 
-// Compensated up-sweep over the preorder: x(i) -> L (fp32 inclusive prefix
-// inside each thread's 4-position chunk) and Bh/Bl (float-float exclusive
-// prefix of the chunks).  The inclusive prefix is I(p) = Bh[p/4] + Bl[p/4]
-// + L[p].  Keeping the uncompensated part to <= 4 terms matters: every
-// subtree on a long path shares the right end I(n-1), so an error there
-// would repeat in every load of the path and add up along its delays.
-template <int T, class XF>
-__device__ void up_scan(int n, XF x, float4* L, float4* Bh, float4* Bl, float* sm) {
-  constexpr int W = T / 32;
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  float ch[NC] = {0.f, 0.f, 0.f, 0.f}, cl[NC] = {0.f, 0.f, 0.f, 0.f};  // carry
-  float* swh = sm;           // [W][4]
-  float* swl = sm + W * NC;  // [W][4]
-  for (int base = 0; base < n; base += T * 4) {
-    const int q0 = base + threadIdx.x * 4;
-    float4 v[4];
+__device__ __forceinline__ float2 f2add(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 f2mul(float2 a, float2 b) { return make_float2(a.x * b.x, a.y * b.y); }
+__device__ __forceinline__ float2 f2scale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
+
+// Warp-level inclusive float-float scan of (h, l) per component, returning
+// the warp-exclusive prefix in (eh, el) and the inclusive one in (h, l).
+__device__ __forceinline__ void warp_ff_scan2(float (&h)[2], float (&l)[2], float (&eh)[2],
+                                              float (&el)[2]) {
+  const int lane = threadIdx.x & 31;
 #pragma unroll
-    for (int k = 0; k < 4; ++k) v[k] = (q0 + k < n) ? x(q0 + k) : make_float4(0.f, 0.f, 0.f, 0.f);
-    float eh[NC], el[NC];  // warp-exclusive ff prefix of this thread's chunk
+  for (int d = 1; d < 32; d <<= 1) {
 #pragma unroll
-    for (int j = 0; j < NC; ++j) {
-      float acc = 0.f, h = 0.f, l = 0.f;
-#pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        const float e = f4get(v[k], j);
-        acc += e;
-        ffadd(h, l, e, 0.f);
-        f4set(v[k], j, acc);
+    for (int j = 0; j < 2; ++j) {
+      const float yh = __shfl_up_sync(FULL, h[j], d), yl = __shfl_up_sync(FULL, l[j], d);
+      if (lane >= d) {
+        float sh = yh, sl = yl;
+        ffadd(sh, sl, h[j], l[j]);
+        h[j] = sh;
+        l[j] = sl;
       }
-      float ih = h, il = l;
-#pragma unroll
-      for (int d = 1; d < 32; d <<= 1) {
-        const float yh = __shfl_up_sync(FULL, ih, d), yl = __shfl_up_sync(FULL, il, d);
-        if (lane >= d) {
-          float sh = yh, sl = yl;
-          ffadd(sh, sl, ih, il);
-          ih = sh;
-          il = sl;
-        }
-      }
-      const float xh = __shfl_up_sync(FULL, ih, 1), xl = __shfl_up_sync(FULL, il, 1);
-      eh[j] = lane ? xh : 0.f;
-      el[j] = lane ? xl : 0.f;
-      if (lane == 31) { swh[w * NC + j] = ih; swl[w * NC + j] = il; }
     }
+  }
 #pragma unroll
-    for (int k = 0; k < 4; ++k)
-      if (q0 + k < n) L[q0 + k] = v[k];
-    __syncthreads();
-    float bh[NC], bl[NC];
-#pragma unroll
-    for (int j = 0; j < NC; ++j) { bh[j] = ch[j]; bl[j] = cl[j]; }
-    for (int u = 0; u < w; ++u)
-#pragma unroll
-      for (int j = 0; j < NC; ++j) ffadd(bh[j], bl[j], swh[u * NC + j], swl[u * NC + j]);
-#pragma unroll
-    for (int j = 0; j < NC; ++j) ffadd(bh[j], bl[j], eh[j], el[j]);
-    if (q0 < n) {
-      Bh[q0 >> 2] = make_float4(bh[0], bh[1], bh[2], bh[3]);
-      Bl[q0 >> 2] = make_float4(bl[0], bl[1], bl[2], bl[3]);
-    }
-    for (int u = 0; u < W; ++u)
-#pragma unroll
-      for (int j = 0; j < NC; ++j) ffadd(ch[j], cl[j], swh[u * NC + j], swl[u * NC + j]);
-    __syncthreads();
+  for (int j = 0; j < 2; ++j) {
+    const float xh = __shfl_up_sync(FULL, h[j], 1), xl = __shfl_up_sync(FULL, l[j], 1);
+    eh[j] = lane ? xh : 0.f;
+    el[j] = lane ? xl : 0.f;
   }
 }
 
-// Compensated inclusive down-sweep over the Euler tour: x(p) gives the
-// signed contribution of tour position p; emit(p, value) receives the
-// rounded inclusive prefix at every position.
-template <int T, class XF, class EmitF>
-__device__ void down_scan(int A, XF x, EmitF emit, float* sm) {
-  constexpr int W = T / 32;
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  float ch[NC] = {0.f, 0.f, 0.f, 0.f}, cl[NC] = {0.f, 0.f, 0.f, 0.f};
-  float* swh = sm;
-  float* swl = sm + W * NC;
-  for (int base = 0; base < A; base += T * 4) {
-    const int q0 = base + threadIdx.x * 4;
-    float4 v[4];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) v[k] = (q0 + k < A) ? x(q0 + k) : make_float4(0.f, 0.f, 0.f, 0.f);
-    float ph[4][NC], pl[4][NC];  // thread-local inclusive prefixes
-    float eh[NC], el[NC];        // warp-exclusive prefix of the thread
-#pragma unroll
-    for (int j = 0; j < NC; ++j) {
-      float h = 0.f, l = 0.f;
-#pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        ffadd(h, l, f4get(v[k], j), 0.f);
-        ph[k][j] = h;
-        pl[k][j] = l;
-      }
-      float ih = h, il = l;
-#pragma unroll
-      for (int d = 1; d < 32; d <<= 1) {
-        float yh = __shfl_up_sync(FULL, ih, d), yl = __shfl_up_sync(FULL, il, d);
-        if (lane >= d) {
-          // prefix of earlier lanes goes first
-          float sh = yh, sl = yl;
-          ffadd(sh, sl, ih, il);
-          ih = sh;
-          il = sl;
-        }
-      }
-      // exclusive = inclusive - own total: recompute as shuffle of neighbour
-      float xh = __shfl_up_sync(FULL, ih, 1), xl = __shfl_up_sync(FULL, il, 1);
-      eh[j] = lane ? xh : 0.f;
-      el[j] = lane ? xl : 0.f;
-      if (lane == 31) { swh[w * NC + j] = ih; swl[w * NC + j] = il; }
-    }
-    __syncthreads();
-    float bh[NC], bl[NC];
-#pragma unroll
-    for (int j = 0; j < NC; ++j) { bh[j] = ch[j]; bl[j] = cl[j]; }
-    for (int u = 0; u < w; ++u)
-#pragma unroll
-      for (int j = 0; j < NC; ++j) ffadd(bh[j], bl[j], swh[u * NC + j], swl[u * NC + j]);
-#pragma unroll
-    for (int j = 0; j < NC; ++j) ffadd(bh[j], bl[j], eh[j], el[j]);
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      if (q0 + k < A) {
-        float4 o;
-#pragma unroll
-        for (int j = 0; j < NC; ++j) {
-          float h = bh[j], l = bl[j];
-          ffadd(h, l, ph[k][j], pl[k][j]);
-          f4set(o, j, h + l);
-        }
-        emit(q0 + k, o);
-      }
-    }
-    for (int u = 0; u < W; ++u)
-#pragma unroll
-      for (int j = 0; j < NC; ++j) ffadd(ch[j], cl[j], swh[u * NC + j], swl[u * NC + j]);
-    __syncthreads();
-  }
-}
-
-// Range sums of an up_scan.
-struct UpPrefix {
-  const float4* L;
-  const float4* Bh;
-  const float4* Bl;
-  // range sum over preorder [lo, hi] (inclusive), compensated
-  __device__ __forceinline__ float4 range(int lo, int hi) const {
-    const int cb = hi >> 2;
-    float4 hb = Bh[cb], lb = Bl[cb], Lb = L[hi];
-    float4 ha, la, La;
-    if (lo > 0) {
-      const int ca = (lo - 1) >> 2;
-      ha = Bh[ca];
-      la = Bl[ca];
-      La = L[lo - 1];
-    } else {
-      ha = la = La = make_float4(0.f, 0.f, 0.f, 0.f);
-    }
-    float4 o;
-#pragma unroll
-    for (int j = 0; j < NC; ++j) {
-      float h = f4get(hb, j), l = f4get(lb, j);
-      ffadd(h, l, -f4get(ha, j), -f4get(la, j));
-      ffadd(h, l, f4get(Lb, j) - f4get(La, j), 0.f);
-      f4set(o, j, h + l);
-    }
-    return o;
-  }
-};
-
-__device__ __forceinline__ unsigned long long lr_pack(int next, int rank) {
-  return ((unsigned long long)(unsigned)rank << 32) | (unsigned)next;
-}
-__device__ __forceinline__ int lr_next(unsigned long long p) { return (int)(unsigned)p; }
-__device__ __forceinline__ int lr_rank(unsigned long long p) { return (int)(p >> 32); }
-
-// Block-path per-net workspace layout (see rc_layout_host for the phases).
+// Block part of a tile scan: warp totals -> per-warp exclusive base (ff)
+// and the tile total; sm holds >= 8*W + 4 floats.  Ends with a barrier.
 template <int T>
+__device__ __forceinline__ void tile_ff_bases(const float (&wh)[2], const float (&wl)[2],
+                                              float (&bh)[2], float (&bl)[2], float (&th)[2],
+                                              float (&tl)[2], float* sm) {
+  constexpr int W = T / 32;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  float* swh = sm;
+  float* swl = sm + 2 * W;
+  float* sph = sm + 4 * W;
+  float* spl = sm + 6 * W;
+  float* stt = sm + 8 * W;
+  if (lane == 31) {
+    swh[2 * w] = wh[0]; swh[2 * w + 1] = wh[1];
+    swl[2 * w] = wl[0]; swl[2 * w + 1] = wl[1];
+  }
+  __syncthreads();
+  if (w == 0) {
+    float h[2], l[2], eh[2], el[2];
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      h[j] = lane < W ? swh[2 * lane + j] : 0.f;
+      l[j] = lane < W ? swl[2 * lane + j] : 0.f;
+    }
+    warp_ff_scan2(h, l, eh, el);
+    if (lane < W) {
+      sph[2 * lane] = eh[0]; sph[2 * lane + 1] = eh[1];
+      spl[2 * lane] = el[0]; spl[2 * lane + 1] = el[1];
+    }
+    if (lane == W - 1) { stt[0] = h[0]; stt[1] = h[1]; stt[2] = l[0]; stt[3] = l[1]; }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int j = 0; j < 2; ++j) {
+    bh[j] = sph[2 * w + j];
+    bl[j] = spl[2 * w + j];
+    th[j] = stt[j];
+    tl[j] = stt[2 + j];
+  }
+}
+
+// Compensated up-sweep over n preorder slots for one corner pair:
+// L[p] = fp32 inclusive prefix inside the thread's K-slot chunk,
+// Bh/Bl[p/K] = float-float exclusive prefix of the chunks.  Only the
+// <= K-term local part is uncompensated, so a range sum carries an error
+// relative to the range itself (every subtree on a long path shares the
+// same right end; an error there would repeat along the path's delays).
+template <int T, int K, class XF>
+__device__ void up_scan(int n, XF x, float2* L, float2* Bh, float2* Bl, float* sm) {
+  float ch[2] = {0.f, 0.f}, cl[2] = {0.f, 0.f};
+  for (int base = 0; base < n; base += T * K) {
+    const int q0 = base + threadIdx.x * K;
+    float2 acc = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      if (q0 + k < n) {
+        acc = f2add(acc, x(q0 + k));
+        L[q0 + k] = acc;
+      }
+    }
+    float h[2] = {acc.x, acc.y}, l[2] = {0.f, 0.f}, eh[2], el[2];
+    warp_ff_scan2(h, l, eh, el);
+    float bh[2], bl[2], th[2], tl[2];
+    tile_ff_bases<T>(h, l, bh, bl, th, tl, sm);
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      ffadd(bh[j], bl[j], ch[j], cl[j]);
+      ffadd(bh[j], bl[j], eh[j], el[j]);
+      ffadd(ch[j], cl[j], th[j], tl[j]);
+    }
+    if (q0 < n) {
+      Bh[q0 / K] = make_float2(bh[0], bh[1]);
+      Bl[q0 / K] = make_float2(bl[0], bl[1]);
+    }
+    __syncthreads();
+  }
+}
+
+// Range sum over preorder slots [lo, hi] of an up_scan.
+template <int K>
+__device__ __forceinline__ float2 up_range(const float2* L, const float2* Bh, const float2* Bl,
+                                           int lo, int hi) {
+  const int cb = hi / K;
+  float2 hb = Bh[cb], lb = Bl[cb], Lb = L[hi];
+  float2 ha = make_float2(0.f, 0.f), la = ha, La = ha;
+  if (lo > 0) {
+    const int ca = (lo - 1) / K;
+    ha = Bh[ca];
+    la = Bl[ca];
+    La = L[lo - 1];
+  }
+  float h0 = hb.x, l0 = lb.x, h1 = hb.y, l1 = lb.y;
+  ffadd(h0, l0, -ha.x, -la.x);
+  ffadd(h1, l1, -ha.y, -la.y);
+  return make_float2(h0 + (l0 + (Lb.x - La.x)), h1 + (l1 + (Lb.y - La.y)));
+}
+
+// Compensated inclusive prefix over A tour slots for one corner pair:
+// x(p) is the signed contribution of slot p, emit(p, v) gets the prefix.
+// The tour alternates +w / -w, so even the thread-local part is kept in
+// float-float: an fp32 thread total would carry an error of order u*|w|
+// into the prefix of every later slot.
+template <int T, int K, class XF, class EmitF>
+__device__ void down_scan(int A, XF x, EmitF emit, float* sm) {
+  float ch[2] = {0.f, 0.f}, cl[2] = {0.f, 0.f};
+  for (int base = 0; base < A; base += T * K) {
+    const int q0 = base + threadIdx.x * K;
+    float ph[K][2], pl[K][2];
+    float h[2] = {0.f, 0.f}, l[2] = {0.f, 0.f};
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const float2 v = (q0 + k < A) ? x(q0 + k) : make_float2(0.f, 0.f);
+      ffadd(h[0], l[0], v.x, 0.f);
+      ffadd(h[1], l[1], v.y, 0.f);
+      ph[k][0] = h[0]; pl[k][0] = l[0];
+      ph[k][1] = h[1]; pl[k][1] = l[1];
+    }
+    float eh[2], el[2];
+    warp_ff_scan2(h, l, eh, el);
+    float bh[2], bl[2], th[2], tl[2];
+    tile_ff_bases<T>(h, l, bh, bl, th, tl, sm);
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      ffadd(bh[j], bl[j], ch[j], cl[j]);
+      ffadd(bh[j], bl[j], eh[j], el[j]);
+      ffadd(ch[j], cl[j], th[j], tl[j]);
+    }
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      if (q0 + k < A) {
+        float h0 = bh[0], l0 = bl[0], h1 = bh[1], l1 = bl[1];
+        ffadd(h0, l0, ph[k][0], pl[k][0]);
+        ffadd(h1, l1, ph[k][1], pl[k][1]);
+        emit(q0 + k, make_float2(h0 + l0, h1 + l1));
+      }
+    }
+    __syncthreads();
+  }
+}
+
+__device__ __forceinline__ unsigned long long sl_pack(unsigned next, unsigned acc) {
+  return ((unsigned long long)acc << 32) | next;
+}
+__device__ __forceinline__ unsigned sl_next(unsigned long long p) { return (unsigned)p; }
+__device__ __forceinline__ unsigned sl_acc(unsigned long long p) { return (unsigned)(p >> 32); }
+
+// Splitter arcs of the tour ranking: the first arc and ~1 in kSplit<<sel
+// others, chosen by a hash of the arc id so that runs of the tour (for
+// example the up arcs of a long path, which have consecutive odd ids)
+// cannot avoid them.
+__device__ __forceinline__ bool is_splitter(int arc, int sel, int first) {
+  unsigned h = (unsigned)arc * 0x9E3779B1u;
+  h ^= h >> 15;
+  h *= 0x85EBCA77u;
+  h ^= h >> 13;
+  return arc == first || (h & (((unsigned)kSplit << sel) - 1u)) == 0u;
+}
+
+template <int T, int K, class Ix>
 __device__ void rc_net_block(const RcArgs& a, int net, char* ws, int n, int* sh) {
+  using S = typename IxT<Ix>::S;
+  constexpr unsigned NONE = IxT<Ix>::NONE;
   const int tid = threadIdx.x;
   const int b = a.nodes_start[net];
   const int m = n - 1, A = 2 * m, eb = b - net;
-  const RcLayout lay = rc_layout(n, T);
-  int* pre = (int*)(ws + lay.pre);
-  int* nap = (int*)(ws + lay.nap);
-  int* size = (int*)(ws + lay.size);
-  int* nas = (int*)(ws + lay.nas);
-  int* tour = (int*)(ws + lay.tour);  // adjacency first, then the tour
-  int* posin = (int*)(ws + lay.posin);
-  // (next, rank) pairs for list ranking, one 64-bit word each so a pair is
-  // always read and written whole (volatile: relaxed, single-copy atomic)
-  volatile unsigned long long* lr = (volatile unsigned long long*)(ws + lay.lr);
-  int* rb0 = (int*)(ws + lay.lr);  // radix ping-pong, aliases lr
-  int* rb1 = rb0 + A;
-  int* es = (int*)(ws + lay.es);
-  int* et = (int*)(ws + lay.et);
-  int* start = (int*)(ws + lay.start);
-  int* depth = (int*)(ws + lay.depth);
-  int* parent = (int*)(ws + lay.parent);
-  int* pedge = (int*)(ws + lay.pedge);
-  int* slot = (int*)(ws + lay.slot);
-  int* hist = (int*)(ws + lay.hist);
+  const RcLayout lay = rc_layout(n, T, K, (int)sizeof(Ix));
+  Ix* pre = (Ix*)(ws + lay.pre);
+  Ix* nap = (Ix*)(ws + lay.nap);
+  Ix* size = (Ix*)(ws + lay.size);
+  Ix* nas = (Ix*)(ws + lay.nas);
+  Ix* tour = (Ix*)(ws + lay.tour);  // adjacency, then the tour
+  S* code = (S*)(ws + lay.tour);    // then the signed tour codes
   float* pres = (float*)(ws + lay.pres);
-  float4* capp = (float4*)(ws + lay.cap);
-  float4* X = (float4*)(ws + lay.X);
-  float4* Y = (float4*)(ws + lay.Y);
-  float4* L = (float4*)(ws + lay.L);
-  float4* Bh = (float4*)(ws + lay.Bh);
-  float4* Bl = (float4*)(ws + lay.Bl);
-  int* wsum = sh;                  // [W]
-  int* s_flag = sh + 32;           // error flag
-  int* s_maxd = sh + 33;           // max depth
-  float* sm = (float*)(sh + 64);   // [2][W][4] floats
+  Ix* es = (Ix*)(ws + lay.es);
+  Ix* et = (Ix*)(ws + lay.et);
+  int* ends = (int*)(ws + lay.ends);
+  Ix* posin = (Ix*)(ws + lay.posin);
+  Ix* rb0 = (Ix*)(ws + lay.rb);
+  Ix* rb1 = rb0 + A;
+  Ix* sub = (Ix*)(ws + lay.sub);
+  Ix* off = (Ix*)(ws + lay.off);
+  Ix* spl = (Ix*)(ws + lay.spl);
+  Ix* splarc = (Ix*)(ws + lay.splarc);
+  volatile unsigned long long* sl = (volatile unsigned long long*)(ws + lay.sl);
+  Ix* depth = (Ix*)(ws + lay.depth);
+  Ix* parent = (Ix*)(ws + lay.parent);
+  Ix* pedge = (Ix*)(ws + lay.pedge);
+  Ix* slot = (Ix*)(ws + lay.slot);
+  Ix* r2 = (Ix*)(ws + lay.r2);  // succ, then subtree size by tour slot, then radix buffers
+  int* hist = (int*)(ws + lay.hist);
+  float2* X = (float2*)(ws + lay.X);
+  float2* Y = (float2*)(ws + lay.Y);
+  float2* L = (float2*)(ws + lay.L);
+  float2* Bh = (float2*)(ws + lay.Bh);
+  float2* Bl = (float2*)(ws + lay.Bl);
+  int* wsum = sh;          // [W]
+  int* s_flag = sh + 32;   // error code
+  int* s_maxd = sh + 33;   // max depth
+  int* s_hub = sh + 34;    // a node of degree > 32 exists
+  float* sm = (float*)(sh + 64);
   const int root = a.roots[net];
+  auto src = [&](int arc) -> int { return (arc & 1) ? (int)et[arc >> 1] : (int)es[arc >> 1]; };
+  auto dst = [&](int arc) -> int { return (arc & 1) ? (int)es[arc >> 1] : (int)et[arc >> 1]; };
+  auto fail = [&]() -> bool {
+    __syncthreads();
+    const int f = *s_flag;
+    if (f && tid == 0) report(a, f, net);
+    return f != 0;
+  };
+  PHASE_BEGIN();
 
   // ---- A1: edges, validation, degrees
-  if (tid == 0) { *s_flag = ((unsigned)root >= (unsigned)n) ? OTG_ERR_INVALID : 0; *s_maxd = 0; }
-  for (int v = tid; v <= n; v += T) start[v] = 0;
+  if (tid == 0) {
+    *s_flag = ((unsigned)root >= (unsigned)n) ? OTG_ERR_INVALID : 0;
+    *s_maxd = 0;
+    *s_hub = 0;
+  }
+  for (int v = tid; v < n; v += T) ends[v] = 0;
   __syncthreads();
   for (int e = tid; e < m; e += T) {
     int2 ed = a.edges[eb + e];
@@ -611,213 +695,273 @@ __device__ void rc_net_block(const RcArgs& a, int net, char* ws, int n, int* sh)
       *s_flag = OTG_ERR_INVALID;
       ed = make_int2(0, 0);
     }
-    es[e] = ed.x;
-    et[e] = ed.y;
-    atomicAdd(&start[ed.x], 1);
-    atomicAdd(&start[ed.y], 1);
+    es[e] = (Ix)ed.x;
+    et[e] = (Ix)ed.y;
+    atomicAdd(&ends[ed.x], 1);
+    atomicAdd(&ends[ed.y], 1);
   }
-  __syncthreads();
-  if (*s_flag) { if (tid == 0) report(a, *s_flag, net); return; }
-  // degree -> offsets; a node without an edge cannot be in a spanning tree
-  block_scan_items<T, 4>(
-      n + 1, [&](int v) { return v < n ? start[v] : 0; },
+  if (fail()) return;
+  PHASE(0);
+  // ---- A2: degree -> begin offsets; a node without an edge is no tree node
+  block_scan_items<T, K>(
+      n, [&](int v) { return ends[v]; },
       [&](int v, int p, int d) {
-        start[v] = p;
-        if (v < n && d == 0) *s_flag = OTG_ERR_NOT_TREE;
+        ends[v] = p;
+        if (d == 0) *s_flag = OTG_ERR_NOT_TREE;
+        if (d > 32) *s_hub = 1;
       },
       wsum);
-  __syncthreads();
-  if (*s_flag) { if (tid == 0) report(a, *s_flag, net); return; }
-
-  // ---- A3: adjacency = arcs stably sorted by source (arc 2e: s->t, 2e+1: t->s)
-  int nbits = 32 - __clz(n - 1);
-  block_radix_sort<T>(
-      A, nbits, [&](int arc) { return (arc & 1) ? et[arc >> 1] : es[arc >> 1]; }, rb0, rb1,
-      tour, hist, wsum);
-  for (int j = tid; j < A; j += T) posin[tour[j]] = j;
-  __syncthreads();
-
-  // ---- A4: Euler-tour successor; the tour starts at the root's first arc
-  for (int arc = tid; arc < A; arc += T) {
-    const int v = (arc & 1) ? es[arc >> 1] : et[arc >> 1];  // head
-    int k = posin[arc ^ 1] + 1;
-    if (k == start[v + 1]) k = start[v];
-    int nx = tour[k];
-    if (nx == tour[start[root]]) nx = END;  // the arc that closes the tour
-    lr[arc] = lr_pack(nx, nx == END ? 0 : 1);
-  }
-  __syncthreads();
-
-  // ---- A5: list ranking by pointer jumping ((next, rank) read as one pair)
-  int rounds = 2;
-  while ((1 << rounds) < A) ++rounds;
-  for (int r = 0; r < rounds + 1; ++r) {
-    for (int arc = tid; arc < A; arc += T) {
-      const unsigned long long p = lr[arc];
-      if (lr_next(p) != END) {
-        const unsigned long long q = lr[lr_next(p)];
-        lr[arc] = lr_pack(lr_next(q), lr_rank(p) + lr_rank(q));
+  if (fail()) return;
+  PHASE(1);
+  // ---- A3: adjacency lists in arc-id order (arc 2e: s->t, 2e+1: t->s).
+  // After this, node v's arcs are tour[begin(v) .. ends[v]).
+  if (!*s_hub) {
+    for (int arc = tid; arc < A; arc += T) tour[atomicAdd(&ends[src(arc)], 1)] = (Ix)arc;
+    __syncthreads();
+    for (int v = tid; v < n; v += T) {
+      const int lo = v ? ends[v - 1] : 0, hi = ends[v];
+      for (int i = lo + 1; i < hi; ++i) {
+        const Ix x = tour[i];
+        int j = i - 1;
+        while (j >= lo && tour[j] > x) {
+          tour[j + 1] = tour[j];
+          --j;
+        }
+        tour[j + 1] = x;
       }
     }
+  } else {
+    block_radix_sort<T>(A, 32 - __clz(n - 1), [&](int arc) { return src(arc); }, rb0, rb1, tour,
+                        hist, wsum);
+    for (int v = tid; v < n; v += T) rb0[v] = (Ix)(v + 1 < n ? ends[v + 1] : A);
     __syncthreads();
+    for (int v = tid; v < n; v += T) ends[v] = (int)rb0[v];
   }
+  __syncthreads();
+  PHASE(2);
+  // ---- A4: Euler-tour successor: after (u->v) comes v's next arc after (v->u)
+  for (int j = tid; j < A; j += T) posin[tour[j]] = (Ix)j;
+  __syncthreads();
+  const int first = (int)tour[root ? ends[root - 1] : 0];
+  for (int arc = tid; arc < A; arc += T) {
+    const int v = dst(arc);
+    int k = (int)posin[arc ^ 1] + 1;
+    if (k == ends[v]) k = v ? ends[v - 1] : 0;
+    const int nx = (int)tour[k];
+    r2[arc] = nx == first ? (Ix)NONE : (Ix)nx;
+  }
+  __syncthreads();
+  PHASE(3);
+  // ---- A5: tour ranking by sublists
+  int sel = 0, ns = 0;
+  while (true) {
+    ns = block_scan_items<T, K>(
+        A, [&](int arc) { return is_splitter(arc, sel, first) ? 1 : 0; },
+        [&](int arc, int p, int f) {
+          sub[arc] = (Ix)NONE;
+          if (f) {
+            spl[arc] = (Ix)p;
+            if (p < (int)lay.ns_cap) splarc[p] = (Ix)arc;
+          }
+        },
+        wsum);
+    if (ns <= (int)lay.ns_cap) break;
+    ++sel;  // uniform: every thread saw the same total
+  }
+  __syncthreads();
+  for (int s = tid; s < ns; s += T) {
+    int cur = (int)splarc[s];
+    unsigned o = 0, next = 0xFFFFFFFFu;
+    for (int step = 0; step < A; ++step) {
+      sub[cur] = (Ix)s;
+      off[cur] = (Ix)o;
+      ++o;
+      const unsigned nx = (unsigned)r2[cur];
+      if (nx == NONE) break;
+      if (is_splitter((int)nx, sel, first)) { next = (unsigned)spl[nx]; break; }
+      cur = (int)nx;
+    }
+    sl[s] = sl_pack(next, o);
+  }
+  __syncthreads();
+  {
+    int rounds = 1;
+    while ((1 << rounds) < ns) ++rounds;
+    for (int r = 0; r <= rounds; ++r) {
+      for (int s = tid; s < ns; s += T) {
+        const unsigned long long p = sl[s];
+        if (sl_next(p) != 0xFFFFFFFFu) {
+          const unsigned long long q = sl[sl_next(p)];
+          sl[s] = sl_pack(sl_next(q), sl_acc(p) + sl_acc(q));
+        }
+      }
+      __syncthreads();
+    }
+  }
+  for (int s = tid; s < ns; s += T)
+    if (sl_next(sl[s]) != 0xFFFFFFFFu) *s_flag = OTG_ERR_NOT_TREE;
   for (int arc = tid; arc < A; arc += T)
-    if (lr_next(lr[arc]) != END) *s_flag = OTG_ERR_NOT_TREE;
-  for (int v = tid; v < n; v += T) pre[v] = -1;
+    if ((unsigned)sub[arc] == NONE) *s_flag = OTG_ERR_NOT_TREE;
+  if (tid == 0 && sl_acc(sl[spl[first]]) != (unsigned)A) *s_flag = OTG_ERR_NOT_TREE;
+  if (fail()) return;
+  // place every arc; remember each down arc's subtree size by tour slot
+  for (int arc = tid; arc < A; arc += T) {
+    const int p = A - (int)sl_acc(sl[sub[arc]]) + (int)off[arc];
+    const int q = A - (int)sl_acc(sl[sub[arc ^ 1]]) + (int)off[arc ^ 1];
+    if ((unsigned)p >= (unsigned)A) { *s_flag = OTG_ERR_NOT_TREE; continue; }
+    tour[p] = (Ix)arc;
+    r2[p] = (Ix)(p < q ? (q - p + 1) >> 1 : 0);
+  }
+  if (fail()) return;
+  PHASE(4);
+  // ---- A6: preorder, depth, parent, subtree size from the down arcs
+  for (int v = tid; v < n; v += T) pre[v] = (Ix)NONE;
   __syncthreads();
-  if (*s_flag) { if (tid == 0) report(a, *s_flag, net); return; }
-  // position in the tour = A-1-rank
-  for (int arc = tid; arc < A; arc += T) tour[A - 1 - lr_rank(lr[arc])] = arc;
-  __syncthreads();
-
-  // ---- A7: scan of down arcs -> preorder, depth, parent, subtree size
   if (tid == 0) {
     pre[root] = 0;
-    nap[0] = root;
-    size[0] = n;
+    nap[0] = (Ix)root;
+    size[0] = (Ix)n;
     depth[root] = 0;
-    parent[root] = root;
-    pedge[root] = -1;
+    parent[root] = (Ix)root;
+    pedge[root] = (Ix)NONE;
   }
-  block_scan_items<T, 4>(
-      A,
-      [&](int p) {
-        const int arc = tour[p];
-        return (p < A - 1 - lr_rank(lr[arc ^ 1])) ? 1 : 0;
-      },
+  __syncthreads();
+  block_scan_items<T, K>(
+      A, [&](int p) { return r2[p] != 0 ? 1 : 0; },
       [&](int p, int ex, int down) {
         if (!down) return;
-        const int arc = tour[p];
-        const int u = (arc & 1) ? et[arc >> 1] : es[arc >> 1];
-        const int v = (arc & 1) ? es[arc >> 1] : et[arc >> 1];
-        const int pv = ex + 1;
-        if (atomicCAS(&pre[v], -1, pv) != -1 || v == root) { *s_flag = OTG_ERR_NOT_TREE; return; }
+        const int arc = (int)tour[p];
+        const int v = dst(arc), pv = ex + 1;
         const int d = 2 * pv - p - 1;
-        depth[v] = d;
-        parent[v] = u;
-        pedge[v] = arc >> 1;
-        nap[pv] = v;
-        size[pv] = ((A - 1 - lr_rank(lr[arc ^ 1])) - p + 1) >> 1;
+        pre[v] = (Ix)pv;
+        depth[v] = (Ix)d;
+        parent[v] = (Ix)src(arc);
+        pedge[v] = (Ix)(arc >> 1);
+        nap[pv] = (Ix)v;
+        size[pv] = r2[p];
         atomicMax(s_maxd, d);
       },
       wsum);
   __syncthreads();
-  for (int v = tid; v < n; v += T)
-    if (pre[v] < 0) *s_flag = OTG_ERR_NOT_TREE;
-  __syncthreads();
-  if (*s_flag) { if (tid == 0) report(a, *s_flag, net); return; }
-  // tour codes for the down-sweeps: +(pre+1) entering a node, -(pre+1) leaving it
+  for (int v = tid; v < n; v += T) {
+    const unsigned pv = (unsigned)pre[v];
+    if (pv == NONE || (int)nap[pv] != v) *s_flag = OTG_ERR_NOT_TREE;
+  }
+  if (fail()) return;
   for (int p = tid; p < A; p += T) {
-    const int arc = tour[p];
-    const bool down = p < A - 1 - lr_rank(lr[arc ^ 1]);
-    const int v = down ? ((arc & 1) ? es[arc >> 1] : et[arc >> 1])
-                       : ((arc & 1) ? et[arc >> 1] : es[arc >> 1]);
-    tour[p] = down ? (pre[v] + 1) : -(pre[v] + 1);
+    const int arc = (int)tour[p];
+    const bool down = r2[p] != 0;
+    const int v = down ? dst(arc) : src(arc);
+    code[p] = (S)(down ? (int)pre[v] + 1 : -((int)pre[v] + 1));
   }
   __syncthreads();
-
-  // ---- A8: BFS slots: stable sort by depth of ids in DESCENDING order
-  const int maxd = *s_maxd;
-  block_radix_sort<T>(
-      n, 32 - __clz(maxd), [&](int j) { return depth[n - 1 - j]; }, rb0, rb1, nas, hist, wsum);
-  for (int r = tid; r < n; r += T) {
-    const int v = n - 1 - nas[r];
-    nas[r] = v;
-    slot[v] = r;
+  PHASE(5);
+  // ---- A7: BFS slots: stable sort by depth of the ids in DESCENDING order
+  {
+    Ix* rs0 = r2;
+    Ix* rs1 = r2 + n;
+    block_radix_sort<T>(
+        n, 32 - __clz(max(*s_maxd, 1)), [&](int j) { return (int)depth[n - 1 - j]; }, rs0, rs1,
+        nas, hist, wsum);
+    for (int r = tid; r < n; r += T) {
+      const int v = n - 1 - (int)nas[r];
+      nas[r] = (Ix)v;
+      slot[v] = (Ix)r;
+    }
+    __syncthreads();
   }
-  __syncthreads();
-
-  // ---- A9: topology outputs
-  for (int v = tid; v < n; v += T) a.node2bfs[b + v] = slot[v];
+  PHASE(6);
+  // ---- A8: topology outputs, parent resistance by preorder
+  for (int v = tid; v < n; v += T) a.node2bfs[b + v] = (int)slot[v];
   for (int r = tid; r < n; r += T) {
-    const int v = nas[r];
-    a.pid[b + r] = r == 0 ? 0 : r - slot[parent[v]];
+    const int v = (int)nas[r];
+    a.pid[b + r] = r == 0 ? 0 : r - (int)slot[parent[v]];
   }
   for (int e = tid; e < m; e += T) {
-    const int s = es[e], t = et[e];
-    a.edges[eb + e] = (pedge[t] == e) ? make_int2(s, t) : make_int2(t, s);
+    const int s = (int)es[e], t = (int)et[e];
+    a.edges[eb + e] = ((int)pedge[t] == e) ? make_int2(s, t) : make_int2(t, s);
   }
-  // ---- A10: resistance to the parent, by preorder
-  for (int i = tid; i < n; i += T) pres[i] = i == 0 ? 0.0f : a.res[eb + pedge[nap[i]]];
+  for (int i = tid; i < n; i += T) pres[i] = i == 0 ? 0.0f : a.res[eb + (int)pedge[nap[i]]];
   __syncthreads();
+  PHASE(7);
 
-  // ---- B: Elmore.  cap by preorder.
-  for (int i = tid; i < n; i += T) capp[i] = a.cap[b + nap[i]];
-  __syncthreads();
-  const UpPrefix up{L, Bh, Bl};
-  // load (up)
-  up_scan<T>(n, [&](int i) { return capp[i]; }, L, Bh, Bl, sm);
-  __syncthreads();
-  for (int i = tid; i < n; i += T) X[i] = up.range(i, i + size[i] - 1);
-  __syncthreads();
-  for (int r = tid; r < n; r += T) a.load[b + r] = X[pre[nas[r]]];
-  // delay (down): +pres*load entering, - leaving
-  if (tid == 0) Y[0] = make_float4(0.f, 0.f, 0.f, 0.f);
-  down_scan<T>(
-      A,
-      [&](int p) {
-        const int c = tour[p];
-        const int i = (c > 0 ? c : -c) - 1;
-        const float s = c > 0 ? pres[i] : -pres[i];
-        return f4scale(X[i], s);
-      },
-      [&](int p, float4 v) {
-        const int c = tour[p];
-        if (c > 0) Y[c - 1] = v;
-      },
-      sm);
-  __syncthreads();
-  for (int r = tid; r < n; r += T) a.delay[b + r] = Y[pre[nas[r]]];
-  // ldelay (up): cap*delay over the subtree
-  up_scan<T>(n, [&](int i) { return f4mul(capp[i], Y[i]); }, L, Bh, Bl, sm);
-  __syncthreads();
-  for (int i = tid; i < n; i += T) X[i] = up.range(i, i + size[i] - 1);
-  __syncthreads();
-  for (int r = tid; r < n; r += T) a.ldelay[b + r] = X[pre[nas[r]]];
-  // beta (down) -> impulse = 2*beta - delay^2, kept in L
-  if (tid == 0) L[0] = make_float4(0.f, 0.f, 0.f, 0.f);
-  down_scan<T>(
-      A,
-      [&](int p) {
-        const int c = tour[p];
-        const int i = (c > 0 ? c : -c) - 1;
-        const float s = c > 0 ? pres[i] : -pres[i];
-        return f4scale(X[i], s);
-      },
-      [&](int p, float4 v) {
-        const int c = tour[p];
-        if (c > 0) {
-          const float4 d = Y[c - 1];
-          L[c - 1] = make_float4(fmaf(-d.x, d.x, 2.0f * v.x), fmaf(-d.y, d.y, 2.0f * v.y),
-                                 fmaf(-d.z, d.z, 2.0f * v.z), fmaf(-d.w, d.w, 2.0f * v.w));
-        }
-      },
-      sm);
-  __syncthreads();
-  for (int r = tid; r < n; r += T) a.impulse[b + r] = L[pre[nas[r]]];
-  if (a.sinks_start) {
-    const int s0 = a.sinks_start[net], s1 = a.sinks_start[net + 1];
-    const float4 si = a.driver_slew[net];
-    for (int k = s0 + tid; k < s1; k += T) {
-      const int v = a.sink_nodes[k];
-      if ((unsigned)v >= (unsigned)n) { report(a, OTG_ERR_INVALID, net); continue; }
-      const float4 iv = L[pre[v]];
-      float4 o;
-      o.x = copysignf(sqrtf(si.x * si.x + iv.x), si.x);
-      o.y = copysignf(sqrtf(si.y * si.y + iv.y), si.y);
-      o.z = copysignf(sqrtf(si.z * si.z + iv.z), si.z);
-      o.w = copysignf(sqrtf(si.w * si.w + iv.w), si.w);
-      a.sink_slew[k] = o;
+  // ---- B: Elmore, one corner pair at a time (corners 2cp, 2cp+1)
+  const float2* cap2 = (const float2*)a.cap;
+  for (int cp = 0; cp < 2; ++cp) {
+    float2* out;
+    auto capx = [&](int i) { return cap2[2 * (size_t)(b + (int)nap[i]) + cp]; };
+    // load (up): cap summed over the subtree
+    up_scan<T, K>(n, capx, L, Bh, Bl, sm);
+    for (int i = tid; i < n; i += T) X[i] = up_range<K>(L, Bh, Bl, i, i + (int)size[i] - 1);
+    __syncthreads();
+    out = (float2*)a.load;
+    for (int r = tid; r < n; r += T) out[2 * (size_t)(b + r) + cp] = X[pre[nas[r]]];
+    PHASE(8);
+    // delay (down): +pres*load entering a node, - leaving it
+    if (tid == 0) Y[0] = make_float2(0.f, 0.f);
+    down_scan<T, K>(
+        A,
+        [&](int p) {
+          const int c = (int)code[p];
+          const int i = (c > 0 ? c : -c) - 1;
+          return f2scale(X[i], c > 0 ? pres[i] : -pres[i]);
+        },
+        [&](int p, float2 v) {
+          const int c = (int)code[p];
+          if (c > 0) Y[c - 1] = v;
+        },
+        sm);
+    out = (float2*)a.delay;
+    for (int r = tid; r < n; r += T) out[2 * (size_t)(b + r) + cp] = Y[pre[nas[r]]];
+    PHASE(9);
+    // ldelay (up): cap*delay over the subtree
+    up_scan<T, K>(n, [&](int i) { return f2mul(capx(i), Y[i]); }, L, Bh, Bl, sm);
+    for (int i = tid; i < n; i += T) X[i] = up_range<K>(L, Bh, Bl, i, i + (int)size[i] - 1);
+    __syncthreads();
+    out = (float2*)a.ldelay;
+    for (int r = tid; r < n; r += T) out[2 * (size_t)(b + r) + cp] = X[pre[nas[r]]];
+    PHASE(10);
+    // beta (down) -> impulse = 2*beta - delay^2, kept in L
+    if (tid == 0) L[0] = make_float2(0.f, 0.f);
+    down_scan<T, K>(
+        A,
+        [&](int p) {
+          const int c = (int)code[p];
+          const int i = (c > 0 ? c : -c) - 1;
+          return f2scale(X[i], c > 0 ? pres[i] : -pres[i]);
+        },
+        [&](int p, float2 v) {
+          const int c = (int)code[p];
+          if (c > 0) {
+            const float2 d = Y[c - 1];
+            L[c - 1] = make_float2(fmaf(-d.x, d.x, 2.0f * v.x), fmaf(-d.y, d.y, 2.0f * v.y));
+          }
+        },
+        sm);
+    out = (float2*)a.impulse;
+    for (int r = tid; r < n; r += T) out[2 * (size_t)(b + r) + cp] = L[pre[nas[r]]];
+    if (a.sinks_start) {
+      const int s0 = a.sinks_start[net], s1 = a.sinks_start[net + 1];
+      const float2 si = ((const float2*)a.driver_slew)[2 * (size_t)net + cp];
+      float2* so = (float2*)a.sink_slew;
+      for (int k = s0 + tid; k < s1; k += T) {
+        const int v = a.sink_nodes[k];
+        if ((unsigned)v >= (unsigned)n) { report(a, OTG_ERR_INVALID, net); continue; }
+        const float2 iv = L[pre[v]];
+        so[2 * (size_t)k + cp] = make_float2(copysignf(sqrtf(si.x * si.x + iv.x), si.x),
+                                             copysignf(sqrtf(si.y * si.y + iv.y), si.y));
+      }
     }
+    __syncthreads();
+    PHASE(11);
   }
-  __syncthreads();
 }
 
-template <int T, bool SMEM>
+template <int T, int K, class Ix, bool SMEM>
 __global__ void __launch_bounds__(T) rc_block_kernel(RcArgs a, const int* list, const int* count,
                                                      int* work, char* gws, size_t ws_stride) {
   extern __shared__ __align__(16) char dsm[];
-  __shared__ int sh[64 + 2 * (T / 32) * NC];
+  __shared__ int sh[64 + 8 * (T / 32) + 8];
   __shared__ int s_item;
   char* ws = SMEM ? dsm : gws + (size_t)blockIdx.x * ws_stride;
   const int cnt = *count;
@@ -829,7 +973,7 @@ __global__ void __launch_bounds__(T) rc_block_kernel(RcArgs a, const int* list, 
     if (item >= cnt) break;
     const int net = list[item];
     const int n = a.nodes_start[net + 1] - a.nodes_start[net];
-    rc_net_block<T>(a, net, ws, n, sh);
+    rc_net_block<T, K, Ix>(a, net, ws, n, sh);
     __syncthreads();
   }
 }
@@ -886,60 +1030,86 @@ DevInfo& dev_info() {
 // kernel (sh[], s_item: under 1 KB).
 constexpr int kStaticSmemReserve = 2048;
 
-// Size classes: warp path, then block paths in shared memory, then the
-// global-workspace path.  T per class is fixed at compile time.
-constexpr int kClassT[RcClasses::kMax] = {32, 128, 128, 256, 256, 512, 512};
+// Size classes.  Class 0: warp path.  Classes 1..6: one CTA per net in
+// shared memory (16-bit indices), T threads with K slots per thread per
+// scan tile.  Class 7: nets beyond the shared-memory budget, in per-CTA
+// slices of the workspace (32-bit indices).
+struct ClassShape {
+  int nmax, T, K;
+};
+constexpr ClassShape kShapes[RcClasses::kMax] = {
+    {32, 32, 1}, {128, 64, 4}, {256, 64, 8}, {512, 128, 8}, {1024, 256, 8},
+    {2048, 512, 8}, {0, 512, 8}, {1 << 30, 512, 8}};
 
 }  // namespace
 
-// Largest n of the last shared-memory class for a given opt-in budget.
-int rc_smem_nmax(int T, int smem_budget) {
-  int lo = 33, hi = 1 << 16;
-  if (rc_layout(lo, T).total > (uint32_t)smem_budget) return 32;
+// Largest n whose 16-bit block layout fits the shared-memory budget.
+int rc_smem_nmax(int T, int K, int smem_budget) {
+  int lo = 33, hi = 32767;
+  if (rc_layout(lo, T, K, 2).total > (uint32_t)smem_budget) return 32;
   while (lo < hi) {
-    int mid = (lo + hi + 1) / 2;
-    if (rc_layout(mid, T).total <= (uint32_t)smem_budget) lo = mid; else hi = mid - 1;
+    const int mid = (lo + hi + 1) / 2;
+    if (rc_layout(mid, T, K, 2).total <= (uint32_t)smem_budget) lo = mid; else hi = mid - 1;
   }
   return lo;
 }
 
 RcClasses rc_classes(int smem_budget) {
   RcClasses c;
-  c.num = 7;
-  c.nmax[0] = 32;
-  c.nmax[1] = 128;
-  c.nmax[2] = 256;
-  c.nmax[3] = 512;
-  c.nmax[4] = 1024;
-  c.nmax[5] = std::max(1025, rc_smem_nmax(512, smem_budget));
-  c.nmax[6] = 1 << 30;  // global workspace
+  c.num = RcClasses::kMax;
+  for (int i = 0; i < c.num; ++i) c.nmax[i] = kShapes[i].nmax;
+  c.nmax[6] = std::max(kShapes[5].nmax + 1, rc_smem_nmax(512, 8, smem_budget));
   return c;
 }
 
-// Workspace: [status 64 B][counters 64 B][lists C x N ints][huge slices]
-static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+namespace {
+
+size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 // CTAs of the global-workspace path: two per SM, fewer when a slice is so
 // large that the slices would exceed 4 GiB.
-static int huge_ctas(int sms, size_t stride) {
+int huge_ctas(int sms, size_t stride) {
   const size_t cap = ((size_t)4 << 30) / std::max<size_t>(stride, 1);
   return (int)std::max<size_t>(1, std::min<size_t>((size_t)sms * 2, cap));
 }
 
+}  // namespace
+
+// Workspace: [status 64 B][counters 64 B][lists C x N ints][huge slices]
 size_t rc_workspace_bytes(int num_nets, int max_net_nodes, int sms, int smem_budget,
                           size_t* off_lists, size_t* off_huge, size_t* huge_stride) {
-  RcClasses c = rc_classes(smem_budget);
+  const RcClasses c = rc_classes(smem_budget);
   size_t o = 128;
   *off_lists = o;
   o = align256(o + (size_t)c.num * (size_t)std::max(num_nets, 1) * 4);
   *off_huge = o;
   *huge_stride = 0;
-  if (max_net_nodes > c.nmax[5]) {
-    *huge_stride = align256(rc_layout(max_net_nodes, 512).total);
+  if (max_net_nodes > c.nmax[6]) {
+    *huge_stride = align256(rc_layout(max_net_nodes, 512, 8, 4).total);
     o += *huge_stride * (size_t)huge_ctas(sms, *huge_stride);
   }
   return o;
 }
+
+namespace {
+
+template <int T, int K>
+cudaError_t launch_smem_class(const RcArgs& a, const int* list, int* count, int* work, int nmax,
+                              int sms, cudaStream_t stream) {
+  auto kern = rc_block_kernel<T, K, uint16_t, true>;
+  const size_t smem = rc_layout(nmax, T, K, 2).total;
+  cudaError_t err =
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  int occ = 1;
+  if (err == cudaSuccess) err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, T, smem);
+  if (err != cudaSuccess) return err;
+  occ = std::max(occ, 1);
+  kern<<<sms * occ, T, smem, stream>>>(a, list, count, work, nullptr, 0);
+  count_launch();
+  return cudaGetLastError();
+}
+
+}  // namespace
 
 otg_status rc_launch(const otg_rc_forest* f, int max_net_nodes, void* workspace,
                      size_t workspace_bytes, cudaStream_t stream) {
@@ -986,49 +1156,36 @@ otg_status rc_launch(const otg_rc_forest* f, int max_net_nodes, void* workspace,
       f->num_nets, f->nodes_start, max_net_nodes, cls, lists, counters, status);
   count_launch();
   const int N = f->num_nets;
-  // Largest nets first so the long tail overlaps the small ones.
   auto L = [&](int c) { return lists + (size_t)c * N; };
   int* work = counters + 8;
-  // huge (global workspace)
-  if (max_net_nodes > cls.nmax[5]) {
-    rc_block_kernel<512, false><<<huge_ctas(di.sms, stride), 512, 0, stream>>>(
-        a, L(6), counters + 6, work + 6, ws + off_huge, stride);
+  cudaError_t err = cudaSuccess;
+  // Largest nets first so the long tail overlaps the small ones.
+  if (max_net_nodes > cls.nmax[6]) {
+    rc_block_kernel<512, 8, int, false><<<huge_ctas(di.sms, stride), 512, 0, stream>>>(
+        a, L(7), counters + 7, work + 7, ws + off_huge, stride);
     count_launch();
+    err = cudaGetLastError();
   }
-  // shared-memory classes, big to small
-  struct K { int c; int T; };
-  const int cmax[7] = {32, 128, 256, 512, 1024, cls.nmax[5], 0};
-  for (int c = 5; c >= 1; --c) {
-    if (max_net_nodes <= cmax[c - 1]) continue;
-    const int nmax = std::min(cmax[c], max_net_nodes);
-    const int T = kClassT[c];
-    const size_t smem = rc_layout(nmax, T).total;
-    int occ = 1;
-    cudaError_t err = cudaSuccess;
-#define LAUNCH_BLOCK(TT)                                                                     \
-  do {                                                                                       \
-    auto kern = rc_block_kernel<TT, true>;                                                   \
-    err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); \
-    if (err == cudaSuccess)                                                                  \
-      err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, TT, smem);             \
-    if (err == cudaSuccess) {                                                                \
-      occ = std::max(occ, 1);                                                                \
-      kern<<<di.sms * occ, TT, smem, stream>>>(a, L(c), counters + c, work + c, nullptr, 0); \
-      count_launch();                                                                        \
-    }                                                                                        \
-  } while (0)
-    if (T == 128) LAUNCH_BLOCK(128);
-    else if (T == 256) LAUNCH_BLOCK(256);
-    else LAUNCH_BLOCK(512);
-#undef LAUNCH_BLOCK
-    if (err != cudaSuccess) {
-      cudaGetLastError();  // do not leave the error for the caller's next call
-      return OTG_ERR_CUDA;
+  for (int c = 6; c >= 1 && err == cudaSuccess; --c) {
+    if (max_net_nodes <= cls.nmax[c - 1]) continue;
+    const int nmax = std::min(cls.nmax[c], max_net_nodes);
+    switch (c) {
+      case 1: err = launch_smem_class<64, 4>(a, L(c), counters + c, work + c, nmax, di.sms, stream); break;
+      case 2: err = launch_smem_class<64, 8>(a, L(c), counters + c, work + c, nmax, di.sms, stream); break;
+      case 3: err = launch_smem_class<128, 8>(a, L(c), counters + c, work + c, nmax, di.sms, stream); break;
+      case 4: err = launch_smem_class<256, 8>(a, L(c), counters + c, work + c, nmax, di.sms, stream); break;
+      default: err = launch_smem_class<512, 8>(a, L(c), counters + c, work + c, nmax, di.sms, stream); break;
     }
   }
-  rc_warp_kernel<<<di.sms * 8, 256, 0, stream>>>(a, L(0), counters + 0, work + 0);
-  count_launch();
-  if (cudaGetLastError() != cudaSuccess) return OTG_ERR_CUDA;
+  if (err == cudaSuccess) {
+    rc_warp_kernel<<<di.sms * 8, 256, 0, stream>>>(a, L(0), counters + 0, work + 0);
+    count_launch();
+    err = cudaGetLastError();
+  }
+  if (err != cudaSuccess) {
+    cudaGetLastError();  // do not leave the error for the caller's next call
+    return OTG_ERR_CUDA;
+  }
   return OTG_OK;
 }
 
@@ -1050,6 +1207,19 @@ otg_status otg_rc_timing(const otg_rc_forest* forest, int32_t max_net_nodes, voi
                          size_t workspace_bytes, otg_stream_t stream) {
   return otg::rc_launch(forest, max_net_nodes, workspace, workspace_bytes, (cudaStream_t)stream);
 }
+
+#ifdef OTG_PHASE_TIMING
+// Instrumented builds only: copies (and clears) the per-phase cycle totals.
+int otg_debug_phase_cycles(unsigned long long* out, int n) {
+  if (n > 32) n = 32;
+  if (cudaMemcpyFromSymbol(out, otg::otg_phase_cycles, sizeof(unsigned long long) * n) !=
+      cudaSuccess)
+    return -1;
+  unsigned long long z[32] = {0};
+  cudaMemcpyToSymbol(otg::otg_phase_cycles, z, sizeof(z));
+  return n;
+}
+#endif
 
 otg_status otg_rc_status(const void* workspace, otg_stream_t stream, int32_t* bad_net) {
   if (!workspace) return OTG_ERR_INVALID;
