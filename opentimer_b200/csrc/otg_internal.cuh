@@ -18,18 +18,19 @@ void count_launch();
 //                   local id), tour[2m] (adjacency, then the Euler tour,
 //                   then signed tour codes), pres[n] f32 (by preorder)
 //   A  (topology)   es[m], et[m], then one of
-//                     A-a  ends[n] i32, posin[2m] (+ radix buffers 2x2m)
+//                     A-a  ends[n] i32, posin[2m]
 //                     A-b  sub[2m], off[2m], spl[2m], splarc[S], sl[S] u64
 //                     A-c  depth[n], parent[n], pedge[n], slot[n]
 //                   then succ[2m] / radix buffers 2n, hist[256*W] i32
 //   B  (Elmore, one corner pair at a time; overlays A)
-//                   X[n] f2, Y[n] f2, L[n] f2, Bh[c] f2, Bl[c] f2
-//                   (c = ceil(n/K) thread chunks of K preorder slots)
+//                   X[n] f2 (load, then ldelay), Y[n] f2 (delay),
+//                   Ip[n] 2 x i64 (fixed-point inclusive prefix of an
+//                   up-sweep; then the impulse, f2)
 struct RcLayout {
   uint32_t pre, nap, size, nas, tour, pres;
-  uint32_t es, et, ends, posin, rb, sub, off, spl, splarc, sl, depth, parent, pedge, slot;
+  uint32_t es, et, ends, posin, sub, off, spl, splarc, sl, depth, parent, pedge, slot;
   uint32_t r2, hist;
-  uint32_t X, Y, L, Bh, Bl;
+  uint32_t X, Y, Ip;
   uint32_t total;
   uint32_t ns_cap;  // capacity of the splitter arrays
 };
@@ -44,7 +45,8 @@ __host__ __device__ inline uint32_t rc_max3(uint32_t a, uint32_t b, uint32_t c) 
 __host__ __device__ inline RcLayout rc_layout(int n, int T, int K, int ib) {
   RcLayout l;
   const uint32_t N = (uint32_t)n, M = n > 0 ? (uint32_t)(n - 1) : 0u, A = 2u * M;
-  const uint32_t W = (uint32_t)T / 32u, NCH = (N + (uint32_t)K - 1u) / (uint32_t)K + 1u;
+  const uint32_t W = (uint32_t)T / 32u;
+  (void)K;
   const uint32_t I = (uint32_t)ib;
   l.ns_cap = 2u * (A / (uint32_t)kSplit) + 64u;
   uint32_t o = 0;
@@ -67,8 +69,7 @@ __host__ __device__ inline RcLayout rc_layout(int n, int T, int K, int ib) {
   // A-a
   OTG_TAKE(ends, 4u * N);
   OTG_TAKE(posin, I * A);
-  l.rb = l.posin;  // adjacency radix fallback: 2 x A indices from here
-  const uint32_t end_a = OTG_AL(l.posin + 2u * I * A);
+  const uint32_t end_a = o;
   // A-b
   o = r1;
   OTG_TAKE(sub, I * A);
@@ -91,9 +92,7 @@ __host__ __device__ inline RcLayout rc_layout(int n, int T, int K, int ib) {
   o = rA;
   OTG_TAKE(X, 8u * N);
   OTG_TAKE(Y, 8u * N);
-  OTG_TAKE(L, 8u * N);
-  OTG_TAKE(Bh, 8u * NCH);
-  OTG_TAKE(Bl, 8u * NCH);
+  OTG_TAKE(Ip, 16u * N);
 #undef OTG_TAKE
 #undef OTG_AL
   l.total = endA > o ? endA : o;

@@ -439,174 +439,169 @@ __device__ void block_radix_sort(int N, int nbits, KeyF key, Ix* b0, Ix* b1, Ix*
   }
 }
 
-__device__ __forceinline__ float2 f2add(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ float2 f2mul(float2 a, float2 b) { return make_float2(a.x * b.x, a.y * b.y); }
 __device__ __forceinline__ float2 f2scale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
 
-// Warp-level inclusive float-float scan of (h, l) per component, returning
-// the warp-exclusive prefix in (eh, el) and the inclusive one in (h, l).
-__device__ __forceinline__ void warp_ff_scan2(float (&h)[2], float (&l)[2], float (&eh)[2],
-                                              float (&el)[2]) {
+// ------------------------------------------------ exact fixed-point sums
+// Every fp32 term x of a sweep is mapped to the integer rint(x * 2^s), with
+// one power of two per net, corner and sweep chosen from n * max|x| so that
+// no partial sum reaches 2^62.  int64 sums of those integers are exact, so
+// a subtree sum taken as a difference of two prefixes has no cancellation
+// error and no result depends on the order of the terms -- the tour may
+// visit children in any order and every output is still bit-reproducible.
+// Each term is rounded once to a grid of 2^-s (relative to n * max|x| that
+// is 2^-61), each result once back to fp32.
+
+__device__ __forceinline__ float pow2f(int e) { return __int_as_float((e + 127) << 23); }
+
+// 2^s and 2^-s for terms with |x| <= mx over n positions.
+__device__ __forceinline__ void fx_scale(float mx, int n, float& up, float& dn) {
+  const float bound = mx * (float)n;
+  int s = 0;
+  if (bound > 0.f) {
+    // bound < 2^e with e from the exponent field; s leaves one bit of margin
+    const int e = ((__float_as_int(bound) >> 23) & 0xff) - 126;
+    s = min(max(61 - e, -126), 126);
+  }
+  up = pow2f(s);
+  dn = pow2f(-s);
+}
+__device__ __forceinline__ long long to_fx(float x, float up) { return __float2ll_rn(x * up); }
+__device__ __forceinline__ float from_fx(long long v, float dn) { return __ll2float_rn(v) * dn; }
+
+// Warp-inclusive int64 scan of two values; ex gets the warp-exclusive prefix.
+__device__ __forceinline__ void warp_i64_scan2(long long (&v)[2], long long (&ex)[2]) {
   const int lane = threadIdx.x & 31;
 #pragma unroll
   for (int d = 1; d < 32; d <<= 1) {
 #pragma unroll
     for (int j = 0; j < 2; ++j) {
-      const float yh = __shfl_up_sync(FULL, h[j], d), yl = __shfl_up_sync(FULL, l[j], d);
-      if (lane >= d) {
-        float sh = yh, sl = yl;
-        ffadd(sh, sl, h[j], l[j]);
-        h[j] = sh;
-        l[j] = sl;
-      }
+      const long long y = __shfl_up_sync(FULL, v[j], d);
+      if (lane >= d) v[j] += y;
     }
   }
 #pragma unroll
   for (int j = 0; j < 2; ++j) {
-    const float xh = __shfl_up_sync(FULL, h[j], 1), xl = __shfl_up_sync(FULL, l[j], 1);
-    eh[j] = lane ? xh : 0.f;
-    el[j] = lane ? xl : 0.f;
+    const long long t = __shfl_up_sync(FULL, v[j], 1);
+    ex[j] = lane ? t : 0;
   }
 }
 
-// Block part of a tile scan: warp totals -> per-warp exclusive base (ff)
-// and the tile total; sm holds >= 8*W + 4 floats.  Ends with a barrier.
+// Block part of a tile scan: per-warp exclusive bases and the tile total
+// from the warps' inclusive totals (held by lane 31).  shl holds 4*W+2
+// int64.  Ends after the second barrier; the caller syncs before reuse.
 template <int T>
-__device__ __forceinline__ void tile_ff_bases(const float (&wh)[2], const float (&wl)[2],
-                                              float (&bh)[2], float (&bl)[2], float (&th)[2],
-                                              float (&tl)[2], float* sm) {
+__device__ __forceinline__ void tile_i64_bases(const long long (&v)[2], long long (&wb)[2],
+                                               long long (&tt)[2], long long* shl) {
   constexpr int W = T / 32;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  float* swh = sm;
-  float* swl = sm + 2 * W;
-  float* sph = sm + 4 * W;
-  float* spl = sm + 6 * W;
-  float* stt = sm + 8 * W;
-  if (lane == 31) {
-    swh[2 * w] = wh[0]; swh[2 * w + 1] = wh[1];
-    swl[2 * w] = wl[0]; swl[2 * w + 1] = wl[1];
-  }
+  if (lane == 31) { shl[2 * w] = v[0]; shl[2 * w + 1] = v[1]; }
   __syncthreads();
   if (w == 0) {
-    float h[2], l[2], eh[2], el[2];
+    long long x[2], ex[2];
 #pragma unroll
-    for (int j = 0; j < 2; ++j) {
-      h[j] = lane < W ? swh[2 * lane + j] : 0.f;
-      l[j] = lane < W ? swl[2 * lane + j] : 0.f;
-    }
-    warp_ff_scan2(h, l, eh, el);
-    if (lane < W) {
-      sph[2 * lane] = eh[0]; sph[2 * lane + 1] = eh[1];
-      spl[2 * lane] = el[0]; spl[2 * lane + 1] = el[1];
-    }
-    if (lane == W - 1) { stt[0] = h[0]; stt[1] = h[1]; stt[2] = l[0]; stt[3] = l[1]; }
+    for (int j = 0; j < 2; ++j) x[j] = lane < W ? shl[2 * lane + j] : 0;
+    warp_i64_scan2(x, ex);
+    if (lane < W) { shl[2 * W + 2 * lane] = ex[0]; shl[2 * W + 2 * lane + 1] = ex[1]; }
+    if (lane == W - 1) { shl[4 * W] = x[0]; shl[4 * W + 1] = x[1]; }
   }
   __syncthreads();
 #pragma unroll
   for (int j = 0; j < 2; ++j) {
-    bh[j] = sph[2 * w + j];
-    bl[j] = spl[2 * w + j];
-    th[j] = stt[j];
-    tl[j] = stt[2 + j];
+    wb[j] = shl[2 * W + 2 * w + j];
+    tt[j] = shl[4 * W + j];
   }
 }
 
-// Compensated up-sweep over n preorder slots for one corner pair:
-// L[p] = fp32 inclusive prefix inside the thread's K-slot chunk,
-// Bh/Bl[p/K] = float-float exclusive prefix of the chunks.  Only the
-// <= K-term local part is uncompensated, so a range sum carries an error
-// relative to the range itself (every subtree on a long path shares the
-// same right end; an error there would repeat along the path's delays).
+// Up-sweep over n preorder slots for one corner pair: Ip[p] = exact
+// fixed-point inclusive prefix of x(0..p).  K slots per thread per tile.
 template <int T, int K, class XF>
-__device__ void up_scan(int n, XF x, float2* L, float2* Bh, float2* Bl, float* sm) {
-  float ch[2] = {0.f, 0.f}, cl[2] = {0.f, 0.f};
+__device__ void up_scan_fx(int n, XF x, const float (&up)[2], longlong2* Ip, long long* shl) {
+  long long carry[2] = {0, 0};
   for (int base = 0; base < n; base += T * K) {
     const int q0 = base + threadIdx.x * K;
-    float2 acc = make_float2(0.f, 0.f);
+    long long loc[K][2];
+    long long acc[2] = {0, 0};
 #pragma unroll
     for (int k = 0; k < K; ++k) {
       if (q0 + k < n) {
-        acc = f2add(acc, x(q0 + k));
-        L[q0 + k] = acc;
+        const float2 v = x(q0 + k);
+        acc[0] += to_fx(v.x, up[0]);
+        acc[1] += to_fx(v.y, up[1]);
       }
+      loc[k][0] = acc[0];
+      loc[k][1] = acc[1];
     }
-    float h[2] = {acc.x, acc.y}, l[2] = {0.f, 0.f}, eh[2], el[2];
-    warp_ff_scan2(h, l, eh, el);
-    float bh[2], bl[2], th[2], tl[2];
-    tile_ff_bases<T>(h, l, bh, bl, th, tl, sm);
+    long long ex[2], wb[2], tt[2];
+    warp_i64_scan2(acc, ex);
+    tile_i64_bases<T>(acc, wb, tt, shl);
+    const long long b0 = carry[0] + wb[0] + ex[0], b1 = carry[1] + wb[1] + ex[1];
 #pragma unroll
-    for (int j = 0; j < 2; ++j) {
-      ffadd(bh[j], bl[j], ch[j], cl[j]);
-      ffadd(bh[j], bl[j], eh[j], el[j]);
-      ffadd(ch[j], cl[j], th[j], tl[j]);
-    }
-    if (q0 < n) {
-      Bh[q0 / K] = make_float2(bh[0], bh[1]);
-      Bl[q0 / K] = make_float2(bl[0], bl[1]);
-    }
+    for (int k = 0; k < K; ++k)
+      if (q0 + k < n) Ip[q0 + k] = make_longlong2(b0 + loc[k][0], b1 + loc[k][1]);
+    carry[0] += tt[0];
+    carry[1] += tt[1];
     __syncthreads();
   }
 }
 
-// Range sum over preorder slots [lo, hi] of an up_scan.
-template <int K>
-__device__ __forceinline__ float2 up_range(const float2* L, const float2* Bh, const float2* Bl,
-                                           int lo, int hi) {
-  const int cb = hi / K;
-  float2 hb = Bh[cb], lb = Bl[cb], Lb = L[hi];
-  float2 ha = make_float2(0.f, 0.f), la = ha, La = ha;
+// Sum over preorder slots [lo, hi] of an up_scan_fx, back in fp32.
+__device__ __forceinline__ float2 up_range_fx(const longlong2* Ip, int lo, int hi,
+                                              const float (&dn)[2]) {
+  longlong2 h = Ip[hi];
   if (lo > 0) {
-    const int ca = (lo - 1) / K;
-    ha = Bh[ca];
-    la = Bl[ca];
-    La = L[lo - 1];
+    const longlong2 l = Ip[lo - 1];
+    h.x -= l.x;
+    h.y -= l.y;
   }
-  float h0 = hb.x, l0 = lb.x, h1 = hb.y, l1 = lb.y;
-  ffadd(h0, l0, -ha.x, -la.x);
-  ffadd(h1, l1, -ha.y, -la.y);
-  return make_float2(h0 + (l0 + (Lb.x - La.x)), h1 + (l1 + (Lb.y - La.y)));
+  return make_float2(from_fx(h.x, dn[0]), from_fx(h.y, dn[1]));
 }
 
-// Compensated inclusive prefix over A tour slots for one corner pair:
-// x(p) is the signed contribution of slot p, emit(p, v) gets the prefix.
-// The tour alternates +w / -w, so even the thread-local part is kept in
-// float-float: an fp32 thread total would carry an error of order u*|w|
-// into the prefix of every later slot.
+// Inclusive prefix over A tour slots for one corner pair: x(p) is the
+// signed term of slot p; emit(p, v0, v1) receives the exact fixed-point
+// prefix (converted by the callee only where it is used).
 template <int T, int K, class XF, class EmitF>
-__device__ void down_scan(int A, XF x, EmitF emit, float* sm) {
-  float ch[2] = {0.f, 0.f}, cl[2] = {0.f, 0.f};
+__device__ void down_scan_fx(int A, XF x, const float (&up)[2], EmitF emit, long long* shl) {
+  long long carry[2] = {0, 0};
   for (int base = 0; base < A; base += T * K) {
     const int q0 = base + threadIdx.x * K;
-    float ph[K][2], pl[K][2];
-    float h[2] = {0.f, 0.f}, l[2] = {0.f, 0.f};
-#pragma unroll
-    for (int k = 0; k < K; ++k) {
-      const float2 v = (q0 + k < A) ? x(q0 + k) : make_float2(0.f, 0.f);
-      ffadd(h[0], l[0], v.x, 0.f);
-      ffadd(h[1], l[1], v.y, 0.f);
-      ph[k][0] = h[0]; pl[k][0] = l[0];
-      ph[k][1] = h[1]; pl[k][1] = l[1];
-    }
-    float eh[2], el[2];
-    warp_ff_scan2(h, l, eh, el);
-    float bh[2], bl[2], th[2], tl[2];
-    tile_ff_bases<T>(h, l, bh, bl, th, tl, sm);
-#pragma unroll
-    for (int j = 0; j < 2; ++j) {
-      ffadd(bh[j], bl[j], ch[j], cl[j]);
-      ffadd(bh[j], bl[j], eh[j], el[j]);
-      ffadd(ch[j], cl[j], th[j], tl[j]);
-    }
+    long long loc[K][2];
+    long long acc[2] = {0, 0};
 #pragma unroll
     for (int k = 0; k < K; ++k) {
       if (q0 + k < A) {
-        float h0 = bh[0], l0 = bl[0], h1 = bh[1], l1 = bl[1];
-        ffadd(h0, l0, ph[k][0], pl[k][0]);
-        ffadd(h1, l1, ph[k][1], pl[k][1]);
-        emit(q0 + k, make_float2(h0 + l0, h1 + l1));
+        const float2 v = x(q0 + k);
+        acc[0] += to_fx(v.x, up[0]);
+        acc[1] += to_fx(v.y, up[1]);
       }
+      loc[k][0] = acc[0];
+      loc[k][1] = acc[1];
     }
+    long long ex[2], wb[2], tt[2];
+    warp_i64_scan2(acc, ex);
+    tile_i64_bases<T>(acc, wb, tt, shl);
+    const long long b0 = carry[0] + wb[0] + ex[0], b1 = carry[1] + wb[1] + ex[1];
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+      if (q0 + k < A) emit(q0 + k, b0 + loc[k][0], b1 + loc[k][1]);
+    carry[0] += tt[0];
+    carry[1] += tt[1];
     __syncthreads();
+  }
+}
+
+// Per-corner maxima of non-negative terms, gathered into smx[0..1] (float
+// bits, which order like unsigned ints for non-negative floats).
+__device__ __forceinline__ void max2_accumulate(float2 v, float (&m)[2]) {
+  m[0] = fmaxf(m[0], fabsf(v.x));
+  m[1] = fmaxf(m[1], fabsf(v.y));
+}
+__device__ __forceinline__ void max2_commit(const float (&m)[2], unsigned* smx) {
+  const unsigned a = __reduce_max_sync(FULL, __float_as_uint(m[0]));
+  const unsigned c = __reduce_max_sync(FULL, __float_as_uint(m[1]));
+  if ((threadIdx.x & 31) == 0) {
+    atomicMax(&smx[0], a);
+    atomicMax(&smx[1], c);
   }
 }
 
@@ -629,7 +624,8 @@ __device__ __forceinline__ bool is_splitter(int arc, int sel, int first) {
 }
 
 template <int T, int K, class Ix>
-__device__ void rc_net_block(const RcArgs& a, int net, char* ws, int n, int* sh) {
+__device__ void rc_net_block(const RcArgs& a, int net, char* ws, int n, int* sh,
+                             long long* shl) {
   using S = typename IxT<Ix>::S;
   constexpr unsigned NONE = IxT<Ix>::NONE;
   const int tid = threadIdx.x;
@@ -647,8 +643,6 @@ __device__ void rc_net_block(const RcArgs& a, int net, char* ws, int n, int* sh)
   Ix* et = (Ix*)(ws + lay.et);
   int* ends = (int*)(ws + lay.ends);
   Ix* posin = (Ix*)(ws + lay.posin);
-  Ix* rb0 = (Ix*)(ws + lay.rb);
-  Ix* rb1 = rb0 + A;
   Ix* sub = (Ix*)(ws + lay.sub);
   Ix* off = (Ix*)(ws + lay.off);
   Ix* spl = (Ix*)(ws + lay.spl);
@@ -662,14 +656,11 @@ __device__ void rc_net_block(const RcArgs& a, int net, char* ws, int n, int* sh)
   int* hist = (int*)(ws + lay.hist);
   float2* X = (float2*)(ws + lay.X);
   float2* Y = (float2*)(ws + lay.Y);
-  float2* L = (float2*)(ws + lay.L);
-  float2* Bh = (float2*)(ws + lay.Bh);
-  float2* Bl = (float2*)(ws + lay.Bl);
+  longlong2* Ip = (longlong2*)(ws + lay.Ip);
   int* wsum = sh;          // [W]
   int* s_flag = sh + 32;   // error code
   int* s_maxd = sh + 33;   // max depth
-  int* s_hub = sh + 34;    // a node of degree > 32 exists
-  float* sm = (float*)(sh + 64);
+  unsigned* smx = (unsigned*)(sh + 40);  // [8] per-sweep maxima (float bits)
   const int root = a.roots[net];
   auto src = [&](int arc) -> int { return (arc & 1) ? (int)et[arc >> 1] : (int)es[arc >> 1]; };
   auto dst = [&](int arc) -> int { return (arc & 1) ? (int)es[arc >> 1] : (int)et[arc >> 1]; };
@@ -685,7 +676,6 @@ __device__ void rc_net_block(const RcArgs& a, int net, char* ws, int n, int* sh)
   if (tid == 0) {
     *s_flag = ((unsigned)root >= (unsigned)n) ? OTG_ERR_INVALID : 0;
     *s_maxd = 0;
-    *s_hub = 0;
   }
   for (int v = tid; v < n; v += T) ends[v] = 0;
   __syncthreads();
@@ -708,35 +698,15 @@ __device__ void rc_net_block(const RcArgs& a, int net, char* ws, int n, int* sh)
       [&](int v, int p, int d) {
         ends[v] = p;
         if (d == 0) *s_flag = OTG_ERR_NOT_TREE;
-        if (d > 32) *s_hub = 1;
       },
       wsum);
   if (fail()) return;
   PHASE(1);
-  // ---- A3: adjacency lists in arc-id order (arc 2e: s->t, 2e+1: t->s).
-  // After this, node v's arcs are tour[begin(v) .. ends[v]).
-  if (!*s_hub) {
-    for (int arc = tid; arc < A; arc += T) tour[atomicAdd(&ends[src(arc)], 1)] = (Ix)arc;
-    __syncthreads();
-    for (int v = tid; v < n; v += T) {
-      const int lo = v ? ends[v - 1] : 0, hi = ends[v];
-      for (int i = lo + 1; i < hi; ++i) {
-        const Ix x = tour[i];
-        int j = i - 1;
-        while (j >= lo && tour[j] > x) {
-          tour[j + 1] = tour[j];
-          --j;
-        }
-        tour[j + 1] = x;
-      }
-    }
-  } else {
-    block_radix_sort<T>(A, 32 - __clz(n - 1), [&](int arc) { return src(arc); }, rb0, rb1, tour,
-                        hist, wsum);
-    for (int v = tid; v < n; v += T) rb0[v] = (Ix)(v + 1 < n ? ends[v + 1] : A);
-    __syncthreads();
-    for (int v = tid; v < n; v += T) ends[v] = (int)rb0[v];
-  }
+  // ---- A3: adjacency lists by atomic fill.  The order inside a list only
+  // decides the tour's child order, which no output depends on (the BFS
+  // slots follow (depth, id), the Elmore sums are exact).  After this, node
+  // v's arcs are tour[begin(v) .. ends[v]).
+  for (int arc = tid; arc < A; arc += T) tour[atomicAdd(&ends[src(arc)], 1)] = (Ix)arc;
   __syncthreads();
   PHASE(2);
   // ---- A4: Euler-tour successor: after (u->v) comes v's next arc after (v->u)
@@ -885,61 +855,102 @@ __device__ void rc_net_block(const RcArgs& a, int net, char* ws, int n, int* sh)
   __syncthreads();
   PHASE(7);
 
-  // ---- B: Elmore, one corner pair at a time (corners 2cp, 2cp+1)
+  // ---- B: Elmore, one corner pair at a time (corners 2cp, 2cp+1), with
+  // exact fixed-point sums (see fx_scale).  The maximum term of every sweep
+  // is gathered in the loop before it (smx) to set its scale.
   const float2* cap2 = (const float2*)a.cap;
   for (int cp = 0; cp < 2; ++cp) {
     float2* out;
+    float up[2], dn[2], m[2];
     auto capx = [&](int i) { return cap2[2 * (size_t)(b + (int)nap[i]) + cp]; };
+    auto scale = [&](int k) {
+      fx_scale(__uint_as_float(smx[2 * k]), n, up[0], dn[0]);
+      fx_scale(__uint_as_float(smx[2 * k + 1]), n, up[1], dn[1]);
+    };
+    if (tid < 8) smx[tid] = 0u;
+    __syncthreads();
+    m[0] = m[1] = 0.f;
+    for (int i = tid; i < n; i += T) max2_accumulate(capx(i), m);
+    max2_commit(m, smx + 0);
+    __syncthreads();
     // load (up): cap summed over the subtree
-    up_scan<T, K>(n, capx, L, Bh, Bl, sm);
-    for (int i = tid; i < n; i += T) X[i] = up_range<K>(L, Bh, Bl, i, i + (int)size[i] - 1);
+    scale(0);
+    up_scan_fx<T, K>(n, capx, up, Ip, shl);
+    m[0] = m[1] = 0.f;
+    for (int i = tid; i < n; i += T) {
+      const float2 v = up_range_fx(Ip, i, i + (int)size[i] - 1, dn);
+      X[i] = v;
+      max2_accumulate(f2scale(v, pres[i]), m);
+    }
+    max2_commit(m, smx + 2);
     __syncthreads();
     out = (float2*)a.load;
     for (int r = tid; r < n; r += T) out[2 * (size_t)(b + r) + cp] = X[pre[nas[r]]];
     PHASE(8);
     // delay (down): +pres*load entering a node, - leaving it
+    scale(1);
     if (tid == 0) Y[0] = make_float2(0.f, 0.f);
-    down_scan<T, K>(
+    down_scan_fx<T, K>(
         A,
         [&](int p) {
           const int c = (int)code[p];
           const int i = (c > 0 ? c : -c) - 1;
           return f2scale(X[i], c > 0 ? pres[i] : -pres[i]);
         },
-        [&](int p, float2 v) {
+        up,
+        [&](int p, long long v0, long long v1) {
           const int c = (int)code[p];
-          if (c > 0) Y[c - 1] = v;
+          if (c > 0) Y[c - 1] = make_float2(from_fx(v0, dn[0]), from_fx(v1, dn[1]));
         },
-        sm);
+        shl);
+    m[0] = m[1] = 0.f;
     out = (float2*)a.delay;
-    for (int r = tid; r < n; r += T) out[2 * (size_t)(b + r) + cp] = Y[pre[nas[r]]];
+    for (int r = tid; r < n; r += T) {
+      const int i = (int)pre[nas[r]];
+      const float2 d = Y[i];
+      out[2 * (size_t)(b + r) + cp] = d;
+      max2_accumulate(f2mul(capx(i), d), m);
+    }
+    max2_commit(m, smx + 4);
+    __syncthreads();
     PHASE(9);
     // ldelay (up): cap*delay over the subtree
-    up_scan<T, K>(n, [&](int i) { return f2mul(capx(i), Y[i]); }, L, Bh, Bl, sm);
-    for (int i = tid; i < n; i += T) X[i] = up_range<K>(L, Bh, Bl, i, i + (int)size[i] - 1);
+    scale(2);
+    up_scan_fx<T, K>(n, [&](int i) { return f2mul(capx(i), Y[i]); }, up, Ip, shl);
+    m[0] = m[1] = 0.f;
+    for (int i = tid; i < n; i += T) {
+      const float2 v = up_range_fx(Ip, i, i + (int)size[i] - 1, dn);
+      X[i] = v;
+      max2_accumulate(f2scale(v, pres[i]), m);
+    }
+    max2_commit(m, smx + 6);
     __syncthreads();
     out = (float2*)a.ldelay;
     for (int r = tid; r < n; r += T) out[2 * (size_t)(b + r) + cp] = X[pre[nas[r]]];
     PHASE(10);
-    // beta (down) -> impulse = 2*beta - delay^2, kept in L
-    if (tid == 0) L[0] = make_float2(0.f, 0.f);
-    down_scan<T, K>(
+    // beta (down) -> impulse = 2*beta - delay^2, kept where Ip was
+    scale(3);
+    float2* imp = (float2*)Ip;
+    if (tid == 0) imp[0] = make_float2(0.f, 0.f);
+    down_scan_fx<T, K>(
         A,
         [&](int p) {
           const int c = (int)code[p];
           const int i = (c > 0 ? c : -c) - 1;
           return f2scale(X[i], c > 0 ? pres[i] : -pres[i]);
         },
-        [&](int p, float2 v) {
+        up,
+        [&](int p, long long v0, long long v1) {
           const int c = (int)code[p];
           if (c > 0) {
             const float2 d = Y[c - 1];
-            L[c - 1] = make_float2(fmaf(-d.x, d.x, 2.0f * v.x), fmaf(-d.y, d.y, 2.0f * v.y));
+            imp[c - 1] = make_float2(fmaf(-d.x, d.x, 2.0f * from_fx(v0, dn[0])),
+                                     fmaf(-d.y, d.y, 2.0f * from_fx(v1, dn[1])));
           }
         },
-        sm);
+        shl);
     out = (float2*)a.impulse;
-    for (int r = tid; r < n; r += T) out[2 * (size_t)(b + r) + cp] = L[pre[nas[r]]];
+    for (int r = tid; r < n; r += T) out[2 * (size_t)(b + r) + cp] = imp[pre[nas[r]]];
     if (a.sinks_start) {
       const int s0 = a.sinks_start[net], s1 = a.sinks_start[net + 1];
       const float2 si = ((const float2*)a.driver_slew)[2 * (size_t)net + cp];
@@ -947,7 +958,7 @@ __device__ void rc_net_block(const RcArgs& a, int net, char* ws, int n, int* sh)
       for (int k = s0 + tid; k < s1; k += T) {
         const int v = a.sink_nodes[k];
         if ((unsigned)v >= (unsigned)n) { report(a, OTG_ERR_INVALID, net); continue; }
-        const float2 iv = L[pre[v]];
+        const float2 iv = imp[pre[v]];
         so[2 * (size_t)k + cp] = make_float2(copysignf(sqrtf(si.x * si.x + iv.x), si.x),
                                              copysignf(sqrtf(si.y * si.y + iv.y), si.y));
       }
@@ -961,7 +972,8 @@ template <int T, int K, class Ix, bool SMEM>
 __global__ void __launch_bounds__(T) rc_block_kernel(RcArgs a, const int* list, const int* count,
                                                      int* work, char* gws, size_t ws_stride) {
   extern __shared__ __align__(16) char dsm[];
-  __shared__ int sh[64 + 8 * (T / 32) + 8];
+  __shared__ int sh[64];
+  __shared__ long long shl[4 * (T / 32) + 4];
   __shared__ int s_item;
   char* ws = SMEM ? dsm : gws + (size_t)blockIdx.x * ws_stride;
   const int cnt = *count;
@@ -973,7 +985,7 @@ __global__ void __launch_bounds__(T) rc_block_kernel(RcArgs a, const int* list, 
     if (item >= cnt) break;
     const int net = list[item];
     const int n = a.nodes_start[net + 1] - a.nodes_start[net];
-    rc_net_block<T, K, Ix>(a, net, ws, n, sh);
+    rc_net_block<T, K, Ix>(a, net, ws, n, sh, shl);
     __syncthreads();
   }
 }
@@ -1038,8 +1050,8 @@ struct ClassShape {
   int nmax, T, K;
 };
 constexpr ClassShape kShapes[RcClasses::kMax] = {
-    {32, 32, 1}, {128, 64, 4}, {256, 64, 8}, {512, 128, 8}, {1024, 256, 8},
-    {2048, 512, 8}, {0, 512, 8}, {1 << 30, 512, 8}};
+    {32, 32, 1}, {128, 64, 4}, {256, 64, 8}, {512, 128, 8}, {1024, 256, 4},
+    {2048, 256, 8}, {0, 512, 8}, {1 << 30, 512, 8}};
 
 }  // namespace
 
@@ -1173,7 +1185,8 @@ otg_status rc_launch(const otg_rc_forest* f, int max_net_nodes, void* workspace,
       case 1: err = launch_smem_class<64, 4>(a, L(c), counters + c, work + c, nmax, di.sms, stream); break;
       case 2: err = launch_smem_class<64, 8>(a, L(c), counters + c, work + c, nmax, di.sms, stream); break;
       case 3: err = launch_smem_class<128, 8>(a, L(c), counters + c, work + c, nmax, di.sms, stream); break;
-      case 4: err = launch_smem_class<256, 8>(a, L(c), counters + c, work + c, nmax, di.sms, stream); break;
+      case 4: err = launch_smem_class<256, 4>(a, L(c), counters + c, work + c, nmax, di.sms, stream); break;
+      case 5: err = launch_smem_class<256, 8>(a, L(c), counters + c, work + c, nmax, di.sms, stream); break;
       default: err = launch_smem_class<512, 8>(a, L(c), counters + c, work + c, nmax, di.sms, stream); break;
     }
   }
