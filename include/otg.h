@@ -147,6 +147,25 @@ otg_status otg_levelize_host(int32_t n, int32_t num_edges, const int32_t* fanin_
 /* Frees the host-path context of the current device. */
 void otg_release_host_context(void);
 
+/*
+ * otg_rc_timing_noalloc -- the fused pass of otg_rc_timing for callers that
+ * may not allocate device memory when they run RC timing (a host whose pool
+ * allocator owns all device memory, a loop that cannot afford cudaMalloc's
+ * device-wide synchronization).  This entry point has no counterpart in the
+ * reference.  Its workspace is a 16 MiB array compiled into libotg, held on
+ * every GPU that loads the library until the process exits; the caller
+ * passes only inputs and outputs (device pointers, as for otg_rc_timing).
+ * The first call on a device looks up that array's address, so make it
+ * before any stream capture.  Calls share the array: calls that overlap on
+ * the GPU race, so serialize them.  Blocks until `stream` finishes and
+ * returns the device-side status.  Limit: at most 524,284 nets per call and
+ * no net beyond the shared-memory classes (about 4,700 nodes on a B200);
+ * larger batches return OTG_ERR_WORKSPACE without launching.  Allocates
+ * nothing.
+ */
+otg_status otg_rc_timing_noalloc(const otg_rc_forest* forest, int32_t max_net_nodes,
+                                 otg_stream_t stream);
+
 /* Human-readable name of a status code. */
 const char* otg_status_string(otg_status s);
 

@@ -23,6 +23,7 @@ C_SYMBOLS = [
     "otg_rc_timing_host", "otg_levelize_host", "otg_release_host_context",
     "otg_status_string", "otg_kernel_launches",
     "otg_synth_rc_forest", "otg_synth_rc_sinks", "otg_synth_rc_forest_host",
+    "otg_rc_timing_noalloc",
 ]
 # The reference-compatible C++ entry points (include/otg_compat.hpp), by
 # their Itanium-mangled names.

@@ -106,4 +106,10 @@ struct RcClasses {
   int nmax[kMax];
 };
 
+
+
+// Entry of the fused RC pass with an explicit workspace (otg_rc.cu); the
+// public otg_rc_timing wraps it.
+otg_status rc_launch(const otg_rc_forest* f, int max_net_nodes, void* workspace,
+                     size_t workspace_bytes, cudaStream_t stream);
 }  // namespace otg
