@@ -31,6 +31,11 @@ METRIC = "RC-tree nodes/s (Elmore, 4 corners) & levelize edges/s; incr. p50/p99 
 NUM_NETS = 1_000_000
 SEED = 2024
 LV_PINS, LV_EDGES, LV_LEVELS = 5_000_000, 12_000_000, 200
+# incremental sizing loop
+INC_GATES, INC_ITERS, INC_FRAC, INC_PLAIN_ITERS, INC_CHECK = 200_000, 1000, 0.005, 20, True
+# serving
+SRV_DESIGNS, SRV_PINS_LO, SRV_PINS_HI = 16, 10_000, 2_000_000
+SRV_RATES, SRV_SECONDS, SRV_SLOTS, SRV_SAT_REQ = (2_000, 10_000, 50_000), 0.5, 4, 20_000
 
 
 def algorithmic_bytes(num_nets, total_nodes, num_sinks):
@@ -302,6 +307,14 @@ def run_ours(args, world, rank, local):
         line["levelize"] = lv
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(g, ns_np)
+    # the per-GPU incremental and serving loops (one GPU only)
+    if world == 1 and not (args.no_incremental and args.no_serving):
+        del batch, g
+        torch.cuda.empty_cache()
+    if world == 1 and not args.no_incremental:
+        line["incremental"] = run_incremental()
+    if world == 1 and not args.no_serving:
+        line["serving"] = run_serving()
     return line
 
 
@@ -379,6 +392,129 @@ def run_levelize(args, world, dev):
             "workload": f"pin DAG {n} pins, {E} edges, {L} levels (seeded)"}
 
 
+def _pct(lat, q):
+    return float(np.percentile(lat, q)) * 1e3 if len(lat) else None
+
+
+def _state_matches(srv, did, design):
+    """The server's state of a design equals a full pass over its updated
+    inputs (bit for bit)."""
+    import opentimer_b200 as otg
+    c = {k: v.copy() for k, v in design.items()}
+    ref = otg.rc_timing_host(c["nodes_start"], c["edges"], c["roots"], c["res"], c["cap"],
+                             c["sinks_start"], c["sink_nodes"], c["driver_slew"])
+    got = srv.read(did)
+    return all(np.array_equal(got[k], ref[k])
+               for k in ["node2bfs", "load", "delay", "ldelay", "impulse", "sink_slew"])
+
+
+def run_incremental():
+    """Batched incremental sizing loop: a 200k-gate design (RC trees 2..512
+    nodes), 1000 iterations each resizing a random 0.5% of the gates.  The
+    batched path applies an iteration as one request (one graph replay
+    re-times all its dirty nets); the plain path applies every gate resize
+    by itself (its own launches and a synchronization)."""
+    from opentimer_b200 import workloads
+    from opentimer_b200.serve import TimingServer, synth_design
+    ns = workloads.net_sizes(SEED + 3, INC_GATES, 2, 512)
+    design = synth_design(SEED + 3, ns)
+    gm = workloads.gate_map(SEED + 4, design)
+    k = int(round(INC_FRAC * INC_GATES))
+    zeros = np.zeros(INC_ITERS, np.int64)
+    tr = workloads.request_trace(SEED + 5, [gm], INC_ITERS, None, lo=k, hi=k,
+                                 design_of=zeros, arrival=zeros)
+    plain_tr = workloads.per_gate_trace(tr, [gm], num_req=INC_PLAIN_ITERS)
+    with TimingServer(slots=2, max_requests=4, max_updates=4 * k) as srv:
+        did, fp = srv.add_design(design)
+        warm_p = workloads.per_gate_trace(tr, [gm], num_req=2)
+        warm_b = workloads.request_trace(SEED + 6, [gm], 3, None, lo=k, hi=k,
+                                         design_of=zeros[:3], arrival=zeros[:3])
+        srv.replay(warm_p, plain=True)
+        srv.replay(warm_b)
+        lat_b, span_b = srv.replay(tr)
+        lat_p, span_p = srv.replay(plain_tr, plain=True)
+        # what the server holds now: the warm-ups, the batched iterations and
+        # the plain iterations, in that order
+        ok = True
+        if INC_CHECK:
+            check_design = {kk: v.copy() for kk, v in design.items()}
+            workloads.apply_trace(check_design, warm_p)
+            workloads.apply_trace(check_design, warm_b)
+            workloads.apply_trace(check_design, tr)
+            workloads.apply_trace(check_design, plain_tr)
+            ok = _state_matches(srv, did, check_design)
+    resizes_b = INC_ITERS * k
+    resizes_p = INC_PLAIN_ITERS * k
+    ups_b = resizes_b / span_b
+    ups_p = resizes_p / span_p
+    return {
+        "workload": f"{INC_GATES} gates/nets (RC 2..512 nodes, {int(ns[-1])} nodes), "
+                    f"{INC_ITERS} iterations x {k} gate resizes (0.5%)",
+        "batched": {"gate_resizes_per_s": ups_b, "ms_per_iteration": 1e3 * span_b / INC_ITERS,
+                    "path": "one request per iteration: graph replay (apply, fused RC pass "
+                            "over the dirty nets, results)"},
+        "plain": {"gate_resizes_per_s": ups_p, "ms_per_iteration": 1e3 * span_p / INC_PLAIN_ITERS,
+                  "iterations_timed": INC_PLAIN_ITERS,
+                  "path": "one otg_server_update_sync per gate resize (direct launches + sync)"},
+        "speedup": ups_b / ups_p,
+        "dirty_nets_per_iteration": float(2.5 * k),
+        "state_bit_exact_vs_full_pass": bool(ok),
+        "design_footprint_bytes": int(fp),
+    }
+
+
+def run_serving():
+    """Served incremental timing: 16 device-resident designs of 10k..2M pins
+    (small-design generator: RC trees 2..16 nodes), Poisson request streams,
+    each request resizing 1..64 random gates of one design.  Batched server
+    vs the plain per-request path on the same trace."""
+    from opentimer_b200 import workloads
+    from opentimer_b200.serve import TimingServer, synth_design
+    rng = np.random.default_rng(SEED + 7)
+    pins = np.exp(rng.uniform(np.log(SRV_PINS_LO), np.log(SRV_PINS_HI), SRV_DESIGNS))
+    gates = np.maximum((pins / 2.5).astype(np.int64), 1000)
+    designs, gmaps = [], []
+    for i, G in enumerate(gates):
+        d = synth_design(SEED + 100 + i, workloads.uniform_sizes(SEED + 100 + i, int(G), 2, 16))
+        designs.append(d)
+        gmaps.append(workloads.gate_map(SEED + 200 + i, d))
+    out = {"workload": f"{SRV_DESIGNS} designs, {int(pins.sum())} pins, {int(gates.sum())} "
+                       "nets (RC 2..16 nodes); requests resize 1..64 gates",
+           "rates": []}
+    with TimingServer(slots=SRV_SLOTS, max_requests=64, max_updates=1 << 14) as srv:
+        ids, fps = zip(*[srv.add_design(d) for d in designs])
+        id_of = np.array(ids, np.int32)
+        out["designs_footprint_bytes"] = int(sum(fps))
+        warm = workloads.request_trace(SEED + 8, gmaps, 500, 1e5)
+        warm["design"] = id_of[warm["design"]]
+        srv.replay(warm)
+        srv.replay(warm, plain=True)
+        for rate in SRV_RATES:
+            n = int(rate * SRV_SECONDS)
+            tr = workloads.request_trace(SEED + int(rate), gmaps, n, rate)
+            tr["design"] = id_of[tr["design"]]
+            gates_total = int(tr["gate_start"][-1])
+            lat_b, span_b = srv.replay(tr)
+            lat_p, span_p = srv.replay(tr, plain=True)
+            out["rates"].append({
+                "offered_req_per_s": rate, "requests": n,
+                "batched": {"p50_ms": _pct(lat_b, 50), "p99_ms": _pct(lat_b, 99),
+                            "req_per_s": n / span_b, "gate_resizes_per_s": gates_total / span_b},
+                "plain": {"p50_ms": _pct(lat_p, 50), "p99_ms": _pct(lat_p, 99),
+                          "req_per_s": n / span_p, "gate_resizes_per_s": gates_total / span_p}})
+        # saturation: every request queued at t=0
+        n = SRV_SAT_REQ
+        tr = workloads.request_trace(SEED + 9, gmaps, n, None, arrival=np.zeros(n, np.int64))
+        tr["design"] = id_of[tr["design"]]
+        gates_total = int(tr["gate_start"][-1])
+        _, span_b = srv.replay(tr)
+        _, span_p = srv.replay(tr, plain=True)
+        out["saturation"] = {"requests": n, "batched_gate_resizes_per_s": gates_total / span_b,
+                             "plain_gate_resizes_per_s": gates_total / span_p,
+                             "speedup": span_p / span_b}
+    return out
+
+
 def cpu_baseline(g, ns_np):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     threads = os.cpu_count() or 1
@@ -399,6 +535,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-levelize", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-incremental", action="store_true")
+    ap.add_argument("--no-serving", action="store_true")
     # smaller cases (profiling); the defaults are the benchmark workload
     ap.add_argument("--nets", type=int, default=NUM_NETS)
     ap.add_argument("--min-nodes", type=int, default=2)

@@ -100,6 +100,18 @@ otg_status otg_rc_workspace_size(int32_t num_nets, int32_t max_net_nodes, size_t
 otg_status otg_rc_timing(const otg_rc_forest* forest, int32_t max_net_nodes, void* workspace,
                          size_t workspace_bytes, otg_stream_t stream);
 
+/*
+ * otg_rc_timing_subset -- the same pass over only the nets listed in
+ * net_list[0 .. *num_listed) (device memory, at most max_listed entries):
+ * the incremental update of dirty nets.  The list and its length are read
+ * on the device, so a CUDA graph captured once serves every update.  The
+ * workspace is sized with otg_rc_workspace_size(max_listed, ...).
+ */
+otg_status otg_rc_timing_subset(const otg_rc_forest* forest, int32_t max_net_nodes,
+                                const int32_t* net_list, const int32_t* num_listed,
+                                int32_t max_listed, void* workspace, size_t workspace_bytes,
+                                otg_stream_t stream);
+
 /* Synchronizes `stream` and returns the first device-side error recorded in
  * `workspace` by the last otg_rc_timing call (OTG_OK if none); *bad_net (if
  * non-NULL) gets the offending net index or -1. */
@@ -165,6 +177,81 @@ void otg_release_host_context(void);
  */
 otg_status otg_rc_timing_noalloc(const otg_rc_forest* forest, int32_t max_net_nodes,
                                  otg_stream_t stream);
+
+/*
+ * ---- Device-resident designs and the incremental timing server ----------
+ * (no counterpart in the reference, whose Timer recomputes dirty nets on the
+ * CPU and whose GPU path is valid only for a first full update).
+ *
+ * A server owns designs whose RC state stays on the device.  A request is
+ * an incremental change to one design -- node capacitance updates (a gate
+ * resize changes the pin caps of its inputs) and driver-slew updates (its
+ * drive strength) -- whose dirty nets are re-timed.  The dispatcher thread
+ * batches the pending requests of all idle designs (continuous batching:
+ * requests that arrive while batches run are taken as soon as a slot and
+ * their design are free), applies the updates, re-times every dirty net of
+ * the batch in one fused pass over all designs, and reduces per request the
+ * worst |sink slew| and worst sink delay over its dirty nets.  Each slot
+ * replays a CUDA graph captured once; request data reach the device through
+ * pinned, mapped host buffers.  Designs are admitted against a device-memory
+ * budget (OTG_ERR_ADMISSION when one does not fit).
+ */
+typedef struct otg_server otg_server;
+
+typedef struct otg_result {
+  float worst_slew[4];   /* max |sink slew| over the request's dirty nets, per corner */
+  float worst_delay[4];  /* max sink Elmore delay over the same nets, per corner       */
+  int32_t status;        /* OTG_OK or the first device-side error of its design       */
+  int32_t dirty_nets;    /* distinct nets the request dirtied                         */
+  int64_t t_submit_ns;   /* steady-clock times of submission and completion           */
+  int64_t t_done_ns;
+} otg_result;
+
+/* budget_bytes: device memory designs may hold (0 = no limit); slots:
+ * batches in flight (>= 1); max_requests / max_updates: capacity of one
+ * batch (requests, and cap + slew updates). */
+otg_status otg_server_create(size_t budget_bytes, int32_t slots, int32_t max_requests,
+                             int32_t max_updates, otg_server** out);
+void otg_server_destroy(otg_server* s);
+/* Uploads a design (host arrays of an otg_rc_forest with sinks), times it
+ * fully once, and returns its id; OTG_ERR_ADMISSION if it does not fit. */
+otg_status otg_server_add_design(otg_server* s, const otg_rc_forest* host_forest,
+                                 int32_t* design_id, size_t* footprint_bytes);
+otg_status otg_server_remove_design(otg_server* s, int32_t design_id);
+/* Queues one request; cap_val is [num_cap][4], slew_val [num_slew][4]. */
+otg_status otg_server_submit(otg_server* s, int32_t design_id, int32_t num_cap,
+                             const int32_t* cap_net, const int32_t* cap_node, const float* cap_val,
+                             int32_t num_slew, const int32_t* slew_net, const float* slew_val,
+                             int64_t* ticket);
+/* Blocks until `ticket` completes (timeout_ms < 0: no limit) and returns
+ * its result; OTG_ERR_TIMEOUT if the limit passed first. */
+otg_status otg_server_wait(otg_server* s, int64_t ticket, int32_t timeout_ms, otg_result* out);
+/* The same request without batching: applied and timed by itself, one set
+ * of launches and a stream synchronization per request (the per-update
+ * path the batched server is measured against).  Blocking. */
+otg_status otg_server_update_sync(otg_server* s, int32_t design_id, int32_t num_cap,
+                                  const int32_t* cap_net, const int32_t* cap_node,
+                                  const float* cap_val, int32_t num_slew, const int32_t* slew_net,
+                                  const float* slew_val, otg_result* out);
+/* Open-loop replay of a request trace (the load generator of the serving
+ * measurement).  Request r goes to design[r] at t0 + arrival_ns[r] (t0 =
+ * the call's start) with the cap updates [cap_start[r], cap_start[r+1])
+ * and slew updates [slew_start[r], slew_start[r+1]) of the update arrays.
+ * plain == 0: submitted to the batching server by a submitter thread;
+ * plain != 0: applied with otg_server_update_sync, one request at a time in
+ * arrival order (the per-update path).  latency_ns[r] = completion minus
+ * scheduled arrival (queueing included); *makespan_ns = last completion
+ * minus t0.  Blocks until every request is done. */
+otg_status otg_server_replay(otg_server* s, int32_t num_req, const int64_t* arrival_ns,
+                             const int32_t* design, const int32_t* cap_start,
+                             const int32_t* cap_net, const int32_t* cap_node,
+                             const float* cap_val, const int32_t* slew_start,
+                             const int32_t* slew_net, const float* slew_val, int32_t plain,
+                             int64_t* latency_ns, int64_t* makespan_ns);
+/* Copies a design's per-node outputs (BFS order, as otg_rc_forest) and
+ * sink slews back to host arrays (any may be NULL). */
+otg_status otg_server_read(otg_server* s, int32_t design_id, int32_t* node2bfs, float* load,
+                           float* delay, float* ldelay, float* impulse, float* sink_slew);
 
 /* Human-readable name of a status code. */
 const char* otg_status_string(otg_status s);

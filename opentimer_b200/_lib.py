@@ -23,7 +23,10 @@ C_SYMBOLS = [
     "otg_rc_timing_host", "otg_levelize_host", "otg_release_host_context",
     "otg_status_string", "otg_kernel_launches",
     "otg_synth_rc_forest", "otg_synth_rc_sinks", "otg_synth_rc_forest_host",
-    "otg_rc_timing_noalloc",
+    "otg_rc_timing_noalloc", "otg_rc_timing_subset",
+    "otg_server_create", "otg_server_destroy", "otg_server_add_design",
+    "otg_server_remove_design", "otg_server_submit", "otg_server_wait",
+    "otg_server_update_sync", "otg_server_read", "otg_server_replay",
 ]
 # The reference-compatible C++ entry points (include/otg_compat.hpp), by
 # their Itanium-mangled names.
@@ -53,6 +56,15 @@ class RcForest(ctypes.Structure):
     ]
 
 
+class RcResult(ctypes.Structure):
+    """otg_result: one incremental request's summary."""
+    _fields_ = [
+        ("worst_slew", ctypes.c_float * 4), ("worst_delay", ctypes.c_float * 4),
+        ("status", ctypes.c_int32), ("dirty_nets", ctypes.c_int32),
+        ("t_submit_ns", ctypes.c_int64), ("t_done_ns", ctypes.c_int64),
+    ]
+
+
 _lib = None
 
 
@@ -69,6 +81,7 @@ def lib():
         L.otg_rc_workspace_size.argtypes = [I32, I32, PS]
         L.otg_rc_timing.argtypes = [ctypes.POINTER(RcForest), I32, P, S, P]
         L.otg_rc_status.argtypes = [P, P, ctypes.POINTER(I32)]
+        L.otg_rc_timing_subset.argtypes = [ctypes.POINTER(RcForest), I32, P, P, I32, P, S, P]
         L.otg_levelize_workspace_size.argtypes = [I32, I32, PS]
         L.otg_levelize.argtypes = [I32, I32, P, P, P, P, I32, P, P, P, P, P, S, P]
         L.otg_levelize_status.argtypes = [P, P]
@@ -83,10 +96,26 @@ def lib():
         L.otg_synth_rc_forest.argtypes = [U64, I32, P, P, P, P, P, P, P, P, P]
         L.otg_synth_rc_sinks.argtypes = [I32, P, P, P, P, P, P, P]
         L.otg_synth_rc_forest_host.argtypes = [U64, I32, P, P, P, P, P, P, P]
-        for name in ["otg_rc_workspace_size", "otg_rc_timing", "otg_rc_status",
+        L.otg_rc_timing_noalloc.argtypes = [ctypes.POINTER(RcForest), I32, P]
+        I64 = ctypes.c_int64
+        PR = ctypes.POINTER(RcResult)
+        L.otg_server_create.argtypes = [S, I32, I32, I32, ctypes.POINTER(P)]
+        L.otg_server_destroy.argtypes = [P]
+        L.otg_server_destroy.restype = None
+        L.otg_server_add_design.argtypes = [P, ctypes.POINTER(RcForest), ctypes.POINTER(I32), PS]
+        L.otg_server_remove_design.argtypes = [P, I32]
+        L.otg_server_submit.argtypes = [P, I32, I32, P, P, P, I32, P, P, ctypes.POINTER(I64)]
+        L.otg_server_wait.argtypes = [P, I64, I32, PR]
+        L.otg_server_update_sync.argtypes = [P, I32, I32, P, P, P, I32, P, P, PR]
+        L.otg_server_read.argtypes = [P, I32, P, P, P, P, P, P]
+        L.otg_server_replay.argtypes = [P, I32, P, P, P, P, P, P, P, P, P, I32, P, P]
+        for name in ["otg_rc_workspace_size", "otg_rc_timing", "otg_rc_status", "otg_rc_timing_subset",
                      "otg_levelize_workspace_size", "otg_levelize", "otg_levelize_status",
                      "otg_rc_timing_host", "otg_levelize_host", "otg_synth_rc_forest",
-                     "otg_synth_rc_sinks", "otg_synth_rc_forest_host"]:
+                     "otg_synth_rc_sinks", "otg_synth_rc_forest_host", "otg_rc_timing_noalloc",
+                     "otg_server_create", "otg_server_add_design", "otg_server_remove_design",
+                     "otg_server_submit", "otg_server_wait", "otg_server_update_sync",
+                     "otg_server_read", "otg_server_replay"]:
             getattr(L, name).restype = ctypes.c_int
         _lib = L
     return _lib

@@ -13,7 +13,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libotg.so")
-SOURCES = ["otg_rc.cu", "otg_levelize.cu", "otg_synth.cu", "otg_host.cu", "otg_noalloc.cu"]
+SOURCES = ["otg_rc.cu", "otg_levelize.cu", "otg_synth.cu", "otg_host.cu", "otg_noalloc.cu",
+           "otg_serve.cu"]
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -112,4 +112,15 @@ struct RcClasses {
 // public otg_rc_timing wraps it.
 otg_status rc_launch(const otg_rc_forest* f, int max_net_nodes, void* workspace,
                      size_t workspace_bytes, cudaStream_t stream);
+
+// Multi-forest form (used by the design server): `forests` is a device
+// array of per-forest kernel arguments (rc_args_bytes() each, filled on the
+// host with rc_args_fill and copied up), `items` a device list of
+// (forest, net) pairs whose length is read from *num_dev (at most cap).
+struct RcArgsOpaque;
+otg_status rc_launch_items(const RcArgsOpaque* forests, const int2* items, const int* num_dev,
+                           int cap, int max_net_nodes, void* workspace, size_t workspace_bytes,
+                           cudaStream_t stream);
+size_t rc_args_bytes();
+void rc_args_fill(const otg_rc_forest* f, int* status, void* out);
 }  // namespace otg

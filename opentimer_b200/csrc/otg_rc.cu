@@ -39,9 +39,7 @@ namespace otg {
 
 namespace {
 
-constexpr int NC = 4;
 constexpr unsigned FULL = 0xffffffffu;
-constexpr int END = -1;
 
 // ------------------------------------------------------------------ args
 
@@ -69,24 +67,37 @@ __device__ __forceinline__ void report(const RcArgs& a, int code, int net) {
   if (atomicCAS(a.status, 0, code) == 0) a.status[1] = net;
 }
 
-// ------------------------------------------------------- float-float math
-// Knuth TwoSum; x += y on (hi, lo) pairs.  No multiplies, so FMA
-// contraction cannot change these.
-__device__ __forceinline__ void ffadd(float& ah, float& al, float bh, float bl) {
-  float s = ah + bh;
-  float bb = s - ah;
-  float e = (ah - (s - bb)) + (bh - bb);
-  e += al + bl;
-  ah = s + e;
-  al = e - (ah - s);
+// One launch's work: all nets of forest a0 (nets == items == null), a
+// device list of nets of a0 (nets), or a device list of (forest, net)
+// pairs over the device array `forests` (items).  The list lengths come
+// from device memory so one captured graph serves every batch.
+struct RcJob {
+  RcArgs a0;
+  const RcArgs* forests;
+  const int* nets;
+  const int2* items;
+  const int* num_dev;  // device count for nets/items
+  int num;             // count when neither list is given
+};
+
+__device__ __forceinline__ int job_count(const RcJob& j) {
+  return (j.nets || j.items) ? *j.num_dev : j.num;
+}
+__device__ __forceinline__ void job_item(const RcJob& j, int k, int& f, int& net) {
+  if (j.items) {
+    const int2 it = j.items[k];
+    f = it.x;
+    net = it.y;
+  } else {
+    f = 0;
+    net = j.nets ? j.nets[k] : k;
+  }
+}
+__device__ __forceinline__ const RcArgs& job_forest(const RcJob& j, int f) {
+  return j.items ? j.forests[f] : j.a0;
 }
 
-__device__ __forceinline__ float f4get(const float4& v, int j) {
-  return j == 0 ? v.x : j == 1 ? v.y : j == 2 ? v.z : v.w;
-}
-__device__ __forceinline__ void f4set(float4& v, int j, float x) {
-  if (j == 0) v.x = x; else if (j == 1) v.y = x; else if (j == 2) v.z = x; else v.w = x;
-}
+// ------------------------------------------------------------ float4 math
 __device__ __forceinline__ float4 f4add(float4 a, float4 b) {
   return make_float4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w);
 }
@@ -253,7 +264,7 @@ __device__ void rc_net_warp(const RcArgs& a, int net, int* s_par, int* s_pe) {
   }
 }
 
-__global__ void __launch_bounds__(256) rc_warp_kernel(RcArgs a, const int* list,
+__global__ void __launch_bounds__(256) rc_warp_kernel(RcJob job, const int* list,
                                                        const int* count, int* work) {
   __shared__ int s_par[8][32];
   __shared__ int s_pe[8][32];
@@ -265,7 +276,9 @@ __global__ void __launch_bounds__(256) rc_warp_kernel(RcArgs a, const int* list,
     if (lane == 0) item = atomicAdd(work, 1);
     item = __shfl_sync(FULL, item, 0);
     if (item >= cnt) break;
-    rc_net_warp(a, list[item], s_par[w], s_pe[w]);
+    int f, net;
+    job_item(job, list[item], f, net);
+    rc_net_warp(job_forest(job, f), net, s_par[w], s_pe[w]);
     __syncwarp();
   }
 }
@@ -969,35 +982,49 @@ __device__ void rc_net_block(const RcArgs& a, int net, char* ws, int n, int* sh,
 }
 
 template <int T, int K, class Ix, bool SMEM>
-__global__ void __launch_bounds__(T) rc_block_kernel(RcArgs a, const int* list, const int* count,
+__global__ void __launch_bounds__(T) rc_block_kernel(RcJob job, const int* list, const int* count,
                                                      int* work, char* gws, size_t ws_stride) {
   extern __shared__ __align__(16) char dsm[];
   __shared__ int sh[64];
   __shared__ long long shl[4 * (T / 32) + 4];
-  __shared__ int s_item;
+  __shared__ int s_item[2];
+  __shared__ RcArgs s_args;  // the current net's forest
   char* ws = SMEM ? dsm : gws + (size_t)blockIdx.x * ws_stride;
   const int cnt = *count;
   while (true) {
-    if (threadIdx.x == 0) s_item = atomicAdd(work, 1);
+    if (threadIdx.x == 0) {
+      const int item = atomicAdd(work, 1);
+      s_item[0] = item;
+      if (item < cnt) {
+        int f, net;
+        job_item(job, list[item], f, net);
+        s_item[1] = net;
+        s_args = job_forest(job, f);
+      }
+    }
     __syncthreads();
-    const int item = s_item;
+    const int item = s_item[0], net = s_item[1];
     __syncthreads();
     if (item >= cnt) break;
-    const int net = list[item];
-    const int n = a.nodes_start[net + 1] - a.nodes_start[net];
-    rc_net_block<T, K, Ix>(a, net, ws, n, sh, shl);
+    const int n = s_args.nodes_start[net + 1] - s_args.nodes_start[net];
+    rc_net_block<T, K, Ix>(s_args, net, ws, n, sh, shl);
     __syncthreads();
   }
 }
 
 // ------------------------------------------------------------ bucketing
-__global__ void rc_classify_kernel(int num_nets, const int* nodes_start, int max_net_nodes,
-                                   RcClasses cls, int* lists, int* counts, int* status) {
+__global__ void rc_classify_kernel(RcJob job, int cap, int max_net_nodes, RcClasses cls,
+                                   int* lists, int* counts, int* status) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int lane = threadIdx.x & 31;
+  const int num = min(job_count(job), cap);
   int c = -1;
-  if (i < num_nets) {
-    const int n = nodes_start[i + 1] - nodes_start[i];
+  if (i < num) {
+    int f, net;
+    job_item(job, i, f, net);
+    const RcArgs& a = job_forest(job, f);
+    const int n = (unsigned)net < (unsigned)a.num_nets
+                      ? a.nodes_start[net + 1] - a.nodes_start[net] : 0;
     if (n < 1 || n > max_net_nodes) {
       if (atomicCAS(status, 0, n < 1 ? OTG_ERR_INVALID : OTG_ERR_TOO_LARGE) == 0) status[1] = i;
     } else {
@@ -1005,7 +1032,9 @@ __global__ void rc_classify_kernel(int num_nets, const int* nodes_start, int max
       while (c < cls.num - 1 && n > cls.nmax[c]) ++c;
     }
   }
-  // warp-aggregated append
+  if (i == 0 && job_count(job) > cap && atomicCAS(status, 0, OTG_ERR_WORKSPACE) == 0)
+    status[1] = -1;
+  // warp-aggregated append of the item index
   const unsigned active = __ballot_sync(FULL, c >= 0);
   const unsigned peers = __match_any_sync(FULL, c);
   if (c >= 0) {
@@ -1013,7 +1042,7 @@ __global__ void rc_classify_kernel(int num_nets, const int* nodes_start, int max
     int base = 0;
     if (lane == leader) base = atomicAdd(&counts[c], __popc(peers));
     base = __shfl_sync(peers, base, leader);
-    lists[(size_t)c * num_nets + base + __popc(peers & ((1u << lane) - 1u))] = i;
+    lists[(size_t)c * cap + base + __popc(peers & ((1u << lane) - 1u))] = i;
   }
 }
 
@@ -1106,45 +1135,24 @@ size_t rc_workspace_bytes(int num_nets, int max_net_nodes, int sms, int smem_bud
 namespace {
 
 template <int T, int K>
-cudaError_t launch_smem_class(const RcArgs& a, const int* list, int* count, int* work, int nmax,
+cudaError_t launch_smem_class(const RcJob& job, const int* list, int* count, int* work, int nmax,
                               int sms, cudaStream_t stream) {
   auto kern = rc_block_kernel<T, K, uint16_t, true>;
   const size_t smem = rc_layout(nmax, T, K, 2).total;
-  cudaError_t err =
-      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  // The attribute is always set to the same (largest) value, so threads
+  // launching with different nmax never lower it under one another.
+  cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         dev_info().smem_optin - kStaticSmemReserve);
   int occ = 1;
   if (err == cudaSuccess) err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, T, smem);
   if (err != cudaSuccess) return err;
   occ = std::max(occ, 1);
-  kern<<<sms * occ, T, smem, stream>>>(a, list, count, work, nullptr, 0);
+  kern<<<sms * occ, T, smem, stream>>>(job, list, count, work, nullptr, 0);
   count_launch();
   return cudaGetLastError();
 }
 
-}  // namespace
-
-otg_status rc_launch(const otg_rc_forest* f, int max_net_nodes, void* workspace,
-                     size_t workspace_bytes, cudaStream_t stream) {
-  if (!f || !workspace || f->num_nets < 0 || max_net_nodes < 1) return OTG_ERR_INVALID;
-  if (f->num_nets == 0) return OTG_OK;
-  if (!f->nodes_start || !f->edges || !f->roots || !f->edges_res || !f->nodes_cap ||
-      !f->node2bfs || !f->pid || !f->load || !f->delay || !f->ldelay || !f->impulse)
-    return OTG_ERR_INVALID;
-  const bool sinks = f->sinks_start != nullptr;
-  if (sinks && (!f->sink_nodes || !f->driver_slew || !f->sink_slew)) return OTG_ERR_INVALID;
-  DevInfo& di = dev_info();
-  const int budget = di.smem_optin - kStaticSmemReserve;
-  size_t off_lists, off_huge, stride;
-  const size_t need = rc_workspace_bytes(f->num_nets, max_net_nodes, di.sms, budget, &off_lists,
-                                         &off_huge, &stride);
-  if (workspace_bytes < need) return OTG_ERR_WORKSPACE;
-  char* ws = (char*)workspace;
-  int* status = (int*)ws;
-  int* counters = (int*)(ws + 64);  // [0..7] counts, [8..15] work
-  int* lists = (int*)(ws + off_lists);
-  const RcClasses cls = rc_classes(budget);
-
-  if (cudaMemsetAsync(ws, 0, 128, stream) != cudaSuccess) return OTG_ERR_CUDA;
+RcArgs make_args(const otg_rc_forest* f, int* status) {
   RcArgs a;
   a.num_nets = f->num_nets;
   a.nodes_start = f->nodes_start;
@@ -1158,23 +1166,58 @@ otg_status rc_launch(const otg_rc_forest* f, int max_net_nodes, void* workspace,
   a.delay = (float4*)f->delay;
   a.ldelay = (float4*)f->ldelay;
   a.impulse = (float4*)f->impulse;
-  a.sinks_start = sinks ? f->sinks_start : nullptr;
+  a.sinks_start = f->sinks_start;
   a.sink_nodes = f->sink_nodes;
   a.driver_slew = (const float4*)f->driver_slew;
   a.sink_slew = (float4*)f->sink_slew;
   a.status = status;
+  return a;
+}
 
-  rc_classify_kernel<<<(f->num_nets + 255) / 256, 256, 0, stream>>>(
-      f->num_nets, f->nodes_start, max_net_nodes, cls, lists, counters, status);
+bool forest_ok(const otg_rc_forest* f) {
+  if (!f || f->num_nets < 0) return false;
+  if (f->num_nets == 0) return true;
+  if (!f->nodes_start || !f->edges || !f->roots || !f->edges_res || !f->nodes_cap ||
+      !f->node2bfs || !f->pid || !f->load || !f->delay || !f->ldelay || !f->impulse)
+    return false;
+  if (f->sinks_start && (!f->sink_nodes || !f->driver_slew || !f->sink_slew)) return false;
+  return true;
+}
+
+}  // namespace
+
+// Launches the fused pass over the items of `job` (at most `cap` of them).
+// The workspace starts with [status 64 B][counters 64 B]; its status word is
+// where a.status should point for single-forest jobs.
+otg_status rc_launch_job(RcJob job, int cap, int max_net_nodes, void* workspace,
+                         size_t workspace_bytes, cudaStream_t stream) {
+  if (!workspace || cap < 0 || max_net_nodes < 1) return OTG_ERR_INVALID;
+  DevInfo& di = dev_info();
+  const int budget = di.smem_optin - kStaticSmemReserve;
+  size_t off_lists, off_huge, stride;
+  const size_t need = rc_workspace_bytes(std::max(cap, 1), max_net_nodes, di.sms, budget,
+                                         &off_lists, &off_huge, &stride);
+  if (workspace_bytes < need) return OTG_ERR_WORKSPACE;
+  char* ws = (char*)workspace;
+  int* status = (int*)ws;
+  int* counters = (int*)(ws + 64);  // [0..7] counts, [8..15] work
+  int* lists = (int*)(ws + off_lists);
+  const RcClasses cls = rc_classes(budget);
+  if (cudaMemsetAsync(ws, 0, 128, stream) != cudaSuccess) {
+    cudaGetLastError();
+    return OTG_ERR_CUDA;
+  }
+  if (cap == 0) return OTG_OK;
+  rc_classify_kernel<<<(cap + 255) / 256, 256, 0, stream>>>(job, cap, max_net_nodes, cls, lists,
+                                                            counters, status);
   count_launch();
-  const int N = f->num_nets;
-  auto L = [&](int c) { return lists + (size_t)c * N; };
+  auto L = [&](int c) { return lists + (size_t)c * cap; };
   int* work = counters + 8;
-  cudaError_t err = cudaSuccess;
+  cudaError_t err = cudaGetLastError();
   // Largest nets first so the long tail overlaps the small ones.
-  if (max_net_nodes > cls.nmax[6]) {
+  if (err == cudaSuccess && max_net_nodes > cls.nmax[6]) {
     rc_block_kernel<512, 8, int, false><<<huge_ctas(di.sms, stride), 512, 0, stream>>>(
-        a, L(7), counters + 7, work + 7, ws + off_huge, stride);
+        job, L(7), counters + 7, work + 7, ws + off_huge, stride);
     count_launch();
     err = cudaGetLastError();
   }
@@ -1182,16 +1225,16 @@ otg_status rc_launch(const otg_rc_forest* f, int max_net_nodes, void* workspace,
     if (max_net_nodes <= cls.nmax[c - 1]) continue;
     const int nmax = std::min(cls.nmax[c], max_net_nodes);
     switch (c) {
-      case 1: err = launch_smem_class<64, 4>(a, L(c), counters + c, work + c, nmax, di.sms, stream); break;
-      case 2: err = launch_smem_class<64, 8>(a, L(c), counters + c, work + c, nmax, di.sms, stream); break;
-      case 3: err = launch_smem_class<128, 8>(a, L(c), counters + c, work + c, nmax, di.sms, stream); break;
-      case 4: err = launch_smem_class<256, 4>(a, L(c), counters + c, work + c, nmax, di.sms, stream); break;
-      case 5: err = launch_smem_class<256, 8>(a, L(c), counters + c, work + c, nmax, di.sms, stream); break;
-      default: err = launch_smem_class<512, 8>(a, L(c), counters + c, work + c, nmax, di.sms, stream); break;
+      case 1: err = launch_smem_class<64, 4>(job, L(c), counters + c, work + c, nmax, di.sms, stream); break;
+      case 2: err = launch_smem_class<64, 8>(job, L(c), counters + c, work + c, nmax, di.sms, stream); break;
+      case 3: err = launch_smem_class<128, 8>(job, L(c), counters + c, work + c, nmax, di.sms, stream); break;
+      case 4: err = launch_smem_class<256, 4>(job, L(c), counters + c, work + c, nmax, di.sms, stream); break;
+      case 5: err = launch_smem_class<256, 8>(job, L(c), counters + c, work + c, nmax, di.sms, stream); break;
+      default: err = launch_smem_class<512, 8>(job, L(c), counters + c, work + c, nmax, di.sms, stream); break;
     }
   }
   if (err == cudaSuccess) {
-    rc_warp_kernel<<<di.sms * 8, 256, 0, stream>>>(a, L(0), counters + 0, work + 0);
+    rc_warp_kernel<<<di.sms * 8, 256, 0, stream>>>(job, L(0), counters + 0, work + 0);
     count_launch();
     err = cudaGetLastError();
   }
@@ -1200,6 +1243,46 @@ otg_status rc_launch(const otg_rc_forest* f, int max_net_nodes, void* workspace,
     return OTG_ERR_CUDA;
   }
   return OTG_OK;
+}
+
+otg_status rc_launch(const otg_rc_forest* f, int max_net_nodes, void* workspace,
+                     size_t workspace_bytes, cudaStream_t stream) {
+  if (!forest_ok(f) || !workspace || max_net_nodes < 1) return OTG_ERR_INVALID;
+  if (f->num_nets == 0) return OTG_OK;
+  RcJob job{};
+  job.a0 = make_args(f, (int*)workspace);
+  job.num = f->num_nets;
+  return rc_launch_job(job, f->num_nets, max_net_nodes, workspace, workspace_bytes, stream);
+}
+
+otg_status rc_launch_subset(const otg_rc_forest* f, int max_net_nodes, const int* nets,
+                            const int* num_dev, int cap, void* workspace, size_t workspace_bytes,
+                            cudaStream_t stream) {
+  if (!forest_ok(f) || !workspace || !nets || !num_dev || cap < 0 || max_net_nodes < 1)
+    return OTG_ERR_INVALID;
+  RcJob job{};
+  job.a0 = make_args(f, (int*)workspace);
+  job.nets = nets;
+  job.num_dev = num_dev;
+  return rc_launch_job(job, cap, max_net_nodes, workspace, workspace_bytes, stream);
+}
+
+otg_status rc_launch_items(const RcArgsOpaque* forests, const int2* items, const int* num_dev,
+                           int cap, int max_net_nodes, void* workspace, size_t workspace_bytes,
+                           cudaStream_t stream) {
+  if (!forests || !items || !num_dev || cap < 0) return OTG_ERR_INVALID;
+  RcJob job{};
+  job.forests = (const RcArgs*)forests;
+  job.items = items;
+  job.num_dev = num_dev;
+  return rc_launch_job(job, cap, max_net_nodes, workspace, workspace_bytes, stream);
+}
+
+size_t rc_args_bytes() { return sizeof(RcArgs); }
+
+void rc_args_fill(const otg_rc_forest* f, int* status, void* out) {
+  const RcArgs a = make_args(f, status);
+  std::memcpy(out, &a, sizeof(a));
 }
 
 }  // namespace otg
@@ -1233,6 +1316,14 @@ int otg_debug_phase_cycles(unsigned long long* out, int n) {
   return n;
 }
 #endif
+
+otg_status otg_rc_timing_subset(const otg_rc_forest* forest, int32_t max_net_nodes,
+                                const int32_t* net_list, const int32_t* num_listed,
+                                int32_t max_listed, void* workspace, size_t workspace_bytes,
+                                otg_stream_t stream) {
+  return otg::rc_launch_subset(forest, max_net_nodes, net_list, num_listed, max_listed, workspace,
+                               workspace_bytes, (cudaStream_t)stream);
+}
 
 otg_status otg_rc_status(const void* workspace, otg_stream_t stream, int32_t* bad_net) {
   if (!workspace) return OTG_ERR_INVALID;
