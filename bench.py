@@ -494,12 +494,15 @@ def run_serving():
             tr = workloads.request_trace(SEED + int(rate), gmaps, n, rate)
             tr["design"] = id_of[tr["design"]]
             gates_total = int(tr["gate_start"][-1])
+            b0, r0 = srv.stats()
             lat_b, span_b = srv.replay(tr)
+            b1, r1 = srv.stats()
             lat_p, span_p = srv.replay(tr, plain=True)
             out["rates"].append({
                 "offered_req_per_s": rate, "requests": n,
                 "batched": {"p50_ms": _pct(lat_b, 50), "p99_ms": _pct(lat_b, 99),
-                            "req_per_s": n / span_b, "gate_resizes_per_s": gates_total / span_b},
+                            "req_per_s": n / span_b, "gate_resizes_per_s": gates_total / span_b,
+                            "requests_per_batch": (r1 - r0) / max(b1 - b0, 1)},
                 "plain": {"p50_ms": _pct(lat_p, 50), "p99_ms": _pct(lat_p, 99),
                           "req_per_s": n / span_p, "gate_resizes_per_s": gates_total / span_p}})
         # saturation: every request queued at t=0
@@ -507,9 +510,12 @@ def run_serving():
         tr = workloads.request_trace(SEED + 9, gmaps, n, None, arrival=np.zeros(n, np.int64))
         tr["design"] = id_of[tr["design"]]
         gates_total = int(tr["gate_start"][-1])
+        b0, r0 = srv.stats()
         _, span_b = srv.replay(tr)
+        b1, r1 = srv.stats()
         _, span_p = srv.replay(tr, plain=True)
         out["saturation"] = {"requests": n, "batched_gate_resizes_per_s": gates_total / span_b,
+                             "requests_per_batch": (r1 - r0) / max(b1 - b0, 1),
                              "plain_gate_resizes_per_s": gates_total / span_p,
                              "speedup": span_p / span_b}
     return out

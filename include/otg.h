@@ -218,7 +218,9 @@ void otg_server_destroy(otg_server* s);
 otg_status otg_server_add_design(otg_server* s, const otg_rc_forest* host_forest,
                                  int32_t* design_id, size_t* footprint_bytes);
 otg_status otg_server_remove_design(otg_server* s, int32_t design_id);
-/* Queues one request; cap_val is [num_cap][4], slew_val [num_slew][4]. */
+/* Queues one request; cap_val is [num_cap][4], slew_val [num_slew][4].
+ * OTG_ERR_INVALID (nothing queued) for an unknown design, a net or node
+ * outside it, or more updates than a batch holds. */
 otg_status otg_server_submit(otg_server* s, int32_t design_id, int32_t num_cap,
                              const int32_t* cap_net, const int32_t* cap_node, const float* cap_val,
                              int32_t num_slew, const int32_t* slew_net, const float* slew_val,
@@ -248,6 +250,8 @@ otg_status otg_server_replay(otg_server* s, int32_t num_req, const int64_t* arri
                              const float* cap_val, const int32_t* slew_start,
                              const int32_t* slew_net, const float* slew_val, int32_t plain,
                              int64_t* latency_ns, int64_t* makespan_ns);
+/* Batches launched by the dispatcher and the requests they carried. */
+otg_status otg_server_stats(otg_server* s, int64_t* batches, int64_t* requests);
 /* Copies a design's per-node outputs (BFS order, as otg_rc_forest) and
  * sink slews back to host arrays (any may be NULL). */
 otg_status otg_server_read(otg_server* s, int32_t design_id, int32_t* node2bfs, float* load,

@@ -26,7 +26,7 @@ C_SYMBOLS = [
     "otg_rc_timing_noalloc", "otg_rc_timing_subset",
     "otg_server_create", "otg_server_destroy", "otg_server_add_design",
     "otg_server_remove_design", "otg_server_submit", "otg_server_wait",
-    "otg_server_update_sync", "otg_server_read", "otg_server_replay",
+    "otg_server_update_sync", "otg_server_read", "otg_server_replay", "otg_server_stats",
 ]
 # The reference-compatible C++ entry points (include/otg_compat.hpp), by
 # their Itanium-mangled names.
@@ -109,13 +109,14 @@ def lib():
         L.otg_server_update_sync.argtypes = [P, I32, I32, P, P, P, I32, P, P, PR]
         L.otg_server_read.argtypes = [P, I32, P, P, P, P, P, P]
         L.otg_server_replay.argtypes = [P, I32, P, P, P, P, P, P, P, P, P, I32, P, P]
+        L.otg_server_stats.argtypes = [P, P, P]
         for name in ["otg_rc_workspace_size", "otg_rc_timing", "otg_rc_status", "otg_rc_timing_subset",
                      "otg_levelize_workspace_size", "otg_levelize", "otg_levelize_status",
                      "otg_rc_timing_host", "otg_levelize_host", "otg_synth_rc_forest",
                      "otg_synth_rc_sinks", "otg_synth_rc_forest_host", "otg_rc_timing_noalloc",
                      "otg_server_create", "otg_server_add_design", "otg_server_remove_design",
                      "otg_server_submit", "otg_server_wait", "otg_server_update_sync",
-                     "otg_server_read", "otg_server_replay"]:
+                     "otg_server_read", "otg_server_replay", "otg_server_stats"]:
             getattr(L, name).restype = ctypes.c_int
         _lib = L
     return _lib

@@ -117,10 +117,22 @@ otg_status rc_launch(const otg_rc_forest* f, int max_net_nodes, void* workspace,
 // array of per-forest kernel arguments (rc_args_bytes() each, filled on the
 // host with rc_args_fill and copied up), `items` a device list of
 // (forest, net) pairs whose length is read from *num_dev (at most cap).
+// `fork` (optional): side streams the size-class launches are spread
+// over, joined back into `stream` before the call returns (also under
+// stream capture, where they become parallel graph branches).
+struct RcFork {
+  static constexpr int kMax = 4;
+  int n = 0;
+  cudaStream_t side[kMax] = {};
+  cudaEvent_t fork = nullptr;
+  cudaEvent_t join[kMax] = {};
+};
+cudaError_t rc_fork_create(RcFork* f, int n);
+void rc_fork_destroy(RcFork* f);
 struct RcArgsOpaque;
 otg_status rc_launch_items(const RcArgsOpaque* forests, const int2* items, const int* num_dev,
                            int cap, int max_net_nodes, void* workspace, size_t workspace_bytes,
-                           cudaStream_t stream);
+                           cudaStream_t stream, const RcFork* fork = nullptr);
 size_t rc_args_bytes();
 void rc_args_fill(const otg_rc_forest* f, int* status, void* out);
 }  // namespace otg

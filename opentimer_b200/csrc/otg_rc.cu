@@ -1190,7 +1190,7 @@ bool forest_ok(const otg_rc_forest* f) {
 // The workspace starts with [status 64 B][counters 64 B]; its status word is
 // where a.status should point for single-forest jobs.
 otg_status rc_launch_job(RcJob job, int cap, int max_net_nodes, void* workspace,
-                         size_t workspace_bytes, cudaStream_t stream) {
+                         size_t workspace_bytes, cudaStream_t stream, const RcFork* fork = nullptr) {
   if (!workspace || cap < 0 || max_net_nodes < 1) return OTG_ERR_INVALID;
   DevInfo& di = dev_info();
   const int budget = di.smem_optin - kStaticSmemReserve;
@@ -1214,9 +1214,23 @@ otg_status rc_launch_job(RcJob job, int cap, int max_net_nodes, void* workspace,
   auto L = [&](int c) { return lists + (size_t)c * cap; };
   int* work = counters + 8;
   cudaError_t err = cudaGetLastError();
+  // With a fork, the class launches go round-robin over the caller's
+  // stream and the side streams (joined back below), so the classes run
+  // side by side instead of one after another.
+  const int nside = fork ? std::min(fork->n, RcFork::kMax) : 0;
+  int nth = 0;
+  auto next_stream = [&]() -> cudaStream_t {
+    const int k = nth++ % (nside + 1);
+    return k == 0 ? stream : fork->side[k - 1];
+  };
+  if (nside > 0 && err == cudaSuccess) {
+    err = cudaEventRecord(fork->fork, stream);
+    for (int i = 0; i < nside && err == cudaSuccess; ++i)
+      err = cudaStreamWaitEvent(fork->side[i], fork->fork, 0);
+  }
   // Largest nets first so the long tail overlaps the small ones.
   if (err == cudaSuccess && max_net_nodes > cls.nmax[6]) {
-    rc_block_kernel<512, 8, int, false><<<huge_ctas(di.sms, stride), 512, 0, stream>>>(
+    rc_block_kernel<512, 8, int, false><<<huge_ctas(di.sms, stride), 512, 0, next_stream()>>>(
         job, L(7), counters + 7, work + 7, ws + off_huge, stride);
     count_launch();
     err = cudaGetLastError();
@@ -1224,19 +1238,26 @@ otg_status rc_launch_job(RcJob job, int cap, int max_net_nodes, void* workspace,
   for (int c = 6; c >= 1 && err == cudaSuccess; --c) {
     if (max_net_nodes <= cls.nmax[c - 1]) continue;
     const int nmax = std::min(cls.nmax[c], max_net_nodes);
+    cudaStream_t st = next_stream();
     switch (c) {
-      case 1: err = launch_smem_class<64, 4>(job, L(c), counters + c, work + c, nmax, di.sms, stream); break;
-      case 2: err = launch_smem_class<64, 8>(job, L(c), counters + c, work + c, nmax, di.sms, stream); break;
-      case 3: err = launch_smem_class<128, 8>(job, L(c), counters + c, work + c, nmax, di.sms, stream); break;
-      case 4: err = launch_smem_class<256, 4>(job, L(c), counters + c, work + c, nmax, di.sms, stream); break;
-      case 5: err = launch_smem_class<256, 8>(job, L(c), counters + c, work + c, nmax, di.sms, stream); break;
-      default: err = launch_smem_class<512, 8>(job, L(c), counters + c, work + c, nmax, di.sms, stream); break;
+      case 1: err = launch_smem_class<64, 4>(job, L(c), counters + c, work + c, nmax, di.sms, st); break;
+      case 2: err = launch_smem_class<64, 8>(job, L(c), counters + c, work + c, nmax, di.sms, st); break;
+      case 3: err = launch_smem_class<128, 8>(job, L(c), counters + c, work + c, nmax, di.sms, st); break;
+      case 4: err = launch_smem_class<256, 4>(job, L(c), counters + c, work + c, nmax, di.sms, st); break;
+      case 5: err = launch_smem_class<256, 8>(job, L(c), counters + c, work + c, nmax, di.sms, st); break;
+      default: err = launch_smem_class<512, 8>(job, L(c), counters + c, work + c, nmax, di.sms, st); break;
     }
   }
   if (err == cudaSuccess) {
-    rc_warp_kernel<<<di.sms * 8, 256, 0, stream>>>(job, L(0), counters + 0, work + 0);
+    rc_warp_kernel<<<di.sms * 8, 256, 0, next_stream()>>>(job, L(0), counters + 0, work + 0);
     count_launch();
     err = cudaGetLastError();
+  }
+  // join (also after a failed launch, so a capture is never left unjoined)
+  for (int i = 0; i < nside; ++i) {
+    cudaError_t e = cudaEventRecord(fork->join[i], fork->side[i]);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(stream, fork->join[i], 0);
+    if (err == cudaSuccess) err = e;
   }
   if (err != cudaSuccess) {
     cudaGetLastError();  // do not leave the error for the caller's next call
@@ -1269,16 +1290,36 @@ otg_status rc_launch_subset(const otg_rc_forest* f, int max_net_nodes, const int
 
 otg_status rc_launch_items(const RcArgsOpaque* forests, const int2* items, const int* num_dev,
                            int cap, int max_net_nodes, void* workspace, size_t workspace_bytes,
-                           cudaStream_t stream) {
+                           cudaStream_t stream, const RcFork* fork) {
   if (!forests || !items || !num_dev || cap < 0) return OTG_ERR_INVALID;
   RcJob job{};
   job.forests = (const RcArgs*)forests;
   job.items = items;
   job.num_dev = num_dev;
-  return rc_launch_job(job, cap, max_net_nodes, workspace, workspace_bytes, stream);
+  return rc_launch_job(job, cap, max_net_nodes, workspace, workspace_bytes, stream, fork);
 }
 
 size_t rc_args_bytes() { return sizeof(RcArgs); }
+
+cudaError_t rc_fork_create(RcFork* f, int n) {
+  *f = RcFork{};
+  f->n = std::min(std::max(n, 0), (int)RcFork::kMax);
+  cudaError_t e = cudaEventCreateWithFlags(&f->fork, cudaEventDisableTiming);
+  for (int i = 0; i < f->n && e == cudaSuccess; ++i) {
+    e = cudaStreamCreateWithFlags(&f->side[i], cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&f->join[i], cudaEventDisableTiming);
+  }
+  return e;
+}
+
+void rc_fork_destroy(RcFork* f) {
+  for (int i = 0; i < RcFork::kMax; ++i) {
+    if (f->side[i]) cudaStreamDestroy(f->side[i]);
+    if (f->join[i]) cudaEventDestroy(f->join[i]);
+  }
+  if (f->fork) cudaEventDestroy(f->fork);
+  *f = RcFork{};
+}
 
 void rc_args_fill(const otg_rc_forest* f, int* status, void* out) {
   const RcArgs a = make_args(f, status);

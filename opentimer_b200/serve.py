@@ -170,6 +170,12 @@ class TimingServer:
             t["slew_val"].ctypes.data, 1 if plain else 0, lat.ctypes.data, ctypes.byref(span)))
         return lat * 1e-9, span.value * 1e-9
 
+    def stats(self):
+        """(batches launched, requests they carried) since creation."""
+        b, r = ctypes.c_int64(), ctypes.c_int64()
+        check("otg_server_stats", lib().otg_server_stats(self._h, ctypes.byref(b), ctypes.byref(r)))
+        return b.value, r.value
+
     def read(self, d):
         """A design's per-node outputs (BFS order) and sink slews."""
         V, S = self._designs[d]

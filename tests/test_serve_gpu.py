@@ -166,12 +166,22 @@ def test_bad_update_is_reported_and_design_unchanged(cuda):
         did, _ = srv.add_design(d)
         before = srv.read(did)
         N = len(d["roots"])
-        t = srv.submit(did, cap=(np.array([N + 5], np.int32), np.array([0], np.int32),
-                                 np.ones((1, 4), np.float32)))
-        with pytest.raises(_lib.OtgError) as e:
-            srv.wait(t, 20000)
-        assert e.value.code == 1  # OTG_ERR_INVALID
+        n0 = int(d["nodes_start"][1] - d["nodes_start"][0])
+        bad = [dict(cap=(np.array([N + 5], np.int32), np.array([0], np.int32),
+                         np.ones((1, 4), np.float32))),
+               dict(cap=(np.array([0], np.int32), np.array([n0], np.int32),
+                         np.ones((1, 4), np.float32))),
+               dict(slew=(np.array([-1], np.int32), np.ones((1, 4), np.float32)))]
+        for kw in bad:
+            for call in (srv.submit, srv.update_sync):
+                with pytest.raises(_lib.OtgError) as e:
+                    call(did, **kw)
+                assert e.value.code == 1  # OTG_ERR_INVALID
         assert_same(srv.read(did), before)
+        # the server still serves the design
+        r = srv.wait(srv.submit(did, slew=(np.array([3], np.int32),
+                                           np.full((1, 4), 50.0, np.float32))), 20000)
+        assert r["dirty_nets"] == 1
     with TimingServer(max_updates=4) as small:
         did, _ = small.add_design(d)
         with pytest.raises(_lib.OtgError) as e:  # more updates than a batch holds
