@@ -257,6 +257,36 @@ otg_status otg_server_stats(otg_server* s, int64_t* batches, int64_t* requests);
 otg_status otg_server_read(otg_server* s, int32_t design_id, int32_t* node2bfs, float* load,
                            float* delay, float* ldelay, float* impulse, float* sink_slew);
 
+/*
+ * Tuning of the fused RC pass (per device; applies to later launches; no
+ * counterpart in the reference, whose kernels have fixed launch shapes).
+ * Nets of <= 32 nodes always take the warp path.  Block class c takes the
+ * nets with class_max[c-1] < n <= class_max[c] (class_max[-1] = 32), one
+ * CTA of class_threads[c] threads with class_items[c] scan items per
+ * thread, in shared memory; nets above the last class_max take the
+ * global-workspace path.  Shapes must be among the compiled ones
+ * (threads x items: 64x4, 64x8, 128x4, 128x8, 256x2, 256x4, 256x8, 512x2,
+ * 512x4, 512x8, 1024x2, 1024x4) and each class must fit shared memory.
+ * Every valid tuning gives identical outputs; only the speed differs.
+ * otg_rc_workspace_size depends on the tuning (the global-workspace
+ * slices): size workspaces after setting it.
+ */
+typedef struct otg_rc_tuning {
+  int32_t num_classes; /* 1..6 */
+  int32_t class_max[6];
+  int32_t class_threads[6];
+  int32_t class_items[6];
+} otg_rc_tuning;
+otg_status otg_rc_get_tuning(otg_rc_tuning* tuning);
+/* NULL restores the default; OTG_ERR_INVALID for a tuning that does not
+ * validate (nothing changes). */
+otg_status otg_rc_set_tuning(const otg_rc_tuning* tuning);
+/* Autotuner: times candidate tunings on a sample forest (device pointers;
+ * its outputs are overwritten) and applies the fastest; returns it in
+ * *tuning (may be NULL).  Allocates a temporary workspace.  Blocks. */
+otg_status otg_rc_autotune(const otg_rc_forest* sample, int32_t max_net_nodes,
+                           otg_stream_t stream, otg_rc_tuning* tuning);
+
 /* Human-readable name of a status code. */
 const char* otg_status_string(otg_status s);
 

@@ -18,7 +18,8 @@ from . import workloads  # noqa: F401
 from ._lib import C_SYMBOLS, CXX_SYMBOLS, OtgError, RcForest, check, lib  # noqa: F401
 
 __all__ = ["RcBatch", "rc_timing", "rc_timing_host", "levelize", "levelize_host",
-           "synth_forest", "kernel_launches", "OtgError", "lib"]
+           "synth_forest", "kernel_launches", "get_tuning", "set_tuning", "autotune",
+           "OtgError", "lib"]
 
 NC = 4  # corners: split*2 + tran
 
@@ -39,6 +40,46 @@ def _stream(stream):
     import torch
     s = stream if stream is not None else torch.cuda.current_stream()
     return ctypes.c_void_p(s.cuda_stream)
+
+
+def _tuning_dict(t):
+    k = t.num_classes
+    return {"class_max": list(t.class_max[:k]), "class_threads": list(t.class_threads[:k]),
+            "class_items": list(t.class_items[:k])}
+
+
+def get_tuning():
+    """The current device's RC-pass tuning: per block size class its upper
+    net size, CTA threads and scan items per thread."""
+    from ._lib import RcTuning
+    t = RcTuning()
+    check("otg_rc_get_tuning", lib().otg_rc_get_tuning(ctypes.byref(t)))
+    return _tuning_dict(t)
+
+
+def set_tuning(tuning=None):
+    """Applies a tuning (dict as from get_tuning; None: the default)."""
+    from ._lib import RcTuning
+    if tuning is None:
+        check("otg_rc_set_tuning", lib().otg_rc_set_tuning(None))
+        return
+    t = RcTuning()
+    t.num_classes = len(tuning["class_max"])
+    for c in range(t.num_classes):
+        t.class_max[c] = tuning["class_max"][c]
+        t.class_threads[c] = tuning["class_threads"][c]
+        t.class_items[c] = tuning["class_items"][c]
+    check("otg_rc_set_tuning", lib().otg_rc_set_tuning(ctypes.byref(t)))
+
+
+def autotune(batch, stream=None):
+    """Runs the autotuner on an RcBatch (its outputs are overwritten),
+    applies the fastest tuning and returns it."""
+    from ._lib import RcTuning
+    t = RcTuning()
+    check("otg_rc_autotune", lib().otg_rc_autotune(
+        ctypes.byref(batch._forest), batch.max_net_nodes, _stream(stream), ctypes.byref(t)))
+    return _tuning_dict(t)
 
 
 def kernel_launches():

@@ -27,6 +27,7 @@ C_SYMBOLS = [
     "otg_server_create", "otg_server_destroy", "otg_server_add_design",
     "otg_server_remove_design", "otg_server_submit", "otg_server_wait",
     "otg_server_update_sync", "otg_server_read", "otg_server_replay", "otg_server_stats",
+    "otg_rc_get_tuning", "otg_rc_set_tuning", "otg_rc_autotune",
 ]
 # The reference-compatible C++ entry points (include/otg_compat.hpp), by
 # their Itanium-mangled names.
@@ -54,6 +55,12 @@ class RcForest(ctypes.Structure):
         ("sinks_start", ctypes.c_void_p), ("sink_nodes", ctypes.c_void_p),
         ("driver_slew", ctypes.c_void_p), ("sink_slew", ctypes.c_void_p),
     ]
+
+
+class RcTuning(ctypes.Structure):
+    """otg_rc_tuning: block size classes of the fused RC pass."""
+    _fields_ = [("num_classes", ctypes.c_int32), ("class_max", ctypes.c_int32 * 6),
+                ("class_threads", ctypes.c_int32 * 6), ("class_items", ctypes.c_int32 * 6)]
 
 
 class RcResult(ctypes.Structure):
@@ -110,13 +117,17 @@ def lib():
         L.otg_server_read.argtypes = [P, I32, P, P, P, P, P, P]
         L.otg_server_replay.argtypes = [P, I32, P, P, P, P, P, P, P, P, P, I32, P, P]
         L.otg_server_stats.argtypes = [P, P, P]
+        L.otg_rc_get_tuning.argtypes = [ctypes.POINTER(RcTuning)]
+        L.otg_rc_set_tuning.argtypes = [ctypes.POINTER(RcTuning)]
+        L.otg_rc_autotune.argtypes = [ctypes.POINTER(RcForest), I32, P, ctypes.POINTER(RcTuning)]
         for name in ["otg_rc_workspace_size", "otg_rc_timing", "otg_rc_status", "otg_rc_timing_subset",
                      "otg_levelize_workspace_size", "otg_levelize", "otg_levelize_status",
                      "otg_rc_timing_host", "otg_levelize_host", "otg_synth_rc_forest",
                      "otg_synth_rc_sinks", "otg_synth_rc_forest_host", "otg_rc_timing_noalloc",
                      "otg_server_create", "otg_server_add_design", "otg_server_remove_design",
                      "otg_server_submit", "otg_server_wait", "otg_server_update_sync",
-                     "otg_server_read", "otg_server_replay", "otg_server_stats"]:
+                     "otg_server_read", "otg_server_replay", "otg_server_stats",
+                     "otg_rc_get_tuning", "otg_rc_set_tuning", "otg_rc_autotune"]:
             getattr(L, name).restype = ctypes.c_int
         _lib = L
     return _lib

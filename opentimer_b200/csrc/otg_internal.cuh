@@ -21,7 +21,7 @@ void count_launch();
 //                     A-a  ends[n] i32, posin[2m]
 //                     A-b  sub[2m], off[2m], spl[2m], splarc[S], sl[S] u64
 //                     A-c  depth[n], parent[n], pedge[n], slot[n]
-//                   then succ[2m] / radix buffers 2n, hist[256*W] i32
+//                   then succ[2m] / radix buffers 2n, hist[bins*W] i32
 //   B  (Elmore, one corner pair at a time; overlays A)
 //                   X[n] f2 (load, then ldelay), Y[n] f2 (delay),
 //                   Ip[n] 2 x i64 (fixed-point inclusive prefix of an
@@ -37,6 +37,10 @@ struct RcLayout {
 
 // Sublist splitters of the Euler-tour ranking: about one arc in kSplit.
 constexpr int kSplit = 16;
+
+// Radix digit of the block sort: 8 bits, 7 for 1024-thread CTAs (whose
+// 32 per-warp histograms would otherwise take 32 KB of shared memory).
+__host__ __device__ constexpr int rc_radix_bits(int T) { return T >= 1024 ? 7 : 8; }
 
 __host__ __device__ inline uint32_t rc_max3(uint32_t a, uint32_t b, uint32_t c) {
   return a > b ? (a > c ? a : c) : (b > c ? b : c);
@@ -87,7 +91,7 @@ __host__ __device__ inline RcLayout rc_layout(int n, int T, int K, int ib) {
   const uint32_t end_c = o;
   o = rc_max3(end_a, end_b, end_c);
   OTG_TAKE(r2, I * (A > 2u * N ? A : 2u * N));
-  OTG_TAKE(hist, 4u * 256u * W);
+  OTG_TAKE(hist, 4u * (1u << rc_radix_bits(T)) * W);
   const uint32_t endA = o;
   o = rA;
   OTG_TAKE(X, 8u * N);

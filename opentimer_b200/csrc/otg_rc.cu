@@ -31,6 +31,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cstring>
+#include <mutex>
 
 #include "../../include/otg.h"
 #include "otg_internal.cuh"
@@ -98,6 +99,16 @@ __device__ __forceinline__ const RcArgs& job_forest(const RcJob& j, int f) {
 }
 
 // ------------------------------------------------------------ float4 math
+// Sink slew sign(si) * sqrt(si^2 + impulse) (ot/timer/net.cpp:280-283).
+// The square and the sum are rounded separately, as in the reference's
+// host code; explicit intrinsics keep the compiler from fusing them into an
+// FMA in some kernels and not in others, so every path and tile shape
+// gives the same bits.
+__device__ __forceinline__ float sink_slew1(float si, float imp) {
+  const float r = sqrtf(__fadd_rn(__fmul_rn(si, si), imp));
+  return si < 0.0f ? -r : r;
+}
+
 __device__ __forceinline__ float4 f4add(float4 a, float4 b) {
   return make_float4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w);
 }
@@ -252,10 +263,10 @@ __device__ void rc_net_warp(const RcArgs& a, int net, int* s_par, int* s_pe) {
       float4 iv = shfl4(imp, ok ? v : 0);
       if (ok) {
         float4 o;
-        o.x = copysignf(sqrtf(si.x * si.x + iv.x), si.x);
-        o.y = copysignf(sqrtf(si.y * si.y + iv.y), si.y);
-        o.z = copysignf(sqrtf(si.z * si.z + iv.z), si.z);
-        o.w = copysignf(sqrtf(si.w * si.w + iv.w), si.w);
+        o.x = sink_slew1(si.x, iv.x);
+        o.y = sink_slew1(si.y, iv.y);
+        o.z = sink_slew1(si.z, iv.z);
+        o.w = sink_slew1(si.w, iv.w);
         a.sink_slew[k] = o;
       } else if (k < s1) {
         report(a, OTG_ERR_INVALID, net);
@@ -396,9 +407,10 @@ __device__ int block_scan_items(int count, ValF val, OutF out, int* wsum) {
   return carry;
 }
 
-// Stable LSD radix sort of the items 0..N-1 by key(i) (nbits bits, up to 8
-// bits per pass).  The final order lands in `out` (out[rank] = item); b0/b1
-// are ping-pong buffers of N entries; hist holds 256*(T/32) ints.  Each
+// Stable LSD radix sort of the items 0..N-1 by key(i) (nbits bits,
+// rc_radix_bits(T) bits per pass).  The final order lands in `out`
+// (out[rank] = item); b0/b1 are ping-pong buffers of N entries; hist holds
+// (1 << rc_radix_bits(T)) * (T/32) ints.  Each
 // warp owns a contiguous range of the current sequence, so ranks inside a
 // warp follow sequence order (match_any + popc) and the digit-major scan of
 // the per-warp counts keeps the sort stable.
@@ -409,11 +421,12 @@ __device__ void block_radix_sort(int N, int nbits, KeyF key, Ix* b0, Ix* b1, Ix*
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const unsigned lt = (1u << lane) - 1u;
   const int per = ((N + W - 1) / W + 31) & ~31;
+  constexpr int DB = rc_radix_bits(T);
   if (nbits < 1) nbits = 1;
-  const int passes = (nbits + 7) / 8;
+  const int passes = (nbits + DB - 1) / DB;
   for (int p = 0; p < passes; ++p) {
-    const int shift = 8 * p;
-    const int db = min(8, nbits - shift);
+    const int shift = DB * p;
+    const int db = min(DB, nbits - shift);
     const int nb = 1 << db;
     const unsigned mask = (unsigned)nb - 1u;
     const Ix* src = (p == 0) ? nullptr : ((p - 1) % 2 == 0 ? b0 : b1);
@@ -972,8 +985,7 @@ __device__ void rc_net_block(const RcArgs& a, int net, char* ws, int n, int* sh,
         const int v = a.sink_nodes[k];
         if ((unsigned)v >= (unsigned)n) { report(a, OTG_ERR_INVALID, net); continue; }
         const float2 iv = imp[pre[v]];
-        so[2 * (size_t)k + cp] = make_float2(copysignf(sqrtf(si.x * si.x + iv.x), si.x),
-                                             copysignf(sqrtf(si.y * si.y + iv.y), si.y));
+        so[2 * (size_t)k + cp] = make_float2(sink_slew1(si.x, iv.x), sink_slew1(si.y, iv.y));
       }
     }
     __syncthreads();
@@ -1071,16 +1083,26 @@ DevInfo& dev_info() {
 // kernel (sh[], s_item: under 1 KB).
 constexpr int kStaticSmemReserve = 2048;
 
-// Size classes.  Class 0: warp path.  Classes 1..6: one CTA per net in
-// shared memory (16-bit indices), T threads with K slots per thread per
-// scan tile.  Class 7: nets beyond the shared-memory budget, in per-CTA
-// slices of the workspace (32-bit indices).
-struct ClassShape {
-  int nmax, T, K;
+// Size classes.  Class 0: the warp path (nets of <= 32 nodes; its
+// lane-per-node scheme fixes that bound).  Classes 1..6: one CTA per net in
+// shared memory (16-bit indices); their upper bounds and tile shapes (T
+// threads, K scan items per thread) come from the device's tuning.
+// Class 7: nets beyond the last block class, in per-CTA slices of the
+// workspace (32-bit indices, 512 x 8).
+struct Shape {
+  int T, K;
 };
-constexpr ClassShape kShapes[RcClasses::kMax] = {
-    {32, 32, 1}, {128, 64, 4}, {256, 64, 8}, {512, 128, 8}, {1024, 256, 4},
-    {2048, 256, 8}, {0, 512, 8}, {1 << 30, 512, 8}};
+// The compiled block-class shapes (launch_shape dispatches on the index).
+constexpr Shape kShapeSet[] = {{64, 4},  {64, 8},  {128, 4}, {128, 8}, {256, 2},  {256, 4},
+                               {256, 8}, {512, 2}, {512, 4}, {512, 8}, {1024, 2}, {1024, 4}};
+constexpr int kNumShapes = (int)(sizeof(kShapeSet) / sizeof(kShapeSet[0]));
+constexpr int kBlockClasses = 6;
+
+int shape_index(int T, int K) {
+  for (int s = 0; s < kNumShapes; ++s)
+    if (kShapeSet[s].T == T && kShapeSet[s].K == K) return s;
+  return -1;
+}
 
 }  // namespace
 
@@ -1095,15 +1117,77 @@ int rc_smem_nmax(int T, int K, int smem_budget) {
   return lo;
 }
 
-RcClasses rc_classes(int smem_budget) {
+namespace {
+
+// Block-class tuning of one device: `num` classes, ascending upper bounds,
+// a kShapeSet index each.  Every tuning gives the same outputs (the sums
+// are exact, the BFS order is fixed); only the speed differs.
+struct RcTune {
+  int num = 0;
+  int nmax[kBlockClasses] = {};
+  int shape[kBlockClasses] = {};
+};
+
+RcTune default_tune(int smem_budget) {
+  RcTune t;
+  const int bounds[kBlockClasses - 1] = {128, 256, 512, 1024, 2048};
+  const Shape shapes[kBlockClasses] = {{64, 4}, {64, 8}, {128, 8}, {256, 4}, {256, 8}, {1024, 4}};
+  t.num = kBlockClasses;
+  for (int c = 0; c < kBlockClasses; ++c) {
+    t.shape[c] = shape_index(shapes[c].T, shapes[c].K);
+    t.nmax[c] = c < kBlockClasses - 1 ? bounds[c] : 0;
+  }
+  t.nmax[kBlockClasses - 1] =
+      std::max(bounds[kBlockClasses - 2] + 1, rc_smem_nmax(shapes[kBlockClasses - 1].T,
+                                                           shapes[kBlockClasses - 1].K, smem_budget));
+  return t;
+}
+
+bool tune_ok(const RcTune& t, int smem_budget) {
+  if (t.num < 1 || t.num > kBlockClasses) return false;
+  int prev = 32;
+  for (int c = 0; c < t.num; ++c) {
+    if (t.shape[c] < 0 || t.shape[c] >= kNumShapes || t.nmax[c] <= prev) return false;
+    const Shape sh = kShapeSet[t.shape[c]];
+    if (rc_layout(t.nmax[c], sh.T, sh.K, 2).total > (uint32_t)smem_budget) return false;
+    prev = t.nmax[c];
+  }
+  return true;
+}
+
+// Device-visible class bounds of a tuning: class c takes nets with
+// nmax[c-1] < n <= nmax[c]; unused block classes are empty ranges.
+RcClasses classes_of(const RcTune& t) {
   RcClasses c;
   c.num = RcClasses::kMax;
-  for (int i = 0; i < c.num; ++i) c.nmax[i] = kShapes[i].nmax;
-  c.nmax[6] = std::max(kShapes[5].nmax + 1, rc_smem_nmax(512, 8, smem_budget));
+  c.nmax[0] = 32;
+  for (int k = 1; k <= kBlockClasses; ++k) c.nmax[k] = t.nmax[std::min(k, t.num) - 1];
+  c.nmax[RcClasses::kMax - 1] = 1 << 30;
   return c;
 }
 
-namespace {
+std::mutex g_tune_mu;
+RcTune g_tune[64];
+bool g_tune_set[64] = {};
+
+RcTune current_tune(int smem_budget) {
+  int d = 0;
+  cudaGetDevice(&d);
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  if (!g_tune_set[d & 63]) {
+    g_tune[d & 63] = default_tune(smem_budget);
+    g_tune_set[d & 63] = true;
+  }
+  return g_tune[d & 63];
+}
+
+void set_tune(const RcTune& t) {
+  int d = 0;
+  cudaGetDevice(&d);
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune[d & 63] = t;
+  g_tune_set[d & 63] = true;
+}
 
 size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
@@ -1117,9 +1201,10 @@ int huge_ctas(int sms, size_t stride) {
 }  // namespace
 
 // Workspace: [status 64 B][counters 64 B][lists C x N ints][huge slices]
-size_t rc_workspace_bytes(int num_nets, int max_net_nodes, int sms, int smem_budget,
-                          size_t* off_lists, size_t* off_huge, size_t* huge_stride) {
-  const RcClasses c = rc_classes(smem_budget);
+// (the slices only when some net may exceed the tuning's last block class)
+size_t rc_workspace_bytes_for(const RcTune& t, int num_nets, int max_net_nodes, int sms,
+                              size_t* off_lists, size_t* off_huge, size_t* huge_stride) {
+  const RcClasses c = classes_of(t);
   size_t o = 128;
   *off_lists = o;
   o = align256(o + (size_t)c.num * (size_t)std::max(num_nets, 1) * 4);
@@ -1130,6 +1215,12 @@ size_t rc_workspace_bytes(int num_nets, int max_net_nodes, int sms, int smem_bud
     o += *huge_stride * (size_t)huge_ctas(sms, *huge_stride);
   }
   return o;
+}
+
+size_t rc_workspace_bytes(int num_nets, int max_net_nodes, int sms, int smem_budget,
+                          size_t* off_lists, size_t* off_huge, size_t* huge_stride) {
+  return rc_workspace_bytes_for(current_tune(smem_budget), num_nets, max_net_nodes, sms,
+                                off_lists, off_huge, huge_stride);
 }
 
 namespace {
@@ -1151,6 +1242,26 @@ cudaError_t launch_smem_class(const RcJob& job, const int* list, int* count, int
   count_launch();
   return cudaGetLastError();
 }
+
+cudaError_t launch_shape(int s, const RcJob& job, const int* list, int* count, int* work,
+                         int nmax, int sms, cudaStream_t st) {
+  switch (s) {
+    case 0: return launch_smem_class<64, 4>(job, list, count, work, nmax, sms, st);
+    case 1: return launch_smem_class<64, 8>(job, list, count, work, nmax, sms, st);
+    case 2: return launch_smem_class<128, 4>(job, list, count, work, nmax, sms, st);
+    case 3: return launch_smem_class<128, 8>(job, list, count, work, nmax, sms, st);
+    case 4: return launch_smem_class<256, 2>(job, list, count, work, nmax, sms, st);
+    case 5: return launch_smem_class<256, 4>(job, list, count, work, nmax, sms, st);
+    case 6: return launch_smem_class<256, 8>(job, list, count, work, nmax, sms, st);
+    case 7: return launch_smem_class<512, 2>(job, list, count, work, nmax, sms, st);
+    case 8: return launch_smem_class<512, 4>(job, list, count, work, nmax, sms, st);
+    case 9: return launch_smem_class<512, 8>(job, list, count, work, nmax, sms, st);
+    case 10: return launch_smem_class<1024, 2>(job, list, count, work, nmax, sms, st);
+    case 11: return launch_smem_class<1024, 4>(job, list, count, work, nmax, sms, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+static_assert(kNumShapes == 12, "launch_shape covers every kShapeSet entry");
 
 RcArgs make_args(const otg_rc_forest* f, int* status) {
   RcArgs a;
@@ -1189,20 +1300,23 @@ bool forest_ok(const otg_rc_forest* f) {
 // Launches the fused pass over the items of `job` (at most `cap` of them).
 // The workspace starts with [status 64 B][counters 64 B]; its status word is
 // where a.status should point for single-forest jobs.
+// `tune` (optional) overrides the device's tuning.
 otg_status rc_launch_job(RcJob job, int cap, int max_net_nodes, void* workspace,
-                         size_t workspace_bytes, cudaStream_t stream, const RcFork* fork = nullptr) {
+                         size_t workspace_bytes, cudaStream_t stream, const RcFork* fork = nullptr,
+                         const RcTune* tune = nullptr) {
   if (!workspace || cap < 0 || max_net_nodes < 1) return OTG_ERR_INVALID;
   DevInfo& di = dev_info();
   const int budget = di.smem_optin - kStaticSmemReserve;
+  const RcTune tn = tune ? *tune : current_tune(budget);
   size_t off_lists, off_huge, stride;
-  const size_t need = rc_workspace_bytes(std::max(cap, 1), max_net_nodes, di.sms, budget,
-                                         &off_lists, &off_huge, &stride);
+  const size_t need = rc_workspace_bytes_for(tn, std::max(cap, 1), max_net_nodes, di.sms,
+                                             &off_lists, &off_huge, &stride);
   if (workspace_bytes < need) return OTG_ERR_WORKSPACE;
   char* ws = (char*)workspace;
   int* status = (int*)ws;
   int* counters = (int*)(ws + 64);  // [0..7] counts, [8..15] work
   int* lists = (int*)(ws + off_lists);
-  const RcClasses cls = rc_classes(budget);
+  const RcClasses cls = classes_of(tn);
   if (cudaMemsetAsync(ws, 0, 128, stream) != cudaSuccess) {
     cudaGetLastError();
     return OTG_ERR_CUDA;
@@ -1235,18 +1349,11 @@ otg_status rc_launch_job(RcJob job, int cap, int max_net_nodes, void* workspace,
     count_launch();
     err = cudaGetLastError();
   }
-  for (int c = 6; c >= 1 && err == cudaSuccess; --c) {
+  for (int c = tn.num; c >= 1 && err == cudaSuccess; --c) {
     if (max_net_nodes <= cls.nmax[c - 1]) continue;
     const int nmax = std::min(cls.nmax[c], max_net_nodes);
-    cudaStream_t st = next_stream();
-    switch (c) {
-      case 1: err = launch_smem_class<64, 4>(job, L(c), counters + c, work + c, nmax, di.sms, st); break;
-      case 2: err = launch_smem_class<64, 8>(job, L(c), counters + c, work + c, nmax, di.sms, st); break;
-      case 3: err = launch_smem_class<128, 8>(job, L(c), counters + c, work + c, nmax, di.sms, st); break;
-      case 4: err = launch_smem_class<256, 4>(job, L(c), counters + c, work + c, nmax, di.sms, st); break;
-      case 5: err = launch_smem_class<256, 8>(job, L(c), counters + c, work + c, nmax, di.sms, st); break;
-      default: err = launch_smem_class<512, 8>(job, L(c), counters + c, work + c, nmax, di.sms, st); break;
-    }
+    err = launch_shape(tn.shape[c - 1], job, L(c), counters + c, work + c, nmax, di.sms,
+                       next_stream());
   }
   if (err == cudaSuccess) {
     rc_warp_kernel<<<di.sms * 8, 256, 0, next_stream()>>>(job, L(0), counters + 0, work + 0);
@@ -1301,6 +1408,128 @@ otg_status rc_launch_items(const RcArgsOpaque* forests, const int2* items, const
 
 size_t rc_args_bytes() { return sizeof(RcArgs); }
 
+namespace {
+
+// Autotuner: coordinate descent over the tuning on a sample forest (device
+// pointers), timing whole passes with CUDA events (best of 3 after one
+// checked pass).  Two rounds of: a shape per class, scaled class bounds
+// (lowering the last bound moves nets to the global-workspace path), and
+// merging a class into the next.  Every candidate gives the same outputs.
+otg_status rc_autotune(const otg_rc_forest* f, int max_net_nodes, cudaStream_t st, RcTune* out) {
+  if (!forest_ok(f) || f->num_nets < 1 || max_net_nodes < 1) return OTG_ERR_INVALID;
+  DevInfo& di = dev_info();
+  const int budget = di.smem_optin - kStaticSmemReserve;
+  RcTune widest;  // sends every block net to the global path: the largest workspace
+  widest.num = 1;
+  widest.nmax[0] = 33;
+  widest.shape[0] = 0;
+  size_t a0, a1, a2;
+  const size_t bytes =
+      rc_workspace_bytes_for(widest, f->num_nets, max_net_nodes, di.sms, &a0, &a1, &a2);
+  void* ws = nullptr;
+  if (cudaMalloc(&ws, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    return OTG_ERR_OOM;
+  }
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  RcJob job{};
+  job.a0 = make_args(f, (int*)ws);
+  job.num = f->num_nets;
+  otg_status err = OTG_OK;
+  auto time_of = [&](const RcTune& t) -> float {
+    if (rc_launch_job(job, f->num_nets, max_net_nodes, ws, bytes, st, nullptr, &t) != OTG_OK)
+      return 1e30f;
+    int code = 0;
+    if (cudaMemcpyAsync(&code, ws, 4, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess) {
+      cudaGetLastError();
+      err = OTG_ERR_CUDA;
+      return 1e30f;
+    }
+    if (code != 0) {
+      err = (otg_status)code;  // the sample itself is bad
+      return 1e30f;
+    }
+    float best = 1e30f;
+    for (int r = 0; r < 3; ++r) {
+      cudaEventRecord(e0, st);
+      rc_launch_job(job, f->num_nets, max_net_nodes, ws, bytes, st, nullptr, &t);
+      cudaEventRecord(e1, st);
+      cudaEventSynchronize(e1);
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      best = std::min(best, ms);
+    }
+    return best;
+  };
+  RcTune best = current_tune(budget);
+  float tb = time_of(best);
+  auto consider = [&](const RcTune& t) {
+    if (err != OTG_OK || !tune_ok(t, budget)) return;
+    const float x = time_of(t);
+    if (x < tb) {
+      tb = x;
+      best = t;
+    }
+  };
+  for (int round = 0; round < 2 && err == OTG_OK; ++round) {
+    for (int c = 0; c < best.num; ++c)
+      for (int sh = 0; sh < kNumShapes; ++sh) {
+        if (sh == best.shape[c]) continue;
+        RcTune t = best;
+        t.shape[c] = sh;
+        consider(t);
+      }
+    for (int c = 0; c < best.num; ++c)
+      for (float fct : {0.5f, 0.7f, 1.4f, 2.0f}) {
+        RcTune t = best;
+        t.nmax[c] = (int)(best.nmax[c] * fct);
+        consider(t);
+      }
+    for (int c = 0; c + 1 < best.num; ++c) {  // merge class c into c+1
+      RcTune t = best;
+      for (int k = c; k + 1 < t.num; ++k) {
+        t.nmax[k] = t.nmax[k + 1];
+        t.shape[k] = t.shape[k + 1];
+      }
+      --t.num;
+      consider(t);
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(ws);
+  if (err != OTG_OK) return err;
+  set_tune(best);
+  *out = best;
+  return OTG_OK;
+}
+
+void to_c(const RcTune& t, otg_rc_tuning* o) {
+  std::memset(o, 0, sizeof(*o));
+  o->num_classes = t.num;
+  for (int c = 0; c < t.num; ++c) {
+    o->class_max[c] = t.nmax[c];
+    o->class_threads[c] = kShapeSet[t.shape[c]].T;
+    o->class_items[c] = kShapeSet[t.shape[c]].K;
+  }
+}
+
+bool from_c(const otg_rc_tuning* o, RcTune* t) {
+  if (o->num_classes < 1 || o->num_classes > kBlockClasses) return false;
+  t->num = o->num_classes;
+  for (int c = 0; c < t->num; ++c) {
+    t->nmax[c] = o->class_max[c];
+    t->shape[c] = shape_index(o->class_threads[c], o->class_items[c]);
+    if (t->shape[c] < 0) return false;
+  }
+  return true;
+}
+
+}  // namespace
+
 cudaError_t rc_fork_create(RcFork* f, int n) {
   *f = RcFork{};
   f->n = std::min(std::max(n, 0), (int)RcFork::kMax);
@@ -1338,6 +1567,32 @@ otg_status otg_rc_workspace_size(int32_t num_nets, int32_t max_net_nodes, size_t
   *bytes = otg::rc_workspace_bytes(num_nets, max_net_nodes, di.sms,
                                    di.smem_optin - otg::kStaticSmemReserve, &a, &b, &c);
   return OTG_OK;
+}
+
+otg_status otg_rc_get_tuning(otg_rc_tuning* out) {
+  if (!out) return OTG_ERR_INVALID;
+  otg::DevInfo& di = otg::dev_info();
+  if (di.sms <= 0) return OTG_ERR_CUDA;
+  otg::to_c(otg::current_tune(di.smem_optin - otg::kStaticSmemReserve), out);
+  return OTG_OK;
+}
+
+otg_status otg_rc_set_tuning(const otg_rc_tuning* t) {
+  otg::DevInfo& di = otg::dev_info();
+  if (di.sms <= 0) return OTG_ERR_CUDA;
+  const int budget = di.smem_optin - otg::kStaticSmemReserve;
+  otg::RcTune tn = otg::default_tune(budget);
+  if (t && (!otg::from_c(t, &tn) || !otg::tune_ok(tn, budget))) return OTG_ERR_INVALID;
+  otg::set_tune(tn);
+  return OTG_OK;
+}
+
+otg_status otg_rc_autotune(const otg_rc_forest* sample, int32_t max_net_nodes,
+                           otg_stream_t stream, otg_rc_tuning* out) {
+  otg::RcTune t;
+  const otg_status st = otg::rc_autotune(sample, max_net_nodes, (cudaStream_t)stream, &t);
+  if (st == OTG_OK && out) otg::to_c(t, out);
+  return st;
 }
 
 otg_status otg_rc_timing(const otg_rc_forest* forest, int32_t max_net_nodes, void* workspace,
