@@ -31,6 +31,7 @@ METRIC = "RC-tree nodes/s (Elmore, 4 corners) & levelize edges/s; incr. p50/p99 
 NUM_NETS = 1_000_000
 SEED = 2024
 LV_PINS, LV_EDGES, LV_LEVELS = 5_000_000, 12_000_000, 200
+TUNE_NETS = 50_000
 # incremental sizing loop
 INC_GATES, INC_ITERS, INC_FRAC, INC_PLAIN_ITERS, INC_CHECK = 200_000, 1000, 0.005, 20, True
 # serving
@@ -232,6 +233,24 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+def autotune_on(seed, nets, lo, hi, dev):
+    """Runs the RC-pass autotuner on a seeded sample with the workload's
+    net-size distribution (a different seed from the timed forest) and
+    leaves its tuning applied.  Returns (tuning, seconds)."""
+    import torch
+    import opentimer_b200 as otg
+    from opentimer_b200 import workloads
+    t0 = time.perf_counter()
+    ns = torch.from_numpy(workloads.net_sizes(seed, nets, lo, hi)).to(dev)
+    g = otg.synth_forest(seed, ns)
+    b = otg.RcBatch(ns, g["edges"], g["roots"], g["res"], g["cap"], sinks_start=g["sinks_start"],
+                    sink_nodes=g["sink_nodes"], driver_slew=g["driver_slew"], max_net_nodes=hi)
+    t = otg.autotune(b)
+    del b, g, ns
+    torch.cuda.empty_cache()
+    return t, time.perf_counter() - t0
+
+
 def run_ours(args, world, rank, local):
     import torch
     import opentimer_b200 as otg
@@ -240,6 +259,10 @@ def run_ours(args, world, rank, local):
     stream = torch.cuda.current_stream(dev)
 
     # ---- workload (per rank: its own 1M nets -> weak scaling)
+    tuning, tune_s = None, 0.0
+    if not args.no_autotune:
+        tuning, tune_s = autotune_on(SEED + 100 + rank, min(TUNE_NETS, args.nets), args.min_nodes,
+                                     args.max_nodes, dev)
     ns_np = workloads.net_sizes(SEED + rank, args.nets, args.min_nodes, args.max_nodes)
     ns = torch.from_numpy(ns_np).to(dev)
     g = otg.synth_forest(SEED + rank, ns)
@@ -293,6 +316,10 @@ def run_ours(args, world, rank, local):
                                "trees / 30% chains, 4 corners, sink slews",
                    "num_nets_per_gpu": N, "total_nodes_per_gpu": V, "sinks_per_gpu": S,
                    "l2": "inputs and outputs (>60 GB) far exceed L2; no flush needed",
+                   "tuning": tuning or "default",
+                   "autotune": (f"otg_rc_autotune on {min(TUNE_NETS, args.nets)} nets of the same "
+                                f"distribution (another seed), {tune_s:.1f} s, before warm-up")
+                   if tuning else "off",
                    "parallelism": f"replicas x{world} (nets shard with no collective)"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": None,
@@ -424,6 +451,8 @@ def run_incremental():
     tr = workloads.request_trace(SEED + 5, [gm], INC_ITERS, None, lo=k, hi=k,
                                  design_of=zeros, arrival=zeros)
     plain_tr = workloads.per_gate_trace(tr, [gm], num_req=INC_PLAIN_ITERS)
+    import torch
+    tuning, tune_s = autotune_on(SEED + 12, int(2.5 * k), 2, 512, torch.device("cuda", 0))
     with TimingServer(slots=2, max_requests=4, max_updates=4 * k) as srv:
         did, fp = srv.add_design(design)
         warm_p = workloads.per_gate_trace(tr, [gm], num_req=2)
@@ -459,6 +488,9 @@ def run_incremental():
         "speedup": ups_b / ups_p,
         "dirty_nets_per_iteration": float(2.5 * k),
         "state_bit_exact_vs_full_pass": bool(ok),
+        "tuning": tuning,
+        "autotune": f"otg_rc_autotune on {int(2.5 * k)} nets of 2..512 nodes (a batch's "
+                    f"size), {tune_s:.1f} s, before the server captured its graphs",
         "design_footprint_bytes": int(fp),
     }
 
@@ -543,6 +575,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-incremental", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true")
     # smaller cases (profiling); the defaults are the benchmark workload
     ap.add_argument("--nets", type=int, default=NUM_NETS)
     ap.add_argument("--min-nodes", type=int, default=2)
