@@ -33,6 +33,11 @@ def build(ref=True):
     refdir = os.environ.get("OTG_REFERENCE_DIR", "/root/reference")
     if ref and os.path.isdir(os.path.join(refdir, "ot")):
         subprocess.run(["make", "-s", "-C", HERE, "ref", "REF=" + refdir, "-j8"], check=True)
+        # the whole reference Timer, linked with the reference CUDA module
+        # and with libotg (needs opentimer_b200/libotg.so built first)
+        if os.path.exists(os.path.join(HERE, "..", "opentimer_b200", "libotg.so")):
+            subprocess.run(["make", "-s", "-C", HERE, "timer", "REF=" + refdir, "-j8"],
+                           check=True)
     return os.path.exists(LIB_REF)
 
 

@@ -1,0 +1,119 @@
+// ot_run.cpp -- runs the reference OpenTimer Timer on a design directory and
+// dumps its results.  TEST INFRASTRUCTURE ONLY (the full-update parity check).
+//
+//   ot_run <dir> cpu|cuda <out.txt>
+//
+// <dir> holds early.lib, late.lib, design.v, design.spef, design.timing.
+// The same Timer sources are linked twice (oracle/Makefile): with the
+// reference's own CUDA module (ot_run_ref) and with libotg in its place
+// (ot_run_otg), so "cuda" runs either the reference kernels or ours behind
+// the unchanged Timer.  Output lines (all values %.9g, corners in the order
+// MIN-RISE, MIN-FALL, MAX-RISE, MAX-FALL; nan where the Timer has none):
+//   P <pin> at[4] slew[4] rat[4] slack[4]
+//   R <net> <node> load[4] delay[4] ldelay[4] impulse[4]   (per RC node)
+//   B <net> <node> <bfs slot> <pid of that slot>            (cuda only)
+// The per-node values are read from Rct::_nodes (cpu) or from the
+// FlatRctStorage arrays in BFS order (cuda), the node's local id being
+// rebuilt with the flat path's first-appearance rule over the SPEF RES
+// lines (ot/timer/net.cpp:388-410).
+#include <cmath>
+#include <cstdio>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#define private public
+#define protected public
+#include <ot/timer/timer.hpp>
+#undef private
+#undef protected
+
+// FlatRct keeps its offsets in the implicit private section of a class
+// (ot/timer/net.hpp:172-178), which the access macro cannot open; this view
+// has the same members in the same order.
+struct FlatRctView {
+  ot::FlatRctStorage* stor;
+  size_t num_nodes;
+  int arr_start;
+  int edge_start;
+  int net_id;
+};
+static_assert(sizeof(FlatRctView) == sizeof(ot::FlatRct), "FlatRct layout changed");
+
+static void put(FILE* f, std::optional<float> v) {
+  if (v) std::fprintf(f, " %.9g", *v);
+  else std::fprintf(f, " nan");
+}
+
+int main(int argc, char** argv) {
+  if (argc != 4) {
+    std::fprintf(stderr, "usage: %s <dir> cpu|cuda <out>\n", argv[0]);
+    return 2;
+  }
+  const std::string dir = argv[1];
+  const bool cuda = std::string(argv[2]) == "cuda";
+  ot::Timer timer;
+  timer.read_celllib(dir + "/early.lib", ot::MIN)
+      .read_celllib(dir + "/late.lib", ot::MAX)
+      .read_verilog(dir + "/design.v")
+      .read_spef(dir + "/design.spef")
+      .read_timing(dir + "/design.timing");
+  timer.cuda(cuda);
+  timer.update_timing();
+
+  FILE* f = std::fopen(argv[3], "w");
+  if (!f) return 3;
+  const ot::Split splits[2] = {ot::MIN, ot::MAX};
+  const ot::Tran trans[2] = {ot::RISE, ot::FALL};
+  for (auto& [name, pin] : timer._pins) {
+    std::fprintf(f, "P %s", name.c_str());
+    for (auto el : splits)
+      for (auto rf : trans) put(f, timer.report_at(name, el, rf));
+    for (auto el : splits)
+      for (auto rf : trans) put(f, timer.report_slew(name, el, rf));
+    for (auto el : splits)
+      for (auto rf : trans) put(f, timer.report_rat(name, el, rf));
+    for (auto el : splits)
+      for (auto rf : trans) put(f, timer.report_slack(name, el, rf));
+    std::fprintf(f, "\n");
+  }
+  for (auto& [nname, net] : timer._nets) {
+    if (const ot::Rct* rct = std::get_if<ot::Rct>(&net._rct)) {
+      for (auto& [node, rn] : rct->_nodes) {
+        std::fprintf(f, "R %s %s", nname.c_str(), node.c_str());
+        for (auto el : splits)
+          for (auto rf : trans) std::fprintf(f, " %.9g", rn._load[el][rf]);
+        for (auto el : splits)
+          for (auto rf : trans) std::fprintf(f, " %.9g", rn._delay[el][rf]);
+        for (auto el : splits)
+          for (auto rf : trans) std::fprintf(f, " %.9g", rn._ldelay[el][rf]);
+        for (auto el : splits)
+          for (auto rf : trans) std::fprintf(f, " %.9g", rn._impulse[el][rf]);
+        std::fprintf(f, "\n");
+      }
+    } else if (const ot::FlatRct* fr = std::get_if<ot::FlatRct>(&net._rct)) {
+      if (!net._spef_net || !timer._flat_rct_stor) continue;
+      const ot::FlatRctStorage& st = *timer._flat_rct_stor;
+      std::unordered_map<std::string, int> id;
+      std::vector<std::string> names;
+      for (const auto& [a, b, r] : net._spef_net->ress) {
+        (void)r;
+        for (const std::string* s : {&a, &b})
+          if (id.emplace(*s, (int)names.size()).second) names.push_back(*s);
+      }
+      const int base = reinterpret_cast<const FlatRctView*>(fr)->arr_start;
+      for (size_t k = 0; k < names.size(); ++k) {
+        const int slot = st.rct_node2bfs_order[base + k];
+        const size_t at = (size_t)(base + slot) * 4;
+        std::fprintf(f, "R %s %s", nname.c_str(), names[k].c_str());
+        for (const std::vector<float>* q : {&st.load, &st.delay, &st.ldelay, &st.impulse})
+          for (int c = 0; c < 4; ++c) std::fprintf(f, " %.9g", (*q)[at + c]);
+        std::fprintf(f, "\n");
+        std::fprintf(f, "B %s %s %d %d\n", nname.c_str(), names[k].c_str(), slot,
+                     slot == 0 ? 0 : st.rct_pid[base + slot]);
+      }
+    }
+  }
+  std::fclose(f);
+  return 0;
+}
