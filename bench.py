@@ -128,13 +128,23 @@ def barrier(world):
 
 
 def max_over_ranks(world, x):
+    """The maximum of x over all ranks (a device tensor under NCCL, a host
+    one under gloo)."""
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def rank_nets(rank, nets, lo, hi):
+    """This rank's share of a weak-scaling run: its own seeded nets (the
+    same count and size distribution on every rank, no data exchanged)."""
+    from opentimer_b200 import workloads
+    return workloads.net_sizes(SEED + rank, nets, lo, hi)
 
 
 def load_peaks():
@@ -263,7 +273,7 @@ def run_ours(args, world, rank, local):
     if not args.no_autotune:
         tuning, tune_s = autotune_on(SEED + 100 + rank, min(TUNE_NETS, args.nets), args.min_nodes,
                                      args.max_nodes, dev)
-    ns_np = workloads.net_sizes(SEED + rank, args.nets, args.min_nodes, args.max_nodes)
+    ns_np = rank_nets(rank, args.nets, args.min_nodes, args.max_nodes)
     ns = torch.from_numpy(ns_np).to(dev)
     g = otg.synth_forest(SEED + rank, ns)
     torch.cuda.synchronize()
