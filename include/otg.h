@@ -287,6 +287,39 @@ otg_status otg_rc_set_tuning(const otg_rc_tuning* tuning);
 otg_status otg_rc_autotune(const otg_rc_forest* sample, int32_t max_net_nodes,
                            otg_stream_t stream, otg_rc_tuning* tuning);
 
+/*
+ * SPEF to the flat RC layout (host side, parallel over nets).  Replaces the
+ * reference's read_spef + Net::_make_flat_rct pair for this layout
+ * (ot/parser-spef/parser-spef.hpp, ot/timer/net.cpp:370-461): ids by first
+ * appearance over each net's *RES lines, edges and res in *RES order, the
+ * root at the net's driver (*I ... O or *P ... I), cap[id][*] = the node's
+ * *CAP value (a coupling line counts for its first node), *NAME_MAP
+ * references expanded, values rounded to float and multiplied by r_scale /
+ * c_scale (a Timer's unit rebasing).  Pin caps are not added: they need the
+ * cell library; otg_spef_pins gives each net's pins with their local ids.
+ * Nets without *RES lines are left out.  threads <= 0: all host threads.
+ */
+typedef struct otg_spef otg_spef;
+otg_status otg_spef_read(const char* path, int32_t threads, float r_scale, float c_scale,
+                         otg_spef** out);
+/* units: ohm, farad and second per unit of the file (*R_UNIT, *C_UNIT,
+ * *T_UNIT); any output may be NULL. */
+otg_status otg_spef_sizes(const otg_spef* spef, int32_t* num_nets, int32_t* total_nodes,
+                          int32_t* total_pins, double* units);
+/* Host arrays in the otg_rc_forest layout: nodes_start[N+1], edges[V-N],
+ * roots[N], res[V-N], cap[V][4]; net_flags[N] (may be NULL): bit 0 no
+ * driver pin in the tree, bit 1 ids != |RES|+1 (not a tree), bit 2 a *CAP
+ * node outside the tree, bit 3 a malformed *CAP or *RES line. */
+otg_status otg_spef_fill(const otg_spef* spef, int32_t* nodes_start, otg_rc_edge* edges,
+                         int32_t* roots, float* res, float* cap, uint8_t* net_flags);
+/* Per net, its *CONN pins: pins_start[N+1], local id (-1: not in the tree),
+ * direction (0 I, 1 O, 2 B) and port flag (1 for *P). */
+otg_status otg_spef_pins(const otg_spef* spef, int32_t* pins_start, int32_t* pin_node,
+                         int8_t* pin_dir, int8_t* pin_port);
+const char* otg_spef_net_name(const otg_spef* spef, int32_t net);
+const char* otg_spef_pin_name(const otg_spef* spef, int32_t net, int32_t k);
+void otg_spef_free(otg_spef* spef);
+
 /* Human-readable name of a status code. */
 const char* otg_status_string(otg_status s);
 

@@ -28,6 +28,8 @@ C_SYMBOLS = [
     "otg_server_remove_design", "otg_server_submit", "otg_server_wait",
     "otg_server_update_sync", "otg_server_read", "otg_server_replay", "otg_server_stats",
     "otg_rc_get_tuning", "otg_rc_set_tuning", "otg_rc_autotune",
+    "otg_spef_read", "otg_spef_sizes", "otg_spef_fill", "otg_spef_pins", "otg_spef_net_name",
+    "otg_spef_pin_name", "otg_spef_free",
 ]
 # The reference-compatible C++ entry points (include/otg_compat.hpp), by
 # their Itanium-mangled names.
@@ -120,6 +122,17 @@ def lib():
         L.otg_rc_get_tuning.argtypes = [ctypes.POINTER(RcTuning)]
         L.otg_rc_set_tuning.argtypes = [ctypes.POINTER(RcTuning)]
         L.otg_rc_autotune.argtypes = [ctypes.POINTER(RcForest), I32, P, ctypes.POINTER(RcTuning)]
+        L.otg_spef_read.argtypes = [ctypes.c_char_p, I32, ctypes.c_float, ctypes.c_float,
+                                    ctypes.POINTER(P)]
+        L.otg_spef_sizes.argtypes = [P, P, P, P, P]
+        L.otg_spef_fill.argtypes = [P, P, P, P, P, P, P]
+        L.otg_spef_pins.argtypes = [P, P, P, P, P]
+        L.otg_spef_net_name.argtypes = [P, I32]
+        L.otg_spef_net_name.restype = ctypes.c_char_p
+        L.otg_spef_pin_name.argtypes = [P, I32, I32]
+        L.otg_spef_pin_name.restype = ctypes.c_char_p
+        L.otg_spef_free.argtypes = [P]
+        L.otg_spef_free.restype = None
         for name in ["otg_rc_workspace_size", "otg_rc_timing", "otg_rc_status", "otg_rc_timing_subset",
                      "otg_levelize_workspace_size", "otg_levelize", "otg_levelize_status",
                      "otg_rc_timing_host", "otg_levelize_host", "otg_synth_rc_forest",
@@ -127,7 +140,8 @@ def lib():
                      "otg_server_create", "otg_server_add_design", "otg_server_remove_design",
                      "otg_server_submit", "otg_server_wait", "otg_server_update_sync",
                      "otg_server_read", "otg_server_replay", "otg_server_stats",
-                     "otg_rc_get_tuning", "otg_rc_set_tuning", "otg_rc_autotune"]:
+                     "otg_rc_get_tuning", "otg_rc_set_tuning", "otg_rc_autotune",
+                     "otg_spef_read", "otg_spef_sizes", "otg_spef_fill", "otg_spef_pins"]:
             getattr(L, name).restype = ctypes.c_int
         _lib = L
     return _lib

@@ -14,7 +14,9 @@ CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libotg.so")
 SOURCES = ["otg_rc.cu", "otg_levelize.cu", "otg_synth.cu", "otg_host.cu", "otg_noalloc.cu",
-           "otg_serve.cu"]
+           "otg_serve.cu", "otg_spef.cpp"]
+CXX = os.environ.get("CXX", "g++")
+CXXFLAGS = ["-O3", "-std=c++17", "-fPIC", "-pthread", "-Wall"]
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -37,15 +39,18 @@ def build(verbose=False, extra_flags=()):
     objs = []
     for s in SOURCES:
         src = os.path.join(CSRC, s)
-        obj = os.path.join(BUILD, s.replace(".cu", ".o"))
+        obj = os.path.join(BUILD, os.path.splitext(s)[0] + ".o")
         objs.append(obj)
         if _newer([src] + headers, obj):
-            cmd = [NVCC] + FLAGS + list(extra_flags) + ["-c", src, "-o", obj]
+            if s.endswith(".cpp"):  # host-only C++
+                cmd = [CXX] + CXXFLAGS + ["-c", src, "-o", obj]
+            else:
+                cmd = [NVCC] + FLAGS + list(extra_flags) + ["-c", src, "-o", obj]
             if verbose:
                 print(" ".join(cmd), flush=True)
             subprocess.run(cmd, check=True)
     if _newer(objs, LIB):
-        cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"]
+        cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart", "-Xcompiler", "-pthread"]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)

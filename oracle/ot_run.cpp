@@ -12,6 +12,10 @@
 //   P <pin> at[4] slew[4] rat[4] slack[4]
 //   R <net> <node> load[4] delay[4] ldelay[4] impulse[4]   (per RC node)
 //   B <net> <node> <bfs slot> <pid of that slot>            (cuda only)
+//   K <pin> cap[4]                                          (pin caps)
+//   S <net> <num nodes> <root id>                           (cuda only:
+//   E <net> <edge k> <s> <t> <res>                           the flat
+//   C <net> <id> cap[4]                                      storage)
 // The per-node values are read from Rct::_nodes (cpu) or from the
 // FlatRctStorage arrays in BFS order (cuda), the node's local id being
 // rebuilt with the flat path's first-appearance rule over the SPEF RES
@@ -76,6 +80,10 @@ int main(int argc, char** argv) {
     for (auto el : splits)
       for (auto rf : trans) put(f, timer.report_slack(name, el, rf));
     std::fprintf(f, "\n");
+    std::fprintf(f, "K %s", name.c_str());
+    for (auto el : splits)
+      for (auto rf : trans) std::fprintf(f, " %.9g", pin.cap(el, rf));
+    std::fprintf(f, "\n");
   }
   for (auto& [nname, net] : timer._nets) {
     if (const ot::Rct* rct = std::get_if<ot::Rct>(&net._rct)) {
@@ -101,7 +109,19 @@ int main(int argc, char** argv) {
         for (const std::string* s : {&a, &b})
           if (id.emplace(*s, (int)names.size()).second) names.push_back(*s);
       }
-      const int base = reinterpret_cast<const FlatRctView*>(fr)->arr_start;
+      const FlatRctView* view = reinterpret_cast<const FlatRctView*>(fr);
+      const int base = view->arr_start;
+      std::fprintf(f, "S %s %zu %d\n", nname.c_str(), view->num_nodes, st.rct_roots[view->net_id]);
+      for (size_t k = 0; k + 1 < view->num_nodes; ++k) {
+        const auto& e = st.rct_edges[view->edge_start + k];
+        std::fprintf(f, "E %s %zu %d %d %.9g\n", nname.c_str(), k, e.s, e.t,
+                     st.rct_edges_res[view->edge_start + k]);
+      }
+      for (size_t k = 0; k < view->num_nodes; ++k) {
+        std::fprintf(f, "C %s %zu", nname.c_str(), k);
+        for (int c = 0; c < 4; ++c) std::fprintf(f, " %.9g", st.rct_nodes_cap[(base + k) * 4 + c]);
+        std::fprintf(f, "\n");
+      }
       for (size_t k = 0; k < names.size(); ++k) {
         const int slot = st.rct_node2bfs_order[base + k];
         const size_t at = (size_t)(base + slot) * 4;

@@ -35,7 +35,7 @@ def run(exe, d, mode):
     p = subprocess.run([exe, d, mode, out], capture_output=True, text=True, timeout=600)
     assert p.returncode == 0, p.stderr[-2000:]
     assert "cannot" not in p.stderr and " E " not in p.stderr, p.stderr[-2000:]
-    P, R, B = {}, {}, {}
+    P, R, B, S = {}, {}, {}, {"pin_cap": {}, "root": {}, "edges": {}, "cap": {}}
     with open(out) as f:
         for line in f:
             t = line.split()
@@ -45,7 +45,17 @@ def run(exe, d, mode):
                 R[(t[1], t[2])] = np.array([float(x) for x in t[3:]], np.float64)
             elif t[0] == "B":
                 B[(t[1], t[2])] = (int(t[3]), int(t[4]))
-    return P, R, B
+            elif t[0] == "K":
+                S["pin_cap"][t[1]] = np.array([float(x) for x in t[2:]], np.float32)
+            elif t[0] == "S":
+                S["root"][t[1]] = int(t[3])
+                S["edges"][t[1]] = []
+                S["cap"][t[1]] = []
+            elif t[0] == "E":
+                S["edges"][t[1]].append((int(t[3]), int(t[4]), np.float32(float(t[5]))))
+            elif t[0] == "C":
+                S["cap"][t[1]].append(np.array([float(x) for x in t[3:]], np.float32))
+    return P, R, B, S
 
 
 def rc_ok(got, ref):
@@ -83,7 +93,8 @@ def runs(tmp_path_factory, cuda):
         pytest.skip("the reference Timer harness (oracle/_ref) is not built")
     d = str(tmp_path_factory.mktemp("config0"))
     info = config0_design.write_design(d, seed=2024, gates=2000)
-    return info, run(EXE_REF, d, "cuda"), run(EXE_OTG, d, "cuda"), run(EXE_REF, d, "cpu")
+    return (dict(info, dir=d), run(EXE_REF, d, "cuda"), run(EXE_OTG, d, "cuda"),
+            run(EXE_REF, d, "cpu"))
 
 
 def test_bfs_order_bit_exact(runs):
@@ -111,3 +122,37 @@ def test_pin_timing_within_tolerance(runs):
     assert w_gpu <= 1.0 and w_cpu <= 1.0
     slack = np.array([v[12:] for v in ours[0].values()])
     assert np.isfinite(slack).sum() > 1000 and not math.isnan(float(np.nanmin(slack)))
+
+
+def test_spef_reader_matches_timer_storage(runs):
+    """otg_spef_read on the design's SPEF gives the flat storage the
+    reference Timer builds (read_spef + Net::_make_flat_rct): the same ids,
+    edges, res and root for every net, and the same caps once each non-root
+    pin's library cap is added in float, as the flat path does
+    (ot/timer/net.cpp:433-446).  The Timer rebases the file's ohms to its
+    kilo-ohm library unit, so the reader gets r_scale = 1e-3."""
+    from opentimer_b200.spef import read_spef
+    info, ref, _, _ = runs
+    S = ref[3]
+    f = read_spef(os.path.join(info["dir"], "design.spef"), r_scale=np.float32(1e-3))
+    ns, ps = f["nodes_start"], f["pins_start"]
+    assert len(f["net_names"]) == len(S["root"])
+    k = 0
+    for i, name in enumerate(f["net_names"]):
+        b, e = int(ns[i]), int(ns[i + 1])
+        eb = b - i
+        assert f["roots"][i] == S["root"][name], name
+        ref_edges = S["edges"][name]
+        assert len(ref_edges) == e - b - 1
+        for j, (s_, t_, r_) in enumerate(ref_edges):
+            # the reference's edges are directed by its BFS by now
+            assert {s_, t_} == {int(f["edges"][eb + j, 0]), int(f["edges"][eb + j, 1])}, name
+            assert f["res"][eb + j] == r_, name
+        cap = f["cap"][b:e].copy()
+        for q in range(ps[i], ps[i + 1]):
+            node = int(f["pin_node"][q])
+            if node != f["roots"][i]:
+                cap[node] = cap[node] + S["pin_cap"][f["pin_names"][q]]
+        assert np.array_equal(cap, np.stack(S["cap"][name])), name
+        k += e - b
+    assert k == int(ns[-1]) > 10000
