@@ -32,6 +32,7 @@ NUM_NETS = 1_000_000
 SEED = 2024
 LV_PINS, LV_EDGES, LV_LEVELS = 5_000_000, 12_000_000, 200
 TUNE_NETS = 50_000
+SPEF_NETS = 20_000
 # incremental sizing loop
 INC_GATES, INC_ITERS, INC_FRAC, INC_PLAIN_ITERS, INC_CHECK = 200_000, 1000, 0.005, 20, True
 # serving
@@ -352,6 +353,8 @@ def run_ours(args, world, rank, local):
         line["incremental"] = run_incremental()
     if world == 1 and not args.no_serving:
         line["serving"] = run_serving()
+    if rank == 0 and not args.no_spef:
+        line["spef_ingest"] = run_spef()
     return line
 
 
@@ -563,6 +566,49 @@ def run_serving():
     return out
 
 
+def run_spef():
+    """SPEF ingestion: a seeded 20k-net SPEF (2..512 nodes per net, ~1.8M
+    nodes) read into the flat RC layout by otg_spef_read (all host threads,
+    and one), against the reference's SPEF parser plus the flat id rule
+    (oracle/_ref, one thread, as the reference reads SPEF)."""
+    import tempfile
+    from opentimer_b200 import synth_forest_host, workloads
+    from opentimer_b200.spef import read_spef
+    ns = workloads.net_sizes(SEED + 20, SPEF_NETS, 2, 512)
+    forest = synth_forest_host(SEED + 20, ns)
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "forest.spef")
+        V = workloads.write_spef(path, forest)
+        mb = os.path.getsize(path) / 1e6
+
+        def best(fn, reps=3):
+            t = 1e30
+            for _ in range(reps):
+                t0 = time.perf_counter()
+                fn()
+                t = min(t, time.perf_counter() - t0)
+            return t
+        t_all = best(lambda: read_spef(path, threads=0, names=False))
+        t_one = best(lambda: read_spef(path, threads=1, names=False))
+        got = read_spef(path, names=False)
+        same = bool(np.array_equal(got["edges"], forest["edges"]) and
+                    np.array_equal(got["roots"], forest["roots"]))
+        ref = None
+        if os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libotref.so")):
+            sys.path.insert(0, os.path.join(ROOT, "oracle"))
+            import oracle as O
+            L = O.ref_lib()
+            n, v = ctypes.c_int(), ctypes.c_int()
+            t_ref = best(lambda: L.otref_spef_load(path.encode(), ctypes.byref(n),
+                                                   ctypes.byref(v)), reps=1)
+            ref = {"nodes_per_s": V / t_ref, "threads": 1,
+                   "what": "the reference's SPEF parser (PEGTL) + the flat id rule"}
+    return {"workload": f"{SPEF_NETS} nets, {V} nodes, {mb:.0f} MB of SPEF text",
+            "nodes_per_s": V / t_all, "threads": os.cpu_count(),
+            "single_thread_nodes_per_s": V / t_one, "ids_round_trip": same,
+            "reference": ref}
+
+
 def cpu_baseline(g, ns_np):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     threads = os.cpu_count() or 1
@@ -586,6 +632,7 @@ def main():
     ap.add_argument("--no-incremental", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--no-spef", action="store_true")
     # smaller cases (profiling); the defaults are the benchmark workload
     ap.add_argument("--nets", type=int, default=NUM_NETS)
     ap.add_argument("--min-nodes", type=int, default=2)

@@ -29,6 +29,7 @@
 #include <charconv>
 #include <cstdint>
 #include <cstring>
+#include <deque>
 #include <string>
 #include <string_view>
 #include <thread>
@@ -110,7 +111,7 @@ std::string expand(sv s, const std::unordered_map<uint64_t, std::string>& map) {
 struct IdTable {
   std::vector<uint64_t> hash;
   std::vector<int32_t> id;
-  std::vector<const std::string*> key;
+  std::vector<sv> key;
   size_t mask = 0;
   void reset(size_t n) {
     size_t cap = 16;
@@ -118,20 +119,20 @@ struct IdTable {
     if (hash.size() < cap) {
       hash.assign(cap, 0);
       id.assign(cap, -1);
-      key.assign(cap, nullptr);
+      key.assign(cap, sv());
     } else {
       std::fill(id.begin(), id.begin() + cap, -1);
     }
     mask = cap - 1;
   }
-  static uint64_t h(const std::string& s) {
+  static uint64_t h(sv s) {
     uint64_t x = 1469598103934665603ull;
     for (unsigned char c : s) x = (x ^ c) * 1099511628211ull;
     return x | 1;
   }
   // returns the id of s, inserting `fresh` when absent
-  int32_t get(const std::string* s, int32_t fresh, bool* inserted) {
-    const uint64_t hv = h(*s);
+  int32_t get(sv s, int32_t fresh, bool* inserted) {
+    const uint64_t hv = h(s);
     for (size_t i = hv & mask;; i = (i + 1) & mask) {
       if (id[i] < 0) {
         hash[i] = hv;
@@ -140,17 +141,17 @@ struct IdTable {
         *inserted = true;
         return fresh;
       }
-      if (hash[i] == hv && *key[i] == *s) {
+      if (hash[i] == hv && key[i] == s) {
         *inserted = false;
         return id[i];
       }
     }
   }
-  int32_t find(const std::string& s) const {
+  int32_t find(sv s) const {
     const uint64_t hv = h(s);
     for (size_t i = hv & mask;; i = (i + 1) & mask) {
       if (id[i] < 0) return -1;
-      if (hash[i] == hv && *key[i] == s) return id[i];
+      if (hash[i] == hv && key[i] == s) return id[i];
     }
   }
 };
@@ -161,9 +162,16 @@ constexpr uint8_t kNoDriver = 1, kNotTree = 2, kCapNode = 4, kSyntax = 8;
 bool parse_net(sv block, const std::unordered_map<uint64_t, std::string>& map, float r_scale,
                float c_scale, IdTable& tab, Net* net) {
   enum { NONE, CONN, CAP, RES, OTHER } sec = NONE;
-  std::vector<std::string> names;  // node names by local id (stable storage)
-  std::vector<std::pair<std::string, float>> caps;
-  std::vector<std::pair<std::string, std::string>> ress;
+  // Node names are views into the file; with a name map, into expanded
+  // copies kept in `store` (a deque: its elements never move).
+  std::deque<std::string> store;
+  auto name = [&](sv s) -> sv {
+    if (map.empty()) return s;
+    store.push_back(expand(s, map));
+    return store.back();
+  };
+  std::vector<std::pair<sv, float>> caps;
+  std::vector<std::pair<sv, sv>> ress;
   std::vector<float> resv;
   sv t[8];
   size_t p = 0;
@@ -201,12 +209,12 @@ bool parse_net(sv block, const std::unordered_map<uint64_t, std::string>& map, f
     }
     float v = 0.f;
     if (sec == CAP) {
-      if (k == 3 && parse_float(t[2], &v)) caps.emplace_back(expand(t[1], map), v);
-      else if (k >= 4 && parse_float(t[3], &v)) caps.emplace_back(expand(t[1], map), v);
+      if (k == 3 && parse_float(t[2], &v)) caps.emplace_back(name(t[1]), v);
+      else if (k >= 4 && parse_float(t[3], &v)) caps.emplace_back(name(t[1]), v);
       else net->flags |= kSyntax;
     } else if (sec == RES) {
       if (k >= 4 && parse_float(t[3], &v)) {
-        ress.emplace_back(expand(t[1], map), expand(t[2], map));
+        ress.emplace_back(name(t[1]), name(t[2]));
         resv.push_back(v);
       } else {
         net->flags |= kSyntax;
@@ -216,21 +224,21 @@ bool parse_net(sv block, const std::unordered_map<uint64_t, std::string>& map, f
   if (ress.empty()) return true;  // no RC tree
   // ids by first appearance over the RES lines
   tab.reset(2 * ress.size() + 2);
-  names.reserve(2 * ress.size() + 2);
+  int32_t count = 0;
   net->edges.resize(ress.size());
   net->res.resize(ress.size());
   for (size_t e = 0; e < ress.size(); ++e) {
     int32_t ids[2];
-    const std::string* nm[2] = {&ress[e].first, &ress[e].second};
+    const sv nm[2] = {ress[e].first, ress[e].second};
     for (int j = 0; j < 2; ++j) {
       bool ins = false;
-      ids[j] = tab.get(nm[j], (int32_t)names.size(), &ins);
-      if (ins) names.push_back(*nm[j]);
+      ids[j] = tab.get(nm[j], count, &ins);
+      if (ins) ++count;
     }
     net->edges[e] = Edge{ids[0], ids[1]};
     net->res[e] = resv[e] * r_scale;
   }
-  net->n = (int32_t)names.size();
+  net->n = count;
   if ((size_t)net->n != ress.size() + 1) net->flags |= kNotTree;
   for (auto& pin : net->pins) {
     pin.node = tab.find(pin.name);

@@ -227,3 +227,42 @@ def apply_trace(design, trace, num_req=None):
     net = trace["slew_net"][:s1]
     last = len(net) - 1 - np.unique(net[::-1], return_index=True)[1]
     design["driver_slew"][net[last]] = trace["slew_val"][:s1][last]
+
+
+def write_spef(path, forest, seed=0):
+    """Writes a flat RC forest (host dict as from synth_forest_host, with
+    sink_count) as SPEF text: one *D_NET per net, the root named as the
+    driver pin D<i>:Z, leaves as sink pins S<i>_<k>:A, other nodes
+    n<i>:<k>; *RES lines in edge order (so the flat ids come back as the
+    forest's own ids), ground caps from corner 0, units ohm / fF / ns.
+    Returns the number of nodes written."""
+    ns = forest["nodes_start"]
+    edges, roots, res, cap = forest["edges"], forest["roots"], forest["res"], forest["cap"]
+    N = len(ns) - 1
+    out = ['*SPEF "IEEE 1481-1998"', '*DESIGN "synth"', "*DIVIDER /", "*DELIMITER :",
+           "*T_UNIT 1 NS", "*C_UNIT 1 FF", "*R_UNIT 1 OHM", "*L_UNIT 1 HENRY", ""]
+    with open(path, "w") as f:
+        f.write("\n".join(out) + "\n")
+        for i in range(N):
+            b, e = int(ns[i]), int(ns[i + 1])
+            n = e - b
+            eb = b - i
+            deg = np.zeros(n, np.int64)
+            ed = edges[eb:eb + n - 1]
+            np.add.at(deg, ed.reshape(-1), 1)
+            r = int(roots[i])
+            names = [f"n{i}:{k}" for k in range(n)]
+            names[r] = f"D{i}:Z"
+            sinks = [k for k in range(n) if k != r and deg[k] == 1]
+            for k in sinks:
+                names[k] = f"S{i}_{k}:A"
+            lines = [f"*D_NET N{i} {float(cap[b:e, 0].sum()):.6g}", "*CONN", f"*I D{i}:Z O"]
+            lines += [f"*I {names[k]} I" for k in sinks]
+            lines.append("*CAP")
+            lines += [f"{k + 1} {names[k]} {float(cap[b + k, 0]):.7g}" for k in range(n)]
+            lines.append("*RES")
+            lines += [f"{j + 1} {names[int(ed[j, 0])]} {names[int(ed[j, 1])]} "
+                      f"{float(res[eb + j]):.7g}" for j in range(n - 1)]
+            lines.append("*END\n")
+            f.write("\n".join(lines) + "\n")
+    return int(ns[-1])
