@@ -320,6 +320,64 @@ const char* otg_spef_net_name(const otg_spef* spef, int32_t net);
 const char* otg_spef_pin_name(const otg_spef* spef, int32_t net, int32_t k);
 void otg_spef_free(otg_spef* spef);
 
+/*
+ * Levelized timing propagation (the consumer of the RC pass): slew, arc
+ * delay, arrival time and timing-test required time forward; required time
+ * and slack backward; corner c = split*2 + tran.  It restates the reference
+ * Timer's per-pin tasks (ot/timer/timer.cpp:733-832, arc.cpp:82-205,
+ * pin.cpp:324-380, test.cpp:88-135) and its NLDM look-ups
+ * (ot/liberty/timing.cpp:198-628, lut.cpp:166-245) over a flat graph; the
+ * Timer has no GPU counterpart for it.  All arrays are device pointers;
+ * "none" (an empty value in the reference) is NaN.
+ */
+typedef struct otg_prop_graph {
+  int32_t num_pins, num_arcs, num_tests;
+  const int32_t* arc_from;     /* [A] */
+  const int32_t* arc_to;       /* [A] */
+  const int32_t* arc_kind;     /* [A] 0 net arc, 1 cell arc */
+  const int32_t* arc_timing;   /* [A][2] cell arcs: timing record per split (-1 none) */
+  const int32_t* arc_net;      /* [A] net arcs: the forest net; cell arcs: the net the
+                                  arc drives (its load), -1 none (load 0) */
+  const int32_t* arc_node;     /* [A] net arcs: the sink's global RC node index
+                                  (nodes_start[net] + local id), -1 not in the tree */
+  const int32_t* fanin_start;  /* [P+1] CSR of the arcs into each pin */
+  const int32_t* fanin;
+  const int32_t* fanout_start; /* [P+1] CSR of the arcs out of each pin */
+  const int32_t* fanout;
+  const int32_t* test_arc;     /* [T] the constraint arc (related -> constrained pin) */
+  const int32_t* test_start;   /* [P+1] CSR of the tests constrained at each pin */
+  const int32_t* test_of_pin;
+  const float* pi_at;          /* [P][4] primary-input assertions (NaN none) */
+  const float* pi_slew;        /* [P][4] */
+  const float* po_rat;         /* [P][4] primary-output assertions */
+  const int32_t* timing;       /* [R][9] sense (0 positive, 1 negative, 2 other unate),
+                                  edge (0 none, 1 rising, 2 falling), constraint flag,
+                                  LUT ids of cell_rise, cell_fall, rise_transition,
+                                  fall_transition, rise_constraint, fall_constraint */
+  const int32_t* lut_meta;     /* [L][4] n1, n2, offset in lut_data, variable order
+                                  (0: slew or related-pin slew first; 1: load or
+                                  constrained-pin slew first; -1: no template) */
+  const float* lut_data;       /* per LUT: index_1[n1], index_2[n2], values[n1*n2] */
+  float period;                /* clock period of the timing tests (NaN: no clock) */
+} otg_prop_graph;
+
+typedef struct otg_prop_rc {   /* outputs of otg_rc_timing for the design's nets */
+  const int32_t* nodes_start;
+  const int32_t* node2bfs;
+  const float* load;
+  const float* delay;
+  const float* impulse;
+} otg_prop_rc;
+
+otg_status otg_prop_workspace_size(int32_t num_arcs, int32_t num_tests, size_t* bytes);
+/* order (device) and level_ends (HOST, num_levels+1 entries) are
+ * otg_levelize's output over the graph's fanin CSR (pins without fanout
+ * are level 0).  Writes at, slew, rat, slack [P][4].  Asynchronous. */
+otg_status otg_propagate(const otg_prop_graph* graph, const otg_prop_rc* rc,
+                         const int32_t* order, const int32_t* level_ends, int32_t num_levels,
+                         float* at, float* slew, float* rat, float* slack, void* workspace,
+                         size_t workspace_bytes, otg_stream_t stream);
+
 /* Human-readable name of a status code. */
 const char* otg_status_string(otg_status s);
 

@@ -1,0 +1,113 @@
+"""Levelized timing propagation on the GPU (otg_propagate in include/otg.h).
+
+    g = TimingGraph(arrays)          # numpy arrays of the otg_prop_graph layout
+    out = g.propagate(rc_batch)      # at / slew / rat / slack [P][4], numpy
+
+The graph is flat: pins, arcs (net arcs onto RC nodes of the RcBatch's
+forest, cell arcs with a timing record per split), timing records, look-up
+tables, timing tests and primary-input/-output assertions.  Levels come
+from otg_levelize over the graph's fanin CSR.
+"""
+import ctypes
+
+import numpy as np
+
+from . import LevelizeBatch, _ptr, _stream, check, lib
+
+NC = 4
+
+
+class PropGraph(ctypes.Structure):
+    _fields_ = [("num_pins", ctypes.c_int32), ("num_arcs", ctypes.c_int32),
+                ("num_tests", ctypes.c_int32)] + [
+        (k, ctypes.c_void_p) for k in
+        ["arc_from", "arc_to", "arc_kind", "arc_timing", "arc_net", "arc_node", "fanin_start",
+         "fanin", "fanout_start", "fanout", "test_arc", "test_start", "test_of_pin", "pi_at",
+         "pi_slew", "po_rat", "timing", "lut_meta", "lut_data"]] + [("period", ctypes.c_float)]
+
+
+class PropRc(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_void_p) for k in
+                ["nodes_start", "node2bfs", "load", "delay", "impulse"]]
+
+
+def _csr(keys, n):
+    """CSR of item indices grouped by key (stable)."""
+    keys = np.asarray(keys, np.int64)
+    start = np.zeros(n + 1, np.int32)
+    start[1:] = np.cumsum(np.bincount(keys, minlength=n))
+    return start, np.argsort(keys, kind="stable").astype(np.int32)
+
+
+class TimingGraph:
+    """arrays: arc_from, arc_to, arc_kind, arc_timing [A,2], arc_net,
+    arc_node, test_arc, pi_at, pi_slew, po_rat [P,4], timing [R,9],
+    lut_meta [L,4], lut_data, period; num_pins."""
+
+    def __init__(self, arrays, device="cuda"):
+        import torch
+        a = arrays
+        P = int(a["num_pins"])
+        A = len(a["arc_from"])
+        self.P, self.A = P, A
+        fanin_start, fanin = _csr(a["arc_to"], P)
+        fanout_start, fanout = _csr(a["arc_from"], P)
+        test_arc = np.asarray(a["test_arc"], np.int32)
+        test_start, test_of_pin = _csr(np.asarray(a["arc_to"])[test_arc], P)
+        host = {
+            "arc_from": a["arc_from"], "arc_to": a["arc_to"], "arc_kind": a["arc_kind"],
+            "arc_timing": a["arc_timing"], "arc_net": a["arc_net"], "arc_node": a["arc_node"],
+            "fanin_start": fanin_start, "fanin": fanin, "fanout_start": fanout_start,
+            "fanout": fanout, "test_arc": test_arc, "test_start": test_start,
+            "test_of_pin": test_of_pin, "timing": a["timing"], "lut_meta": a["lut_meta"],
+        }
+        t = lambda x, dt: torch.from_numpy(  # noqa: E731
+            np.ascontiguousarray(x, dt).reshape(-1) if np.size(x) else np.zeros(1, dt)).to(device)
+        self.dev = {k: t(v, np.int32) for k, v in host.items()}
+        for k in ("pi_at", "pi_slew", "po_rat", "lut_data"):
+            self.dev[k] = t(a[k], np.float32)
+        self.graph = PropGraph(P, A, len(test_arc),
+                               *[self.dev[k].data_ptr() for k in
+                                 ["arc_from", "arc_to", "arc_kind", "arc_timing", "arc_net",
+                                  "arc_node", "fanin_start", "fanin", "fanout_start", "fanout",
+                                  "test_arc", "test_start", "test_of_pin", "pi_at", "pi_slew",
+                                  "po_rat", "timing", "lut_meta", "lut_data"]],
+                               float(a["period"]))
+        # levels over the pin graph: a pin's level is its longest path to a pin
+        # without fanout (otg_levelize, the reference's frontier rule)
+        fin_src = np.asarray(a["arc_from"], np.int32)[fanin]
+        out_deg = np.diff(fanout_start).astype(np.int32)
+        frontier0 = np.nonzero(out_deg == 0)[0].astype(np.int32)
+        lb = LevelizeBatch(t(fanin_start, np.int32), t(fin_src, np.int32), t(out_deg, np.int32),
+                           t(frontier0, np.int32))
+        lb.run()
+        lb.check()
+        order, ends, _ = lb.result()
+        assert len(order) == P, "the timing graph has a cycle"
+        self.order = t(order, np.int32)
+        self.level_ends = np.ascontiguousarray(ends, np.int32)
+        self.num_levels = len(ends) - 1
+        ws = ctypes.c_size_t()
+        check("otg_prop_workspace_size", lib().otg_prop_workspace_size(A, len(test_arc),
+                                                                       ctypes.byref(ws)))
+        self.workspace = torch.empty(max(ws.value, 256), dtype=torch.uint8, device=device)
+        self.out = {k: torch.empty(P, NC, dtype=torch.float32, device=device)
+                    for k in ("at", "slew", "rat", "slack")}
+
+    def propagate(self, batch, stream=None):
+        """Forward and backward propagation on the RC outputs of `batch`
+        (an RcBatch whose forest the graph's net arcs refer to)."""
+        rc = PropRc(_ptr(batch.nodes_start).value, _ptr(batch.node2bfs).value,
+                    _ptr(batch.load).value, _ptr(batch.delay).value, _ptr(batch.impulse).value)
+        o = self.out
+        check("otg_propagate", lib().otg_propagate(
+            ctypes.byref(self.graph), ctypes.byref(rc), _ptr(self.order),
+            self.level_ends.ctypes.data, self.num_levels, _ptr(o["at"]), _ptr(o["slew"]),
+            _ptr(o["rat"]), _ptr(o["slack"]), _ptr(self.workspace), self.workspace.numel(),
+            _stream(stream)))
+        return self
+
+    def result(self):
+        import torch
+        torch.cuda.synchronize()
+        return {k: v.cpu().numpy() for k, v in self.out.items()}

@@ -1,8 +1,13 @@
 // ot_run.cpp -- runs the reference OpenTimer Timer on a design directory and
 // dumps its results.  TEST INFRASTRUCTURE ONLY (the full-update parity check).
 //
-//   ot_run <dir> cpu|cuda <out.txt>
+//   ot_run <dir> cpu|cuda <out.txt> [graph.txt]
 //
+// graph.txt (optional) is the Timer's timing graph, for the GPU propagation
+// check: pins, arcs (net arcs with their net, cell arcs with one timing
+// record per split), timing records (sense, edge, constraint flag, six
+// LUT ids), LUTs (variable order, indices, values), timing tests, the clock
+// period and the primary-input/-output assertions, all by pin index.
 // <dir> holds early.lib, late.lib, design.v, design.spef, design.timing.
 // The same Timer sources are linked twice (oracle/Makefile): with the
 // reference's own CUDA module (ot_run_ref) and with libotg in its place
@@ -49,9 +54,101 @@ static void put(FILE* f, std::optional<float> v) {
   else std::fprintf(f, " nan");
 }
 
+// ---- graph export
+static void opt4(FILE* f, const ot::TimingData<std::optional<float>, ot::MAX_SPLIT, ot::MAX_TRAN>& d) {
+  for (int el = 0; el < 2; ++el)
+    for (int rf = 0; rf < 2; ++rf) {
+      if (d[el][rf]) std::fprintf(f, " %.9g", *d[el][rf]);
+      else std::fprintf(f, " nan");
+    }
+}
+
+static void dump_graph(ot::Timer& timer, const char* path) {
+  FILE* f = std::fopen(path, "w");
+  if (!f) return;
+  std::unordered_map<const ot::Timing*, int> tid;
+  std::unordered_map<const ot::Lut*, int> lid;
+  std::vector<const ot::Timing*> timings;
+  std::vector<const ot::Lut*> luts;
+  auto lut_id = [&](const std::optional<ot::Lut>& l) -> int {
+    if (!l) return -1;
+    auto it = lid.find(&*l);
+    if (it != lid.end()) return it->second;
+    lid[&*l] = (int)luts.size();
+    luts.push_back(&*l);
+    return (int)luts.size() - 1;
+  };
+  auto timing_id = [&](const ot::Timing* t) -> int {
+    if (!t) return -1;
+    auto it = tid.find(t);
+    if (it != tid.end()) return it->second;
+    tid[t] = (int)timings.size();
+    timings.push_back(t);
+    return (int)timings.size() - 1;
+  };
+  // pins by index
+  std::vector<const ot::Pin*> pins(timer._pins.size(), nullptr);
+  for (auto& [name, pin] : timer._pins)
+    if (pin._idx < pins.size()) pins[pin._idx] = &pin;
+  for (size_t i = 0; i < pins.size(); ++i) {
+    const ot::Pin* p = pins[i];
+    if (!p) continue;
+    std::fprintf(f, "p %zu %s %s", i, p->name().c_str(), p->_net ? p->_net->name().c_str() : "-");
+    ot::TimingData<std::optional<float>, ot::MAX_SPLIT, ot::MAX_TRAN> none{};
+    opt4(f, p->primary_input() ? p->primary_input()->_at : none);
+    opt4(f, p->primary_input() ? p->primary_input()->_slew : none);
+    opt4(f, p->primary_output() ? p->primary_output()->_rat : none);
+    std::fprintf(f, "\n");
+  }
+  // arcs
+  std::unordered_map<const ot::Arc*, int> aid;
+  int k = 0;
+  for (auto& arc : timer._arcs) {
+    aid[&arc] = k;
+    std::fprintf(f, "a %d %zu %zu %d", k, arc._from._idx, arc._to._idx, arc._state);
+    if (auto net = std::get_if<ot::Net*>(&arc._handle)) {
+      std::fprintf(f, " net %s -1 -1\n", (*net)->name().c_str());
+    } else {
+      auto tv = std::get<ot::TimingView>(arc._handle);
+      std::fprintf(f, " cell - %d %d\n", timing_id(tv[ot::MIN]), timing_id(tv[ot::MAX]));
+    }
+    ++k;
+  }
+  for (auto& [name, pin] : timer._pins)
+    for (auto* test : pin._tests) std::fprintf(f, "s %d\n", aid[&test->_arc]);
+  for (size_t i = 0; i < timings.size(); ++i) {
+    const ot::Timing* t = timings[i];
+    const int sense = !t->sense ? 2 : (*t->sense == ot::TimingSense::POSITIVE_UNATE ? 0
+                                      : *t->sense == ot::TimingSense::NEGATIVE_UNATE ? 1 : 2);
+    const int edge = t->is_rising_edge_triggered() ? 1 : (t->is_falling_edge_triggered() ? 2 : 0);
+    const int l[6] = {lut_id(t->cell_rise), lut_id(t->cell_fall), lut_id(t->rise_transition),
+                      lut_id(t->fall_transition), lut_id(t->rise_constraint),
+                      lut_id(t->fall_constraint)};
+    std::fprintf(f, "t %zu %d %d %d %d %d %d %d %d %d\n", i, sense, edge, t->is_constraint() ? 1 : 0,
+                 l[0], l[1], l[2], l[3], l[4], l[5]);
+  }
+  for (size_t i = 0; i < luts.size(); ++i) {
+    const ot::Lut* l = luts[i];
+    // variable order: 0 = (slew | related, ...), 1 = (load | constrained, ...), -1 = no template
+    int var = -1;
+    if (l->lut_template && l->lut_template->variable1) {
+      const auto v = *l->lut_template->variable1;
+      var = (v == ot::LutVar::TOTAL_OUTPUT_NET_CAPACITANCE ||
+             v == ot::LutVar::CONSTRAINED_PIN_TRANSITION) ? 1 : 0;
+    }
+    std::fprintf(f, "l %zu %d %zu %zu", i, var, l->indices1.size(), l->indices2.size());
+    for (float x : l->indices1) std::fprintf(f, " %.9g", x);
+    for (float x : l->indices2) std::fprintf(f, " %.9g", x);
+    for (float x : l->table) std::fprintf(f, " %.9g", x);
+    std::fprintf(f, "\n");
+  }
+  if (!timer._clocks.empty()) std::fprintf(f, "c %.9g\n", timer._clocks.begin()->second._period);
+  std::fclose(f);
+}
+
 int main(int argc, char** argv) {
-  if (argc != 4) {
-    std::fprintf(stderr, "usage: %s <dir> cpu|cuda <out>\n", argv[0]);
+  if (argc != 4 && argc != 5) {
+    std::fprintf(stderr, "usage: %s <dir> cpu|cuda <out> [graph]\n", argv[0]);
     return 2;
   }
   const std::string dir = argv[1];
@@ -135,5 +232,6 @@ int main(int argc, char** argv) {
     }
   }
   std::fclose(f);
+  if (argc == 5) dump_graph(timer, argv[4]);
   return 0;
 }

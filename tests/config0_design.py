@@ -20,8 +20,9 @@ writes into `dirpath`:
                         rooted at the driver, R ~ U(0.5, 20) ohm, ground
                         C ~ U(0.1, 3) fF, RES lines shuffled with random
                         orientation.
-  design.timing         TAU15 assertions: a 1 ns clock, input arrival times
-                        and slews, output loads and required times.
+  design.timing         TAU15 assertions: a 1 ns clock (arriving at 0 rising,
+                        0.5 falling), input arrival times and slews, output
+                        loads and required times.
 
 The formats are the ones the reference's parsers read (Liberty, structural
 Verilog, SPEF, the TAU 2015 .timing file); every number is drawn here.
@@ -288,7 +289,7 @@ def write_design(dirpath, seed=2024, gates=2000):
     nets = {n: (drivers[n][0], drivers[n][1], sinks.get(n, [])) for n in drivers}
     with open(os.path.join(dirpath, "design.spef"), "w") as f:
         f.write(spef(rng, nets))
-    lines = ["clock clk 1.0"]
+    lines = ["clock clk 1.0", "at clk 0.0 0.5 0.0 0.5"]  # rise at 0, fall at half a period
     for p in ins:
         a = rng.uniform(0.0, 0.05)
         lines.append(f"at {p} {a:.4f} {a:.4f} {a:.4f} {a:.4f}")
