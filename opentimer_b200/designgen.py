@@ -35,18 +35,26 @@ SLEW_IDX = [0.01, 0.02, 0.05, 0.1, 0.2, 0.5, 1.0]   # ns
 LOAD_IDX = [1.0, 2.0, 5.0, 10.0, 20.0, 50.0, 100.0]   # fF
 
 
+def f32(x):
+    """Values as the parsers will hold them: float32, written with 9
+    significant digits (which read back as the same float32)."""
+    return np.asarray(x, np.float64).astype(np.float32)
+
+
 def _fmt_row(r):
-    return ", ".join(f"{x:.6f}" for x in r)
+    return ", ".join(f"{float(x):.9g}" for x in f32(r))
 
 
 def _table(rng, a, b, c, scale):
     s = np.array(SLEW_IDX)[:, None]
     ld = np.array(LOAD_IDX)[None, :]
     base = (a + b * s + c * ld) * scale
-    return base * (1.0 + rng.uniform(-0.1, 0.1, base.shape))
+    return f32(base * (1.0 + rng.uniform(-0.1, 0.1, base.shape)))
 
 
-def _lut(name, tmpl, vals):
+def _lut(name, tmpl, vals, groups=None):
+    if groups is not None:
+        groups[name] = vals
     rows = ", \\\n          ".join(f'"{_fmt_row(r)}"' for r in vals)
     return (f"      {name}({tmpl}) {{\n"
             f'        index_1 ("{_fmt_row(SLEW_IDX)}");\n'
@@ -55,49 +63,60 @@ def _lut(name, tmpl, vals):
             f"      }}\n")
 
 
-def _arc(rng, related, sense, scale, kind=None):
+def _arc(rng, related, sense, scale, kind=None, groups=None):
     # delay ~ a + b*slew + c*load (ns, fF), transition likewise
     a, b, c = rng.uniform(0.01, 0.03), rng.uniform(0.1, 0.3), rng.uniform(0.002, 0.006)
     ta, tb, tc = rng.uniform(0.005, 0.02), rng.uniform(0.05, 0.2), rng.uniform(0.004, 0.01)
+    g = {"related": related, "sense": sense, "type": kind} if groups is not None else None
     out = "    timing() {\n"
     out += f'      related_pin : "{related}";\n'
     out += f"      timing_sense : {sense};\n"
     if kind:
         out += f"      timing_type : {kind};\n"
-    out += _lut("cell_rise", "tbl7x7", _table(rng, a, b, c, scale))
-    out += _lut("cell_fall", "tbl7x7", _table(rng, a * 0.9, b, c * 1.1, scale))
-    out += _lut("rise_transition", "tbl7x7", _table(rng, ta, tb, tc, scale))
-    out += _lut("fall_transition", "tbl7x7", _table(rng, ta * 1.1, tb, tc, scale))
+    out += _lut("cell_rise", "tbl7x7", _table(rng, a, b, c, scale), g)
+    out += _lut("cell_fall", "tbl7x7", _table(rng, a * 0.9, b, c * 1.1, scale), g)
+    out += _lut("rise_transition", "tbl7x7", _table(rng, ta, tb, tc, scale), g)
+    out += _lut("fall_transition", "tbl7x7", _table(rng, ta * 1.1, tb, tc, scale), g)
     out += "    }\n"
+    if groups is not None:
+        groups.append(g)
     return out
 
 
-def _constraint(rng, kind, scale):
+def _constraint(rng, kind, scale, groups=None):
     a = rng.uniform(0.02, 0.05) if kind == "setup_rising" else rng.uniform(0.005, 0.015)
+    g = {"related": "CK", "sense": None, "type": kind}
     out = "    timing() {\n"
     out += '      related_pin : "CK";\n'
     out += f"      timing_type : {kind};\n"
     for name in ("rise_constraint", "fall_constraint"):
         vals = _table(rng, a, 0.05, 0.0, scale)
+        g[name] = vals
         rows = ", \\\n          ".join(f'"{_fmt_row(r)}"' for r in vals)
         out += (f"      {name}(cons7x7) {{\n"
                 f'        index_1 ("{_fmt_row(SLEW_IDX)}");\n'
                 f'        index_2 ("{_fmt_row(SLEW_IDX)}");\n'
                 f"        values ( \\\n          {rows});\n      }}\n")
     out += "    }\n"
+    if groups is not None:
+        groups.append(g)
     return out
 
 
 def _pin_in(name, cap, clock=False):
-    s = f"  pin({name}) {{\n    direction : input;\n    capacitance : {cap:.6f};\n"
+    s = f"  pin({name}) {{\n    direction : input;\n    capacitance : {float(cap):.9g};\n"
     if clock:
         s += "    clock : true;\n"
     return s
 
 
-def liberty(seed, scale, name):
+def liberty(seed, scale, name, cells=None):
+    """Liberty text; with `cells` (a dict), also fills cells[cell] = {
+    "caps": {pin: cap}, "timings": {output pin: [timing groups]}}."""
     rng = np.random.default_rng(seed)  # same seed for both corners: same shapes
-    caps = rng.uniform(1.0, 3.0, 16)
+    caps = f32(rng.uniform(1.0, 3.0, 16))
+    if cells is None:
+        cells = {}
     out = [f"library({name}) {{",
            "  delay_model : table_lookup;",
            '  time_unit : "1ns";',
@@ -128,24 +147,30 @@ def liberty(seed, scale, name):
            "  }"]
     text = "\n".join(out) + "\n"
     # INV_X1
+    inv = cells["INV_X1"] = {"caps": {"A": caps[0]}, "timings": {"ZN": []}}
     text += "cell(INV_X1) {\n  area : 1;\n" + _pin_in("A", caps[0]) + "  }\n"
     text += '  pin(ZN) {\n    direction : output;\n    function : "(!A)";\n'
-    text += _arc(rng, "A", "negative_unate", scale) + "  }\n}\n"
+    text += _arc(rng, "A", "negative_unate", scale, groups=inv["timings"]["ZN"]) + "  }\n}\n"
     # NAND2_X1, NOR2_X1
     for k, (cell, fn) in enumerate([("NAND2_X1", "(!(A1 A2))"), ("NOR2_X1", "(!(A1+A2))")]):
+        c = cells[cell] = {"caps": {"A1": caps[1 + 2 * k], "A2": caps[2 + 2 * k]},
+                           "timings": {"ZN": []}}
         text += f"cell({cell}) {{\n  area : 2;\n"
         text += _pin_in("A1", caps[1 + 2 * k]) + "  }\n" + _pin_in("A2", caps[2 + 2 * k]) + "  }\n"
         text += f'  pin(ZN) {{\n    direction : output;\n    function : "{fn}";\n'
-        text += _arc(rng, "A1", "negative_unate", scale) + _arc(rng, "A2", "negative_unate", scale)
+        text += _arc(rng, "A1", "negative_unate", scale, groups=c["timings"]["ZN"])
+        text += _arc(rng, "A2", "negative_unate", scale, groups=c["timings"]["ZN"])
         text += "  }\n}\n"
     # DFF_X1
+    ff = cells["DFF_X1"] = {"caps": {"CK": caps[5], "D": caps[6]}, "timings": {"D": [], "Q": []}}
     text += "cell(DFF_X1) {\n  area : 5;\n"
     text += '  ff(IQ, IQN) {\n    next_state : "D";\n    clocked_on : "CK";\n  }\n'
     text += _pin_in("CK", caps[5], clock=True) + "  }\n"
-    text += _pin_in("D", caps[6]) + _constraint(rng, "setup_rising", scale)
-    text += _constraint(rng, "hold_rising", scale) + "  }\n"
+    text += _pin_in("D", caps[6]) + _constraint(rng, "setup_rising", scale, ff["timings"]["D"])
+    text += _constraint(rng, "hold_rising", scale, ff["timings"]["D"]) + "  }\n"
     text += '  pin(Q) {\n    direction : output;\n    function : "IQ";\n'
-    text += _arc(rng, "CK", "non_unate", scale, kind="rising_edge") + "  }\n}\n"
+    text += _arc(rng, "CK", "non_unate", scale, kind="rising_edge",
+                 groups=ff["timings"]["Q"]) + "  }\n}\n"
     text += "}\n"
     return text
 
@@ -256,13 +281,16 @@ def spef(rng, nets):
     return "\n".join(out) + "\n"
 
 
-def write_design(dirpath, seed=2024, gates=2000):
+def write_design(dirpath, seed=2024, gates=2000, keep=None):
+    """Writes the design files; returns a summary.  With `keep` (a dict), it
+    also receives the in-memory design for timing_graph/pin_caps."""
     rng = np.random.default_rng(seed)
     os.makedirs(dirpath, exist_ok=True)
+    libs = {"early": {}, "late": {}}
     with open(os.path.join(dirpath, "late.lib"), "w") as f:
-        f.write(liberty(seed + 1, 1.0, "late"))
+        f.write(liberty(seed + 1, 1.0, "late", libs["late"]))
     with open(os.path.join(dirpath, "early.lib"), "w") as f:
-        f.write(liberty(seed + 1, 0.9, "early"))
+        f.write(liberty(seed + 1, 0.9, "early", libs["early"]))
     glist, ins, outs = netlist(rng, gates)
     vtext, po_chain = verilog(glist, ins, outs)
     with open(os.path.join(dirpath, "design.v"), "w") as f:
@@ -289,16 +317,152 @@ def write_design(dirpath, seed=2024, gates=2000):
     nets = {n: (drivers[n][0], drivers[n][1], sinks.get(n, [])) for n in drivers}
     with open(os.path.join(dirpath, "design.spef"), "w") as f:
         f.write(spef(rng, nets))
-    lines = ["clock clk 1.0", "at clk 0.0 0.5 0.0 0.5"]  # rise at 0, fall at half a period
+    period = 1.0
+    assert_at, assert_slew, assert_rat, assert_load = {}, {}, {}, {}
+    assert_at["clk"] = f32([0.0, 0.5, 0.0, 0.5])  # rise at 0, fall at half a period
     for p in ins:
-        a = rng.uniform(0.0, 0.05)
-        lines.append(f"at {p} {a:.4f} {a:.4f} {a:.4f} {a:.4f}")
-        s = rng.uniform(0.01, 0.1)
-        lines.append(f"slew {p} {s:.4f} {s:.4f} {s:.4f} {s:.4f}")
-    lines.append("slew clk 0.02 0.02 0.02 0.02")
+        assert_at[p] = f32([rng.uniform(0.0, 0.05)] * 4)
+        assert_slew[p] = f32([rng.uniform(0.01, 0.1)] * 4)
+    assert_slew["clk"] = f32([0.02] * 4)
     for i in range(len(outs)):
-        lines.append(f"load out{i} 4.0")
-        lines.append(f"rat out{i} 0.0 0.0 1.0 1.0")
+        assert_load[f"out{i}"] = f32([4.0] * 4)
+        assert_rat[f"out{i}"] = f32([0.0, 0.0, 1.0, 1.0])
+    v = lambda x: " ".join(f"{float(t):.9g}" for t in x)  # noqa: E731
+    lines = [f"clock clk {period}"]
+    for p, x in assert_at.items():
+        lines.append(f"at {p} {v(x)}")
+    for p, x in assert_slew.items():
+        lines.append(f"slew {p} {v(x)}")
+    for p in assert_load:
+        lines.append(f"load {p} {v(assert_load[p][:1])}")
+        lines.append(f"rat {p} {v(assert_rat[p])}")
     with open(os.path.join(dirpath, "design.timing"), "w") as f:
         f.write("\n".join(lines) + "\n")
+    if keep is not None:
+        gates_all = list(glist) + [(a, "INV_X1", {"A": s, "ZN": mid}) for a, s, mid, _, _ in po_chain]
+        gates_all += [(b, "INV_X1", {"A": mid, "ZN": po}) for _, _, mid, b, po in po_chain]
+        keep.update(libs=libs, gates=gates_all, ports_in=ins + ["clk"],
+                    ports_out=[f"out{i}" for i in range(len(outs))], nets=nets,
+                    at=assert_at, slew=assert_slew, rat=assert_rat, load=assert_load,
+                    period=period)
     return {"gates": len(glist) + 2 * len(outs), "nets": len(nets)}
+
+
+_SENSE = {"positive_unate": 0, "negative_unate": 1}
+_MIN_CONSTRAINT = {"hold_rising", "hold_falling"}
+_MAX_CONSTRAINT = {"setup_rising", "setup_falling"}
+_LUTS = ["cell_rise", "cell_fall", "rise_transition", "fall_transition", "rise_constraint",
+         "fall_constraint"]
+
+
+def timing_graph(design):
+    """The timing graph of a kept design in the otg_prop_graph layout, by
+    the Timer's construction rules: a net arc from each net's driver to
+    each of its other pins; per split (early library for MIN, late for
+    MAX) one cell arc per timing group of each gate's cell, leaving out
+    setup checks on MIN and hold checks on MAX, and a timing test on every
+    constraint arc (ot/timer/timer.cpp:240-268, ot/timer/celllib.cpp:6-23).
+    Returns (arrays, pin_names, pin_net_names); net arcs carry the net's
+    name in `arc_net_name` and their sink pin in `arc_to`, for the caller
+    to resolve against its RC forest."""
+    pins, index = [], {}
+
+    def pin(name):
+        if name not in index:
+            index[name] = len(pins)
+            pins.append(name)
+        return index[name]
+
+    pin_net = {}
+    for p in design["ports_in"] + design["ports_out"]:
+        pin(p)
+    for inst, cell, conn in design["gates"]:
+        for cp, net in conn.items():
+            pin_net[pin(f"{inst}:{cp}")] = net
+    for p in design["ports_in"] + design["ports_out"]:
+        pin_net[index[p]] = p
+    arc_from, arc_to, arc_kind, arc_timing, arc_net_name, tests = [], [], [], [], [], []
+    for name, (drv, _, sinks) in sorted(design["nets"].items()):
+        for s, _ in sinks:
+            arc_from.append(index[drv])
+            arc_to.append(index[s])
+            arc_kind.append(0)
+            arc_timing.append((-1, -1))
+            arc_net_name.append(name)
+    # timing records and look-up tables, per library and group
+    timing, lut_meta, lut_data, off = [], [], [], 0
+    rec = {}
+
+    def lut_id(vals, cons):
+        nonlocal off
+        v = f32(vals)
+        idx1 = f32(SLEW_IDX)
+        idx2 = f32(SLEW_IDX) if cons else f32(LOAD_IDX)
+        lut_meta.append((len(idx1), len(idx2), off, 0))  # variable_1: input / related slew
+        lut_data.extend([idx1, idx2, v.reshape(-1)])
+        off += len(idx1) + len(idx2) + v.size
+        return len(lut_meta) - 1
+
+    def record(lib, cell, cp, k, g):
+        key = (lib, cell, cp, k)
+        if key not in rec:
+            t = g["type"] or ""
+            edge = 1 if t.endswith("rising") or t == "rising_edge" else (
+                2 if t.endswith("falling") or t == "falling_edge" else 0)
+            cons = t in _MIN_CONSTRAINT or t in _MAX_CONSTRAINT
+            luts = [lut_id(g[n], cons) if n in g else -1 for n in _LUTS]
+            timing.append([_SENSE.get(g["sense"], 2), edge, int(cons)] + luts)
+            rec[key] = len(timing) - 1
+        return rec[key]
+
+    for el, lib in ((0, "early"), (1, "late")):
+        cells = design["libs"][lib]
+        for inst, cell, conn in design["gates"]:
+            for cp, groups in cells[cell]["timings"].items():
+                for k, g in enumerate(groups):
+                    t = g["type"] or ""
+                    if (el == 0 and t in _MAX_CONSTRAINT) or (el == 1 and t in _MIN_CONSTRAINT):
+                        continue
+                    tm = [-1, -1]
+                    tm[el] = record(lib, cell, cp, k, g)
+                    arc_from.append(index[f"{inst}:{g['related']}"])
+                    arc_to.append(index[f"{inst}:{cp}"])
+                    arc_kind.append(1)
+                    arc_timing.append(tuple(tm))
+                    arc_net_name.append(None)
+                    if t in _MIN_CONSTRAINT or t in _MAX_CONSTRAINT:
+                        tests.append(len(arc_from) - 1)
+    P = len(pins)
+    nan4 = lambda: np.full((P, 4), np.nan, np.float32)  # noqa: E731
+    pi_at, pi_slew, po_rat = nan4(), nan4(), nan4()
+    for p, x in design["at"].items():
+        pi_at[index[p]] = x
+    for p, x in design["slew"].items():
+        pi_slew[index[p]] = x
+    for p, x in design["rat"].items():
+        po_rat[index[p]] = x
+    arrays = {"num_pins": P, "arc_from": np.array(arc_from, np.int32),
+              "arc_to": np.array(arc_to, np.int32), "arc_kind": np.array(arc_kind, np.int32),
+              "arc_timing": np.array(arc_timing, np.int32).reshape(-1, 2),
+              "test_arc": np.array(tests, np.int32), "pi_at": pi_at, "pi_slew": pi_slew,
+              "po_rat": po_rat, "timing": np.array(timing, np.int32),
+              "lut_meta": np.array(lut_meta, np.int32),
+              "lut_data": np.concatenate(lut_data).astype(np.float32),
+              "period": design["period"], "arc_net_name": arc_net_name}
+    return arrays, pins, [pin_net.get(i) for i in range(P)]
+
+
+def pin_caps(design):
+    """Per pin name, the capacitance the flat RC path adds at its node
+    (Pin::cap, ot/timer/pin.cpp:286-305): a primary output's load, an
+    instance pin's library capacitance (the same in both libraries here),
+    0 for a primary input."""
+    caps = {p: f32([0.0] * 4) for p in design["ports_in"]}
+    for p, x in design["load"].items():
+        caps[p] = x
+    cells = design["libs"]["late"]
+    for inst, cell, conn in design["gates"]:
+        for cp in conn:
+            c = cells[cell]["caps"].get(cp)
+            caps[f"{inst}:{cp}"] = f32([c if c is not None else 0.0] * 4)
+    return caps

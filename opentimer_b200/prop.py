@@ -111,3 +111,45 @@ class TimingGraph:
         import torch
         torch.cuda.synchronize()
         return {k: v.cpu().numpy() for k, v in self.out.items()}
+
+
+def rc_inputs(spef, pin_caps):
+    """Flat RC inputs from read_spef's output plus each non-root pin's cap
+    (pin_caps: name -> [4]), as the flat path adds them (ot/timer/
+    net.cpp:433-446).  Returns (cap [V,4], node_of {(net, pin name):
+    global node})."""
+    ns, ps = spef["nodes_start"], spef["pins_start"]
+    cap = spef["cap"].copy()
+    node_of = {}
+    names = spef["pin_names"]
+    for i in range(len(ns) - 1):
+        b = int(ns[i])
+        for q in range(ps[i], ps[i + 1]):
+            node = int(spef["pin_node"][q])
+            if node < 0:
+                continue
+            node_of[(i, names[q])] = b + node
+            if node != spef["roots"][i] and names[q] in pin_caps:
+                cap[b + node] = cap[b + node] + np.asarray(pin_caps[names[q]], np.float32)
+    return cap, node_of
+
+
+def attach_nets(arrays, pin_names, pin_net_names, spef, node_of):
+    """Fills arc_net / arc_node of a graph whose net arcs name their net
+    (arrays["arc_net_name"]): a net arc gets its forest net and its sink's
+    RC node, a cell arc the forest net of the pin it drives (its load)."""
+    net_idx = {n: i for i, n in enumerate(spef["net_names"])}
+    A = len(arrays["arc_from"])
+    arc_net = np.full(A, -1, np.int32)
+    arc_node = np.full(A, -1, np.int32)
+    for k in range(A):
+        to = int(arrays["arc_to"][k])
+        if arrays["arc_kind"][k] == 0:
+            i = net_idx[arrays["arc_net_name"][k]]
+            arc_net[k] = i
+            arc_node[k] = node_of.get((i, pin_names[to]), -1)
+        else:
+            arc_net[k] = net_idx.get(pin_net_names[to], -1)
+    out = dict(arrays)
+    out["arc_net"], out["arc_node"] = arc_net, arc_node
+    return out

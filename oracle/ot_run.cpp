@@ -25,6 +25,7 @@
 // FlatRctStorage arrays in BFS order (cuda), the node's local id being
 // rebuilt with the flat path's first-appearance rule over the SPEF RES
 // lines (ot/timer/net.cpp:388-410).
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <string>
@@ -160,7 +161,11 @@ int main(int argc, char** argv) {
       .read_spef(dir + "/design.spef")
       .read_timing(dir + "/design.timing");
   timer.cuda(cuda);
+  const auto t0 = std::chrono::steady_clock::now();
   timer.update_timing();
+  const double secs =
+      std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  std::printf("update_timing_s %.6f\n", secs);
 
   FILE* f = std::fopen(argv[3], "w");
   if (!f) return 3;

@@ -21,7 +21,7 @@ import subprocess
 import numpy as np
 import pytest
 
-import config0_design
+from opentimer_b200 import designgen as config0_design
 
 pytestmark = pytest.mark.gpu
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))

@@ -13,7 +13,7 @@ import subprocess
 import numpy as np
 import pytest
 
-import config0_design
+from opentimer_b200 import designgen as config0_design
 import opentimer_b200 as otg
 
 pytestmark = pytest.mark.gpu
@@ -158,3 +158,33 @@ def test_propagation_matches_reference_timer(design):
           f"{w_gpu}, vs CPU path {w_cpu}")
     assert max(w_gpu.values()) <= 1.0 and max(w_cpu.values()) <= 1.0
     assert np.isfinite(out["slack"]).sum() > 10000
+
+
+def test_own_graph_matches_reference_timer(design, tmp_path):
+    """The same check with nothing from the reference on the input side:
+    the design's timing graph as the generator builds it by the Timer's
+    construction rules (designgen.timing_graph), the library pin caps from
+    the generator, the SPEF reader, the RC pass and the propagation."""
+    import torch
+    from opentimer_b200 import designgen
+    from opentimer_b200.prop import TimingGraph, attach_nets, rc_inputs
+    from opentimer_b200.spef import read_spef
+    _, _, _, ref_gpu, ref_cpu = design
+    keep = {}
+    d = str(tmp_path)
+    designgen.write_design(d, seed=2024, gates=2000, keep=keep)
+    arrays, names, nets = designgen.timing_graph(keep)
+    f = read_spef(os.path.join(d, "design.spef"), r_scale=np.float32(1e-3))
+    cap, node_of = rc_inputs(f, designgen.pin_caps(keep))
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()  # noqa: E731
+    batch = otg.RcBatch(t(f["nodes_start"]), t(f["edges"].copy()), t(f["roots"]), t(f["res"]),
+                        t(cap))
+    batch.run()
+    batch.check()
+    g = TimingGraph(attach_nets(arrays, names, nets, f, node_of))
+    out = g.propagate(batch).result()
+    out["rat"] = np.where(np.isnan(out["at"]), np.nan, out["rat"])
+    w_gpu = compare(names, out, ref_gpu)
+    w_cpu = compare(names, out, ref_cpu)
+    print(f"own graph: err/tol vs reference GPU path {w_gpu}, vs CPU path {w_cpu}")
+    assert max(w_gpu.values()) <= 1.0 and max(w_cpu.values()) <= 1.0

@@ -9,7 +9,7 @@ import os
 import numpy as np
 import pytest
 
-import config0_design
+from opentimer_b200 import designgen as config0_design
 import oracle as O
 from opentimer_b200.spef import read_spef
 
