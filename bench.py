@@ -33,6 +33,8 @@ SEED = 2024
 LV_PINS, LV_EDGES, LV_LEVELS = 5_000_000, 12_000_000, 200
 TUNE_NETS = 50_000
 SPEF_NETS = 20_000
+FU_GATES = 50_000
+FU_REPS = 5
 # incremental sizing loop
 INC_GATES, INC_ITERS, INC_FRAC, INC_PLAIN_ITERS, INC_CHECK = 200_000, 1000, 0.005, 20, True
 # serving
@@ -355,6 +357,8 @@ def run_ours(args, world, rank, local):
         line["serving"] = run_serving()
     if rank == 0 and not args.no_spef:
         line["spef_ingest"] = run_spef()
+    if world == 1 and not args.no_full_update:
+        line["full_update"] = run_full_update()
     return line
 
 
@@ -609,6 +613,114 @@ def run_spef():
             "reference": ref}
 
 
+def pin_err(got, ref):
+    """Worst |got - ref| / (1e-5 |ref| + 1e-5) over pins and quantities
+    (inf where one side has a value the other lacks)."""
+    worst = 0.0
+    for name, r in ref.items():
+        g = got[name]
+        m = ~np.isnan(r)
+        if not np.array_equal(m, ~np.isnan(g)):
+            return float("inf")
+        if m.any():
+            worst = max(worst, float(np.max(np.abs(g[m] - r[m]) / (1e-5 * np.abs(r[m]) + 1e-5))))
+    return worst
+
+
+def run_full_update(dump=None):
+    """A full timing update on the GPU for a seeded gate-level design
+    (designgen: 4-cell library with 7x7 NLDM tables, a random DAG with 5%
+    flops, one RC tree per net): SPEF read into the flat layout, the fused
+    RC pass, and levelized propagation of slew/delay/arrival/required time
+    and slack over the design's timing graph.  The reference Timer's own
+    update_timing on the same files (oracle/_ref/ot_run_ref, its CPU path,
+    all host threads) is timed beside it, and every pin's results are
+    compared."""
+    import subprocess
+    import tempfile
+    import torch
+    import opentimer_b200 as otg
+    from opentimer_b200 import designgen
+    from opentimer_b200.prop import TimingGraph, attach_nets, rc_inputs
+    from opentimer_b200.spef import read_spef
+    out = {}
+    with tempfile.TemporaryDirectory() as d:
+        keep = {}
+        info = designgen.write_design(d, seed=SEED + 30, gates=FU_GATES, keep=keep)
+        arrays, names, nets = designgen.timing_graph(keep)
+        caps = designgen.pin_caps(keep)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        t0 = time.perf_counter()
+        f = read_spef(os.path.join(d, "design.spef"), r_scale=np.float32(1e-3))
+        t_spef = time.perf_counter() - t0
+        cap, node_of = rc_inputs(f, caps)
+        graph = TimingGraph(attach_nets(arrays, names, nets, f, node_of))
+        t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()  # noqa: E731
+        batch = otg.RcBatch(t(f["nodes_start"]), t(f["edges"].copy()), t(f["roots"]),
+                            t(f["res"]), t(cap))
+        for _ in range(3):  # warm-up
+            batch.run()
+            graph.propagate(batch)
+        graph.check()
+        rc_t, prop_t = [], []
+        for _ in range(FU_REPS):
+            torch.cuda.synchronize()
+            ev[0].record()
+            batch.run()
+            ev[1].record()
+            graph.propagate(batch)
+            ev[2].record()
+            torch.cuda.synchronize()
+            rc_t.append(ev[0].elapsed_time(ev[1]))
+            prop_t.append(ev[1].elapsed_time(ev[2]))
+        batch.check()
+        res = graph.result()
+        res["rat"] = np.where(np.isnan(res["at"]), np.nan, res["rat"])
+        rc_ms, prop_ms = float(np.median(rc_t)), float(np.median(prop_t))
+        out = {"workload": f"{info['gates']} gates, {info['nets']} nets, {graph.P} pins, "
+                           f"{graph.A} arcs, {graph.num_levels} levels",
+               "gpu_ms": rc_ms + prop_ms, "rc_pass_ms": rc_ms, "propagation_ms": prop_ms,
+               "timed": f"median of {FU_REPS}", "spef_read_ms": 1e3 * t_spef,
+               "levels": graph.num_levels, "launches_per_propagation": 1}
+        exe = os.path.join(ROOT, "oracle", "_ref", "ot_run_ref")
+        if os.path.exists(exe):
+            ours = {n: np.stack([res[k][i] for k in ("at", "slew", "rat", "slack")])
+                    for i, n in enumerate(names)}
+            ref = {}
+            for mode in ("cpu", "cuda"):
+                ref_out = os.path.join(d, f"ref_{mode}.txt")
+                p = subprocess.run([exe, d, mode, ref_out], capture_output=True, text=True,
+                                   timeout=600)
+                secs = [float(x.split()[1]) for x in p.stdout.splitlines()
+                        if x.startswith("update_timing_s")]
+                if p.returncode != 0 or not secs:
+                    continue
+                pins = {}
+                with open(ref_out) as fh:
+                    for line in fh:
+                        if line.startswith("P "):
+                            tk = line.split()
+                            pins[tk[1]] = np.array([float(x) for x in tk[2:]]).reshape(4, 4)
+                ref[mode] = (1e3 * secs[0], pins)
+            if dump is not None:  # the raw results, for a caller's own analysis
+                dump.update(names=names, ours=ours, ref={k: v[1] for k, v in ref.items()},
+                            order=graph.order.cpu().numpy(),
+                            level_ends=graph.level_ends.cpu().numpy())
+            if "cpu" in ref:
+                out["reference"] = {"update_timing_ms": ref["cpu"][0], "path": "CPU",
+                                    "threads": os.cpu_count(),
+                                    "what": "the reference Timer's update_timing (oracle/_ref)"}
+                out["pins_err_over_tol_vs_reference_cpu"] = pin_err(ours, ref["cpu"][1])
+            if "cuda" in ref:
+                out["reference_cuda_update_timing_ms"] = ref["cuda"][0]
+                out["pins_err_over_tol_vs_reference_cuda"] = pin_err(ours, ref["cuda"][1])
+                if "cpu" in ref:
+                    # the reference's own two paths against each other, same tolerance
+                    out["pins_err_over_tol_reference_cuda_vs_cpu"] = pin_err(ref["cuda"][1],
+                                                                             ref["cpu"][1])
+    return out
+
+
 def cpu_baseline(g, ns_np):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     threads = os.cpu_count() or 1
@@ -633,6 +745,7 @@ def main():
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--no-spef", action="store_true")
+    ap.add_argument("--no-full-update", action="store_true")
     # smaller cases (profiling); the defaults are the benchmark workload
     ap.add_argument("--nets", type=int, default=NUM_NETS)
     ap.add_argument("--min-nodes", type=int, default=2)

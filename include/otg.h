@@ -369,14 +369,18 @@ typedef struct otg_prop_rc {   /* outputs of otg_rc_timing for the design's nets
   const float* impulse;
 } otg_prop_rc;
 
-otg_status otg_prop_workspace_size(int32_t num_arcs, int32_t num_tests, size_t* bytes);
-/* order (device) and level_ends (HOST, num_levels+1 entries) are
- * otg_levelize's output over the graph's fanin CSR (pins without fanout
- * are level 0).  Writes at, slew, rat, slack [P][4].  Asynchronous. */
+otg_status otg_prop_workspace_size(int32_t num_pins, int32_t num_arcs, int32_t num_tests,
+                                   size_t* bytes);
+/* order (device, num_pins entries) is otg_levelize's output over the
+ * graph's fanin CSR: every pin after all of its fanout pins.  Writes at,
+ * slew, rat, slack [P][4].  lut_meta must be 16-byte aligned, the
+ * workspace 256-byte aligned.  One cooperative launch, dataflow-scheduled
+ * (per-pin ready flags, bounded waits); asynchronous.  otg_prop_status
+ * synchronizes the stream and returns OTG_ERR_TIMEOUT if a wait gave up. */
 otg_status otg_propagate(const otg_prop_graph* graph, const otg_prop_rc* rc,
-                         const int32_t* order, const int32_t* level_ends, int32_t num_levels,
-                         float* at, float* slew, float* rat, float* slack, void* workspace,
-                         size_t workspace_bytes, otg_stream_t stream);
+                         const int32_t* order, float* at, float* slew, float* rat, float* slack,
+                         void* workspace, size_t workspace_bytes, otg_stream_t stream);
+otg_status otg_prop_status(const void* workspace, otg_stream_t stream);
 
 /* Human-readable name of a status code. */
 const char* otg_status_string(otg_status s);

@@ -30,6 +30,7 @@ C_SYMBOLS = [
     "otg_rc_get_tuning", "otg_rc_set_tuning", "otg_rc_autotune",
     "otg_spef_read", "otg_spef_sizes", "otg_spef_fill", "otg_spef_pins", "otg_spef_net_name",
     "otg_spef_pin_name", "otg_spef_free", "otg_prop_workspace_size", "otg_propagate",
+    "otg_prop_status",
 ]
 # The reference-compatible C++ entry points (include/otg_compat.hpp), by
 # their Itanium-mangled names.
@@ -132,8 +133,9 @@ def lib():
         L.otg_spef_pin_name.argtypes = [P, I32, I32]
         L.otg_spef_pin_name.restype = ctypes.c_char_p
         L.otg_spef_free.argtypes = [P]
-        L.otg_prop_workspace_size.argtypes = [I32, I32, PS]
-        L.otg_propagate.argtypes = [P, P, P, P, I32, P, P, P, P, P, S, P]
+        L.otg_prop_workspace_size.argtypes = [I32, I32, I32, PS]
+        L.otg_propagate.argtypes = [P, P, P, P, P, P, P, P, S, P]
+        L.otg_prop_status.argtypes = [P, P]
         L.otg_spef_free.restype = None
         for name in ["otg_rc_workspace_size", "otg_rc_timing", "otg_rc_status", "otg_rc_timing_subset",
                      "otg_levelize_workspace_size", "otg_levelize", "otg_levelize_status",
@@ -144,7 +146,7 @@ def lib():
                      "otg_server_read", "otg_server_replay", "otg_server_stats",
                      "otg_rc_get_tuning", "otg_rc_set_tuning", "otg_rc_autotune",
                      "otg_spef_read", "otg_spef_sizes", "otg_spef_fill", "otg_spef_pins",
-                     "otg_prop_workspace_size", "otg_propagate"]:
+                     "otg_prop_workspace_size", "otg_propagate", "otg_prop_status"]:
             getattr(L, name).restype = ctypes.c_int
         _lib = L
     return _lib

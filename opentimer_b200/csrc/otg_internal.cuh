@@ -10,6 +10,60 @@ namespace otg {
 // Kernel-launch counter (reported by otg_kernel_launches()).
 void count_launch();
 
+// ---- bounded grid barrier of the cooperative kernels (levelization,
+// propagation).  Every wait gives up after kGridWaitNs of %globaltimer,
+// raises `abort` (which every other wait watches) and records
+// OTG_ERR_TIMEOUT, so a stuck launch returns instead of hanging.
+constexpr unsigned long long kGridWaitNs = 2000000000ull;  // 2 s per barrier wait
+
+struct GridCtl {
+  unsigned count;  // barrier arrivals
+  unsigned gen;    // barrier generation
+  int abort;       // set by a wait that timed out
+  int status;      // OTG_* status of the launch
+};
+
+__device__ __forceinline__ unsigned long long gtime() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Returns false if the barrier was abandoned (timeout somewhere).
+__device__ inline bool grid_barrier(GridCtl* c) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile GridCtl* vc = c;
+    int ok = 1;
+    const unsigned gen = vc->gen;
+    __threadfence();
+    const unsigned arrived = atomicAdd(&c->count, 1u);
+    if (arrived == gridDim.x - 1) {
+      c->count = 0;
+      __threadfence();
+      atomicAdd(&c->gen, 1u);
+    } else {
+      const unsigned long long t0 = gtime();
+      while (vc->gen == gen) {
+        if (vc->abort) { ok = 0; break; }
+        if (gtime() - t0 > kGridWaitNs) {
+          atomicExch(&c->abort, 1);
+          atomicCAS(&c->status, 0, (int)OTG_ERR_TIMEOUT);
+          ok = 0;
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+    if (vc->abort) ok = 0;
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
 // Per-net workspace of the block path, in bytes from the slice base.  The
 // slice is shared memory for nets that fit (16-bit indices), a per-CTA
 // slice of the caller's workspace otherwise (32-bit indices).  Regions:

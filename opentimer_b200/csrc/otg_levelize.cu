@@ -33,55 +33,7 @@ namespace {
 
 constexpr unsigned FULL = 0xffffffffu;
 constexpr int LT = 512;                              // threads per CTA
-constexpr unsigned long long kWaitNs = 2000000000ull;  // 2 s per barrier wait
-
-struct LvCtl {
-  unsigned count;   // barrier arrivals
-  unsigned gen;     // barrier generation
-  int abort;        // set by a wait that timed out
-  int status;       // OTG_* status of the launch
-};
-
-__device__ __forceinline__ unsigned long long gtime() {
-  unsigned long long t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
-
-// Returns false if the barrier was abandoned (timeout somewhere).
-__device__ bool grid_barrier(LvCtl* c) {
-  __shared__ int s_ok;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    volatile LvCtl* vc = c;
-    int ok = 1;
-    const unsigned gen = vc->gen;
-    __threadfence();
-    const unsigned arrived = atomicAdd(&c->count, 1u);
-    if (arrived == gridDim.x - 1) {
-      c->count = 0;
-      __threadfence();
-      atomicAdd(&c->gen, 1u);
-    } else {
-      const unsigned long long t0 = gtime();
-      while (vc->gen == gen) {
-        if (vc->abort) { ok = 0; break; }
-        if (gtime() - t0 > kWaitNs) {
-          atomicExch(&c->abort, 1);
-          atomicCAS(&c->status, 0, (int)OTG_ERR_TIMEOUT);
-          ok = 0;
-          break;
-        }
-        __nanosleep(64);
-      }
-    }
-    __threadfence();
-    if (vc->abort) ok = 0;
-    s_ok = ok;
-  }
-  __syncthreads();
-  return s_ok != 0;
-}
+using LvCtl = GridCtl;
 
 // Decrement the fanout counters of u's fanins; pins that become ready set
 // their bit in `bm`.  Lanes of a warp that target the same pin combine.

@@ -15,10 +15,21 @@
 // empty std::optional is NaN here.  Every add and multiply is an explicit
 // rounding intrinsic, so no compiler fusion changes a bit.
 //
-// Order: one launch per level, a thread per pin; the levels come from
-// otg_levelize over the same graph (a pin's fanins sit on higher levels,
-// its fanouts on lower ones), forward from the last level to the first,
-// backward from the first to the last.
+// Schedule: one cooperative launch, a warp per pin, dataflow instead of
+// level barriers.  Pins are numbered in level order (otg_levelize: every
+// pin after all of its fanouts); the forward pass takes them last level
+// first, warp w the items w, w+W, w+2W, ...  A pin waits (bounded) on the
+// ready flag of each fanin, computes, and raises its own flag.  Because a
+// pin depends only on lower-numbered items and each warp works through its
+// items in order, the lowest unfinished item always has every input ready:
+// the schedule cannot deadlock while all CTAs are resident, which the
+// cooperative launch guarantees.  One grid barrier separates the forward
+// pass from the backward pass, which runs the same way first level first.
+// Inside a warp the lanes split a pin's (arc, split, from-transition,
+// to-transition) combinations and reduce with shuffles; min/max reductions
+// are order-free, so the lane split does not change a value.  Values that
+// other warps wrote in the launch are read with __ldcg (L2); the graph and
+// the library are read-only for the launch and go through __ldg.
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
@@ -51,27 +62,9 @@ __device__ int lower_bound(const float* a, int n, float v) {
   int lo = 0, hi = n;
   while (lo < hi) {
     const int mid = (lo + hi) >> 1;
-    if (a[mid] < v) lo = mid + 1; else hi = mid;
+    if (__ldg(a + mid) < v) lo = mid + 1; else hi = mid;
   }
   return lo;
-}
-
-// meta: n1, n2, offset, variable order (unused here)
-__device__ float lut_eval(const int* meta, const float* data, float v1, float v2) {
-  const int n1 = meta[0], n2 = meta[1];
-  const float* i1 = data + meta[2];
-  const float* i2 = i1 + n1;
-  const float* tb = i2 + n2;
-  if (n1 < 1 || n2 < 1) return nanf("");
-  if (n1 == 1 && n2 == 1) return tb[0];
-  const int a1 = max(1, min(lower_bound(i1, n1, v1), n1 - 1));
-  const int a2 = max(1, min(lower_bound(i2, n2, v2), n2 - 1));
-  if (n1 == 1) return interpolate(v2, i2[a2 - 1], i2[a2], tb[a2 - 1], tb[a2]);
-  if (n2 == 1) return interpolate(v1, i1[a1 - 1], i1[a1], tb[(a1 - 1) * n2], tb[a1 * n2]);
-  const float lo = interpolate(v1, i1[a1 - 1], i1[a1], tb[(a1 - 1) * n2 + a2 - 1],
-                               tb[a1 * n2 + a2 - 1]);
-  const float hi = interpolate(v1, i1[a1 - 1], i1[a1], tb[(a1 - 1) * n2 + a2], tb[a1 * n2 + a2]);
-  return interpolate(v2, i2[a2 - 1], i2[a2], lo, hi);
 }
 
 struct G {
@@ -79,272 +72,424 @@ struct G {
   otg_prop_rc rc;
 };
 
+constexpr unsigned FULL = 0xffffffffu;
+
+// A table chosen before the query values are known: lut_meta's (n1, n2,
+// offset, variable order), n1 = -1 for "no table".
+struct Lut {
+  int n1, n2, off, var;
+};
+
+__device__ __forceinline__ Lut no_lut() { return Lut{-1, 0, 0, 0}; }
+
+// Lut::operator() on (v1, v2) in the table's own axis order.
+__device__ float lut_eval(const Lut& m, const float* data, float v1, float v2) {
+  const int n1 = m.n1, n2 = m.n2;
+  const float* i1 = data + m.off;
+  const float* i2 = i1 + n1;
+  const float* tb = i2 + n2;
+  if (n1 < 1 || n2 < 1) return nanf("");
+  if (n1 == 1 && n2 == 1) return __ldg(tb);
+  const int a1 = max(1, min(lower_bound(i1, n1, v1), n1 - 1));
+  const int a2 = max(1, min(lower_bound(i2, n2, v2), n2 - 1));
+  if (n1 == 1)
+    return interpolate(v2, __ldg(i2 + a2 - 1), __ldg(i2 + a2), __ldg(tb + a2 - 1), __ldg(tb + a2));
+  const float x1 = __ldg(i1 + a1 - 1), x2 = __ldg(i1 + a1);
+  if (n2 == 1) return interpolate(v1, x1, x2, __ldg(tb + (a1 - 1) * n2), __ldg(tb + a1 * n2));
+  const float lo = interpolate(v1, x1, x2, __ldg(tb + (a1 - 1) * n2 + a2 - 1),
+                               __ldg(tb + a1 * n2 + a2 - 1));
+  const float hi = interpolate(v1, x1, x2, __ldg(tb + (a1 - 1) * n2 + a2),
+                               __ldg(tb + a1 * n2 + a2));
+  return interpolate(v2, __ldg(i2 + a2 - 1), __ldg(i2 + a2), lo, hi);
+}
+
 // timing record: [sense, edge, constraint, lut x6]
 __device__ bool transition_defined(const int* tr, int irf, int orf) {
-  const int edge = tr[1];
+  const int edge = __ldg(tr + 1), sense = __ldg(tr);
   if (edge == 1 && irf != RISE_) return false;
   if (edge == 2 && irf != FALL_) return false;
-  if (tr[0] == 0 && irf != orf) return false;  // positive unate
-  if (tr[0] == 1 && irf == orf) return false;  // negative unate
+  if (sense == 0 && irf != orf) return false;  // positive unate
+  if (sense == 1 && irf == orf) return false;  // negative unate
   return true;
 }
 
-// which = 0 delay, 1 slew, 2 constraint; (a, b) = (slew, load) for delay and
-// slew, (related slew, constrained slew) for constraint
-__device__ float timing_query(const G& G_, int t, int which, int irf, int orf, float a, float b) {
+// The table a Timing::delay/slew/constraint query of record t reads:
+// which = 0 delay, 1 slew, 2 constraint.
+__device__ Lut timing_lut(const G& G_, int t, int which, int irf, int orf) {
+  if (t < 0) return no_lut();
   const int* tr = G_.g.timing + 9 * t;
-  if (!transition_defined(tr, irf, orf)) return nanf("");
-  const int lut = tr[3 + 2 * which + orf];
-  if (lut < 0) return nanf("");
-  const int* meta = G_.g.lut_meta + 4 * lut;
-  const int var = meta[3];
-  if (var < 0) {  // no template: a scalar only
-    if (meta[0] == 1 && meta[1] == 1) return G_.g.lut_data[meta[2] + 2];
+  if (!transition_defined(tr, irf, orf)) return no_lut();
+  const int lut = __ldg(tr + 3 + 2 * which + orf);
+  if (lut < 0) return no_lut();
+  const int4 m = __ldg(reinterpret_cast<const int4*>(G_.g.lut_meta) + lut);
+  return Lut{m.x, m.y, m.z, m.w};
+}
+
+// The query itself; (a, b) = (slew, load) for delay and slew, (related
+// slew, constrained slew) for constraint.
+__device__ float timing_value(const G& G_, const Lut& m, float a, float b) {
+  if (m.n1 < 0) return nanf("");
+  if (m.var < 0) {  // no template: a scalar only
+    if (m.n1 == 1 && m.n2 == 1) return __ldg(G_.g.lut_data + m.off + 2);
     return nanf("");
   }
   // var 0: (slew | related) first; var 1: (load | constrained) first
-  return var == 0 ? lut_eval(meta, G_.g.lut_data, a, b) : lut_eval(meta, G_.g.lut_data, b, a);
-}
-
-__device__ __forceinline__ float rc_load(const G& G_, int net, int el, int trf) {
-  if (net < 0) return 0.0f;
-  return G_.rc.load[4 * (size_t)G_.rc.nodes_start[net] + 2 * el + trf];
+  return m.var == 0 ? lut_eval(m, G_.g.lut_data, a, b) : lut_eval(m, G_.g.lut_data, b, a);
 }
 
 // RC node of a net arc's sink: global BFS slot (-1: none)
 __device__ __forceinline__ int rc_slot(const G& G_, int arc) {
-  const int node = G_.g.arc_node[arc];
+  const int node = __ldg(G_.g.arc_node + arc);
   if (node < 0) return -1;
-  const int net = G_.g.arc_net[arc];
-  return G_.rc.nodes_start[net] + G_.rc.node2bfs[node];
+  const int net = __ldg(G_.g.arc_net + arc);
+  return __ldg(G_.rc.nodes_start + net) + __ldg(G_.rc.node2bfs + node);
 }
 
-__device__ __forceinline__ void relax_min(float& cur, float v) {
-  if (none(cur) || v < cur) cur = v;
-}
-__device__ __forceinline__ void relax_max(float& cur, float v) {
-  if (none(cur) || v > cur) cur = v;
+__device__ __forceinline__ int ld_acquire(const int* p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
 }
 
-__global__ void fprop_kernel(G G_, const int* order, int lo, int hi, float* at, float* slew,
-                             float* arc_delay, float* test_rat) {
-  const otg_prop_graph& g = G_.g;
-  for (int idx = lo + blockIdx.x * blockDim.x + threadIdx.x; idx < hi;
-       idx += gridDim.x * blockDim.x) {
-    const int v = order[idx];
-    float sl[4], a[4];
-    for (int c = 0; c < 4; ++c) {
-      sl[c] = g.pi_slew[4 * v + c];  // a primary input's assertion (NaN: none)
-      a[c] = g.pi_at[4 * v + c];
-    }
-    const int f0 = g.fanin_start[v], f1 = g.fanin_start[v + 1];
-    // slew
-    for (int k = f0; k < f1; ++k) {
-      const int arc = g.fanin[k], u = g.arc_from[arc];
-      if (g.arc_kind[arc] == 0) {
-        const int s = rc_slot(G_, arc);
-        for (int c = 0; c < 4; ++c) {
-          const float si = slew[4 * u + c];
-          if (none(si) || s < 0) continue;
-          const float imp = G_.rc.impulse[4 * (size_t)s + c];
-          const float r = sqrtf(__fadd_rn(__fmul_rn(si, si), imp));
-          const float so = si < 0.0f ? -r : r;
-          if (c < 2) relax_min(sl[c], so); else relax_max(sl[c], so);
-        }
-      } else {
-        for (int el = 0; el < 2; ++el) {
-          const int t = g.arc_timing[2 * arc + el];
-          if (t < 0) continue;
-          for (int frf = 0; frf < 2; ++frf) {
-            const float si = slew[4 * u + 2 * el + frf];
-            if (none(si)) continue;
-            for (int trf = 0; trf < 2; ++trf) {
-              const float so = timing_query(G_, t, 1, frf, trf, si,
-                                            rc_load(G_, g.arc_net[arc], el, trf));
-              if (none(so)) continue;
-              if (el == MIN_) relax_min(sl[2 * el + trf], so);
-              else relax_max(sl[2 * el + trf], so);
-            }
-          }
-        }
-      }
-    }
-    for (int c = 0; c < 4; ++c) slew[4 * v + c] = sl[c];
-    // arc delays and arrival times
-    for (int k = f0; k < f1; ++k) {
-      const int arc = g.fanin[k], u = g.arc_from[arc];
-      float* d = arc_delay + 8 * (size_t)arc;  // [el][frf][trf]
-      for (int j = 0; j < 8; ++j) d[j] = nanf("");
-      if (g.arc_kind[arc] == 0) {
-        const int s = rc_slot(G_, arc);
-        for (int el = 0; el < 2; ++el)
-          for (int rf = 0; rf < 2; ++rf)
-            d[4 * el + 2 * rf + rf] = s < 0 ? nanf("") : G_.rc.delay[4 * (size_t)s + 2 * el + rf];
-      } else {
-        for (int el = 0; el < 2; ++el) {
-          const int t = g.arc_timing[2 * arc + el];
-          if (t < 0) continue;
-          for (int frf = 0; frf < 2; ++frf) {
-            const float si = slew[4 * u + 2 * el + frf];
-            if (none(si)) continue;
-            for (int trf = 0; trf < 2; ++trf)
-              d[4 * el + 2 * frf + trf] =
-                  timing_query(G_, t, 0, frf, trf, si, rc_load(G_, g.arc_net[arc], el, trf));
-          }
-        }
-      }
-      for (int el = 0; el < 2; ++el)
-        for (int frf = 0; frf < 2; ++frf) {
-          const float fa = at[4 * u + 2 * el + frf];
-          if (none(fa)) continue;
-          for (int trf = 0; trf < 2; ++trf) {
-            const float dl = d[4 * el + 2 * frf + trf];
-            if (none(dl)) continue;
-            const float val = __fadd_rn(dl, fa);
-            if (el == MIN_) relax_min(a[2 * el + trf], val);
-            else relax_max(a[2 * el + trf], val);
-          }
-        }
-    }
-    for (int c = 0; c < 4; ++c) at[4 * v + c] = a[c];
-    // timing tests constrained at v (Test::_fprop_rat)
-    for (int k = g.test_start[v]; k < g.test_start[v + 1]; ++k) {
-      const int test = g.test_of_pin[k], arc = g.test_arc[test], u = g.arc_from[arc];
-      float* tr = test_rat + 4 * (size_t)test;
-      for (int c = 0; c < 4; ++c) tr[c] = nanf("");
-      if (none(g.period)) continue;
-      for (int el = 0; el < 2; ++el) {
-        const int t = g.arc_timing[2 * arc + el];
-        if (t < 0) continue;
-        const int edge = g.timing[9 * t + 1];
-        const int fel = el == MIN_ ? MAX_ : MIN_;
-        const int frf = edge == 1 ? RISE_ : FALL_;
-        if (frf == FALL_ && edge != 2) continue;
-        for (int rf = 0; rf < 2; ++rf) {
-          if (none(sl[2 * el + rf])) continue;
-          const float rat_at = at[4 * u + 2 * fel + frf], rsl = slew[4 * u + 2 * fel + frf];
-          if (none(rat_at) || none(rsl)) continue;
-          const float related = el == MIN_ ? rat_at : __fadd_rn(rat_at, g.period);
-          const float cons = timing_query(G_, t, 2, frf, rf, rsl, sl[2 * el + rf]);
-          if (none(cons)) continue;
-          tr[2 * el + rf] = el == MIN_ ? __fadd_rn(cons, related) : __fsub_rn(related, cons);
-        }
-      }
+__device__ __forceinline__ void st_release(int* p, int v) {
+  asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Bounded wait for a ready flag; false when this or another wait gave up.
+__device__ bool wait_ready(const int* flag, GridCtl* c) {
+  if (ld_acquire(flag)) return true;
+  const unsigned long long t0 = gtime();
+  for (;;) {
+    __nanosleep(32);
+    if (ld_acquire(flag)) return true;
+    if (*(volatile int*)&c->abort) return false;
+    if (gtime() - t0 > kGridWaitNs) {
+      atomicExch(&c->abort, 1);
+      atomicCAS(&c->status, 0, (int)OTG_ERR_TIMEOUT);
+      return false;
     }
   }
 }
 
-__global__ void bprop_kernel(G G_, const int* order, int lo, int hi, const float* at,
-                             float* rat, float* slack, const float* arc_delay,
-                             const float* test_rat) {
+// Order-free relax of Pin::_relax_slew/_relax_at (MIN keeps the smallest,
+// MAX the largest) and Pin::_relax_rat (the other way round); NaN is the
+// empty value and loses to any number.
+__device__ __forceinline__ float relax_fwd(int el, float cur, float v) {
+  return el == MIN_ ? fminf(cur, v) : fmaxf(cur, v);
+}
+__device__ __forceinline__ float relax_bwd(int el, float cur, float v) {
+  return el == MIN_ ? fmaxf(cur, v) : fminf(cur, v);
+}
+
+// Writes of this warp visible GPU-wide, then the pin's ready flag.
+__device__ __forceinline__ void publish(int* flag, int lane) {
+  __threadfence();
+  __syncwarp();
+  if (lane == 0) st_release(flag, 1);
+}
+
+// Forward at pin v (one warp): Timer::_fprop_slew, _fprop_delay, _fprop_at
+// and _fprop_test.  Lane j of a pass takes fanin arc j/8 and the combination
+// (el, frf, trf) = bits (2, 1, 0) of j; its slew and arrival candidates go to
+// output corner (el, trf).  Returns false if a wait gave up.
+__device__ bool fprop_warp(const G& G_, int v, int lane, float* at, float* slew, float* arc_delay,
+                           float* test_rat, int* fready, GridCtl* ctl) {
   const otg_prop_graph& g = G_.g;
-  for (int idx = lo + blockIdx.x * blockDim.x + threadIdx.x; idx < hi;
-       idx += gridDim.x * blockDim.x) {
-    const int v = order[idx];
-    float r[4];
-    for (int c = 0; c < 4; ++c) r[c] = g.po_rat[4 * v + c];  // a primary output's assertion
-    // Pin::_relax_rat: the MIN split keeps the largest, MAX the smallest
-    auto relax = [&](int el, int rf, float val) {
-      if (el == MIN_) relax_max(r[2 * el + rf], val);
-      else relax_min(r[2 * el + rf], val);
-    };
-    for (int k = g.test_start[v]; k < g.test_start[v + 1]; ++k) {
-      const float* tr = test_rat + 4 * (size_t)g.test_of_pin[k];
-      for (int c = 0; c < 4; ++c)
-        if (!none(tr[c])) relax(c >> 1, c & 1, tr[c]);
+  const int el = (lane >> 2) & 1, frf = (lane >> 1) & 1, trf = lane & 1;
+  const int c_out = 2 * el + trf;
+  const int f0 = __ldg(g.fanin_start + v), nitems = 8 * (__ldg(g.fanin_start + v + 1) - f0);
+  // a primary input's assertions (NaN: none) seed the lanes with frf 0 of
+  // the first pass, one per output corner
+  float sl = nanf(""), a = nanf("");
+  if (lane < 8 && frf == 0) {
+    sl = __ldg(g.pi_slew + 4 * v + c_out);
+    a = __ldg(g.pi_at + 4 * v + c_out);
+  }
+  bool ok = true;
+  for (int j = lane; j < nitems; j += 32) {
+    const int arc = __ldg(g.fanin + f0 + (j >> 3));
+    const int u = __ldg(g.arc_from + arc);
+    const int kind = __ldg(g.arc_kind + arc);
+    float d = nanf(""), so = nanf(""), imp = nanf("");
+    Lut ls = no_lut(), ld = no_lut();
+    float load = 0.0f;
+    int s = -1;
+    if (kind == 0) {
+      s = frf == trf ? rc_slot(G_, arc) : -1;
+      if (s >= 0) {
+        imp = __ldg(G_.rc.impulse + 4 * (size_t)s + c_out);
+        d = __ldg(G_.rc.delay + 4 * (size_t)s + c_out);
+      }
+    } else {
+      const int t = __ldg(g.arc_timing + 2 * arc + el);
+      ls = timing_lut(G_, t, 1, frf, trf);
+      ld = timing_lut(G_, t, 0, frf, trf);
+      const int net = __ldg(g.arc_net + arc);
+      if (net >= 0 && t >= 0)
+        load = __ldg(G_.rc.load + 4 * (size_t)__ldg(G_.rc.nodes_start + net) + c_out);
     }
-    for (int k = g.fanout_start[v]; k < g.fanout_start[v + 1]; ++k) {
-      const int arc = g.fanout[k], w = g.arc_to[arc];
+    if (!wait_ready(fready + u, ctl)) {
+      ok = false;
+      break;
+    }
+    const float si = __ldcg(slew + 4 * u + 2 * el + frf);
+    const float fa = __ldcg(at + 4 * u + 2 * el + frf);
+    if (kind == 0) {
+      // sign(si) * sqrt(si^2 + impulse) at the sink (FlatRct::slew)
+      if (s >= 0 && !none(si)) {
+        const float r = sqrtf(__fadd_rn(__fmul_rn(si, si), imp));
+        so = si < 0.0f ? -r : r;
+      }
+    } else if (!none(si)) {
+      so = timing_value(G_, ls, si, load);
+      d = timing_value(G_, ld, si, load);
+    } else {
+      d = nanf("");
+    }
+    arc_delay[8 * (size_t)arc + (j & 7)] = d;
+    sl = relax_fwd(el, sl, so);
+    if (!none(fa) && !none(d)) a = relax_fwd(el, a, __fadd_rn(d, fa));
+  }
+  ok = __all_sync(FULL, ok);
+  if (!ok) return false;
+  // lanes sharing (el, trf) differ in bits 1, 3 and 4
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const int m = k == 0 ? 2 : (k == 1 ? 8 : 16);
+    sl = relax_fwd(el, sl, __shfl_xor_sync(FULL, sl, m));
+    a = relax_fwd(el, a, __shfl_xor_sync(FULL, a, m));
+  }
+  // corner c's result sits in lane 4 * (c >> 1) + (c & 1)
+  float slc[4];
+#pragma unroll
+  for (int c = 0; c < 4; ++c) slc[c] = __shfl_sync(FULL, sl, 4 * (c >> 1) + (c & 1));
+  if (lane < 8 && frf == 0) {
+    slew[4 * v + c_out] = sl;
+    at[4 * v + c_out] = a;
+  }
+  // timing tests constrained at v (Test::_fprop_rat): lane j of a pass takes
+  // test j/4 and output corner j%4
+  const int t0 = __ldg(g.test_start + v), ntest = 4 * (__ldg(g.test_start + v + 1) - t0);
+  for (int j = lane; j < ntest; j += 32) {
+    const int test = __ldg(g.test_of_pin + t0 + (j >> 2));
+    const int arc = __ldg(g.test_arc + test), u = __ldg(g.arc_from + arc);
+    const int tel = (j >> 1) & 1, rf = j & 1;
+    const int t = __ldg(g.arc_timing + 2 * arc + tel);
+    float val = nanf("");
+    if (!none(g.period) && t >= 0) {
+      const int edge = __ldg(g.timing + 9 * t + 1);
+      const int fel = tel == MIN_ ? MAX_ : MIN_;
+      const int rrf = edge == 1 ? RISE_ : FALL_;
+      const float csl = slc[2 * tel + rf];
+      if (!(rrf == FALL_ && edge != 2) && !none(csl)) {
+        const Lut lc = timing_lut(G_, t, 2, rrf, rf);
+        if (!wait_ready(fready + u, ctl)) {
+          ok = false;
+          break;
+        }
+        const float rat_at = __ldcg(at + 4 * u + 2 * fel + rrf);
+        const float rsl = __ldcg(slew + 4 * u + 2 * fel + rrf);
+        if (!none(rat_at) && !none(rsl)) {
+          const float related = tel == MIN_ ? rat_at : __fadd_rn(rat_at, g.period);
+          const float cons = timing_value(G_, lc, rsl, csl);
+          if (!none(cons))
+            val = tel == MIN_ ? __fadd_rn(cons, related) : __fsub_rn(related, cons);
+        }
+      }
+    }
+    test_rat[4 * (size_t)test + (j & 3)] = val;
+  }
+  ok = __all_sync(FULL, ok);
+  if (!ok) return false;
+  publish(fready + v, lane);
+  return true;
+}
+
+// Backward at pin v (one warp): Timer::_bprop_rat and the slack.  Lanes
+// first take the tests constrained at v (4 corners each), then the fanout
+// arcs (8 combinations each); every candidate lands in a 4-corner register
+// set reduced over the whole warp.
+__device__ bool bprop_warp(const G& G_, int v, int lane, const float* at, float* rat, float* slack,
+                           const float* arc_delay, const float* test_rat, int* bready,
+                           GridCtl* ctl) {
+  const otg_prop_graph& g = G_.g;
+  float r[4];
+#pragma unroll
+  for (int c = 0; c < 4; ++c) r[c] = lane == 0 ? __ldg(g.po_rat + 4 * v + c) : nanf("");
+  const int t0 = __ldg(g.test_start + v), ntest = 4 * (__ldg(g.test_start + v + 1) - t0);
+  const int o0 = __ldg(g.fanout_start + v), nitems = ntest + 8 * (__ldg(g.fanout_start + v + 1) - o0);
+  bool ok = true;
+  for (int j = lane; j < nitems; j += 32) {
+    int tc = 0;  // target corner
+    float cand = nanf("");
+    if (j < ntest) {
+      tc = j & 3;
+      cand = __ldcg(test_rat + 4 * (size_t)__ldg(g.test_of_pin + t0 + (j >> 2)) + tc);
+    } else {
+      const int jj = j - ntest;
+      const int arc = __ldg(g.fanout + o0 + (jj >> 3)), w = __ldg(g.arc_to + arc);
+      const int el = (jj >> 2) & 1, frf = (jj >> 1) & 1, trf = jj & 1;
+      const int kind = __ldg(g.arc_kind + arc);
       const float* d = arc_delay + 8 * (size_t)arc;
-      if (g.arc_kind[arc] == 0) {
-        for (int el = 0; el < 2; ++el)
-          for (int rf = 0; rf < 2; ++rf) {
-            const float wr = rat[4 * w + 2 * el + rf], dl = d[4 * el + 2 * rf + rf];
-            if (!none(wr) && !none(dl)) relax(el, rf, __fsub_rn(wr, dl));
-          }
-        continue;
+      int mode = 0;  // 0 none, 1 propagation, 2 MIN constraint, 3 MAX constraint
+      if (kind == 0) {
+        mode = frf == trf ? 1 : 0;
+      } else {
+        const int t = __ldg(g.arc_timing + 2 * arc + el);
+        if (t >= 0) {
+          const int* tr = g.timing + 9 * t;
+          if (!__ldg(tr + 2)) mode = 1;
+          else if (transition_defined(tr, frf, trf)) mode = el == MIN_ ? 2 : 3;
+        }
       }
-      for (int el = 0; el < 2; ++el) {
-        const int t = g.arc_timing[2 * arc + el];
-        if (t < 0) continue;
-        const int* tr = g.timing + 9 * t;
-        for (int frf = 0; frf < 2; ++frf)
-          for (int trf = 0; trf < 2; ++trf) {
-            if (!tr[2]) {  // a propagation arc
-              const float wr = rat[4 * w + 2 * el + trf], dl = d[4 * el + 2 * frf + trf];
-              if (!none(wr) && !none(dl)) relax(el, frf, __fsub_rn(wr, dl));
-              continue;
-            }
-            if (!transition_defined(tr, frf, trf)) continue;  // a constraint arc
-            if (el == MIN_) {
-              const float a = at[4 * v + 2 * MAX_ + frf];
-              const float wa = at[4 * w + trf], wr = rat[4 * w + trf];  // w's MIN slack
-              if (!none(a) && !none(wa) && !none(wr))
-                relax(MAX_, frf, __fadd_rn(a, __fsub_rn(wa, wr)));
-            } else {
-              const float a = at[4 * v + 2 * MIN_ + frf];
-              const float wa = at[4 * w + 2 + trf], wr = rat[4 * w + 2 + trf];  // w's MAX slack
-              if (!none(a) && !none(wa) && !none(wr))
-                relax(MIN_, frf, __fsub_rn(a, __fsub_rn(wr, wa)));
-            }
-          }
+      if (mode != 0) {
+        if (!wait_ready(bready + w, ctl)) {
+          ok = false;
+          break;
+        }
+        if (mode == 1) {
+          tc = 2 * el + frf;
+          const float wr = __ldcg(rat + 4 * w + 2 * el + trf);
+          const float dl = __ldcg(d + 4 * el + 2 * frf + trf);
+          if (!none(wr) && !none(dl)) cand = __fsub_rn(wr, dl);
+        } else if (mode == 2) {  // hold-like: w's MIN slack moves v's MAX rat
+          tc = 2 * MAX_ + frf;
+          const float a = __ldcg(at + 4 * v + 2 * MAX_ + frf);
+          const float wa = __ldcg(at + 4 * w + trf), wr = __ldcg(rat + 4 * w + trf);
+          if (!none(a) && !none(wa) && !none(wr)) cand = __fadd_rn(a, __fsub_rn(wa, wr));
+        } else {  // setup-like: w's MAX slack moves v's MIN rat
+          tc = 2 * MIN_ + frf;
+          const float a = __ldcg(at + 4 * v + 2 * MIN_ + frf);
+          const float wa = __ldcg(at + 4 * w + 2 + trf), wr = __ldcg(rat + 4 * w + 2 + trf);
+          if (!none(a) && !none(wa) && !none(wr)) cand = __fsub_rn(a, __fsub_rn(wr, wa));
+        }
       }
     }
-    for (int c = 0; c < 4; ++c) {
-      rat[4 * v + c] = r[c];
-      const float a = at[4 * v + c];
-      slack[4 * v + c] = (none(a) || none(r[c])) ? nanf("")
-                         : (c < 2 ? __fsub_rn(a, r[c]) : __fsub_rn(r[c], a));
-    }
+#pragma unroll
+    for (int c = 0; c < 4; ++c)
+      if (c == tc) r[c] = relax_bwd(c >> 1, r[c], cand);
   }
+  ok = __all_sync(FULL, ok);
+  if (!ok) return false;
+#pragma unroll
+  for (int c = 0; c < 4; ++c)
+#pragma unroll
+    for (int m = 1; m < 32; m <<= 1) r[c] = relax_bwd(c >> 1, r[c], __shfl_xor_sync(FULL, r[c], m));
+  if (lane < 4) {
+    float rc = r[0];
+#pragma unroll
+    for (int c = 1; c < 4; ++c)
+      if (lane == c) rc = r[c];
+    rat[4 * v + lane] = rc;
+    const float a = __ldcg(at + 4 * v + lane);
+    slack[4 * v + lane] = (none(a) || none(rc)) ? nanf("")
+                          : (lane < 2 ? __fsub_rn(a, rc) : __fsub_rn(rc, a));
+  }
+  publish(bready + v, lane);
+  return true;
+}
+
+// The whole propagation in one cooperative launch; warp w of W takes items
+// w, w + W, ... of each pass.
+__global__ void __launch_bounds__(256) prop_kernel(G G_, const int* order, int num_pins,
+                                                   float* at, float* slew, float* rat,
+                                                   float* slack, float* arc_delay,
+                                                   float* test_rat, int* fready, int* bready,
+                                                   GridCtl* ctl) {
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int W = (gridDim.x * blockDim.x) >> 5;
+  bool ok = true;
+  for (int j = warp; ok && j < num_pins; j += W)
+    ok = fprop_warp(G_, __ldg(order + num_pins - 1 - j), lane, at, slew, arc_delay, test_rat,
+                    fready, ctl);
+  // the barrier also lets every CTA leave together when a wait gave up
+  if (!grid_barrier(ctl) || !ok) return;
+  for (int j = warp; ok && j < num_pins; j += W)
+    ok = bprop_warp(G_, __ldg(order + j), lane, at, rat, slack, arc_delay, test_rat, bready, ctl);
 }
 
 size_t align256p(size_t x) { return (x + 255) & ~(size_t)255; }
+
+struct PropDev {
+  int sms = 0, occ = 0;
+  bool init = false;
+};
+PropDev g_pdev[64];
 
 }  // namespace
 }  // namespace otg
 
 extern "C" {
 
-otg_status otg_prop_workspace_size(int32_t num_arcs, int32_t num_tests, size_t* bytes) {
-  if (!bytes || num_arcs < 0 || num_tests < 0) return OTG_ERR_INVALID;
-  *bytes = otg::align256p(32 * (size_t)num_arcs) + otg::align256p(16 * (size_t)num_tests) + 256;
+otg_status otg_prop_workspace_size(int32_t num_pins, int32_t num_arcs, int32_t num_tests,
+                                   size_t* bytes) {
+  if (!bytes || num_pins < 0 || num_arcs < 0 || num_tests < 0) return OTG_ERR_INVALID;
+  *bytes = 256 + otg::align256p(8 * (size_t)num_pins) + otg::align256p(32 * (size_t)num_arcs) +
+           otg::align256p(16 * (size_t)num_tests);
   return OTG_OK;
 }
 
 otg_status otg_propagate(const otg_prop_graph* g, const otg_prop_rc* rc, const int32_t* order,
-                         const int32_t* level_ends, int32_t num_levels, float* at, float* slew,
-                         float* rat, float* slack, void* workspace, size_t workspace_bytes,
-                         otg_stream_t stream) {
-  if (!g || !rc || !order || !level_ends || num_levels < 0 || !at || !slew || !rat || !slack ||
-      !workspace)
+                         float* at, float* slew, float* rat, float* slack, void* workspace,
+                         size_t workspace_bytes, otg_stream_t stream) {
+  if (!g || !rc || !order || !at || !slew || !rat || !slack || !workspace || g->num_pins < 0)
     return OTG_ERR_INVALID;
+  if (((uintptr_t)g->lut_meta & 15) != 0 || ((uintptr_t)workspace & 255) != 0)
+    return OTG_ERR_INVALID;  // lut_meta rows are read as int4
   size_t need = 0;
-  otg_prop_workspace_size(g->num_arcs, g->num_tests, &need);
+  otg_prop_workspace_size(g->num_pins, g->num_arcs, g->num_tests, &need);
   if (workspace_bytes < need) return OTG_ERR_WORKSPACE;
-  float* arc_delay = (float*)workspace;
-  float* test_rat = (float*)((char*)workspace + otg::align256p(32 * (size_t)g->num_arcs));
+  const int P = g->num_pins;
+  char* ws = (char*)workspace;
+  otg::GridCtl* ctl = (otg::GridCtl*)ws;
+  int* fready = (int*)(ws + 256);
+  int* bready = fready + P;
+  const size_t head = 256 + otg::align256p(8 * (size_t)P);
+  float* arc_delay = (float*)(ws + head);
+  float* test_rat = (float*)(ws + head + otg::align256p(32 * (size_t)g->num_arcs));
   cudaStream_t st = (cudaStream_t)stream;
+  // the control block and the ready flags start at zero
+  if (cudaMemsetAsync(ws, 0, head, st) != cudaSuccess) {
+    cudaGetLastError();
+    return OTG_ERR_CUDA;
+  }
+  if (P == 0) return OTG_OK;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  otg::PropDev& d = otg::g_pdev[dev & 63];
+  if (!d.init) {
+    cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d.occ, otg::prop_kernel, 256, 0);
+    d.init = true;
+  }
+  // every CTA resident (the schedule and the barrier rely on it), no more
+  // warps than pins
+  const int grid = std::max(1, std::min(d.sms * std::max(d.occ, 1), (P + 7) / 8));
   otg::G G_{*g, *rc};
-  // at and slew start as "none": pins are written as their level runs, and
-  // a pin only reads pins of higher levels
-  auto grid = [](int n) { return std::max(1, std::min(1184, (n + 127) / 128)); };
-  for (int L = num_levels - 1; L >= 0; --L) {
-    const int lo = level_ends[L], hi = level_ends[L + 1];
-    if (hi <= lo) continue;
-    otg::fprop_kernel<<<grid(hi - lo), 128, 0, st>>>(G_, order, lo, hi, at, slew, arc_delay,
-                                                      test_rat);
-    otg::count_launch();
+  int num_pins = P;
+  void* args[] = {&G_,  (void*)&order, &num_pins, &at,     &slew,   &rat,
+                  &slack, &arc_delay,  &test_rat, &fready, &bready, &ctl};
+  const cudaError_t e =
+      cudaLaunchCooperativeKernel((const void*)otg::prop_kernel, dim3(grid), dim3(256), args, 0, st);
+  otg::count_launch();
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return OTG_ERR_CUDA;
   }
-  for (int L = 0; L < num_levels; ++L) {
-    const int lo = level_ends[L], hi = level_ends[L + 1];
-    if (hi <= lo) continue;
-    otg::bprop_kernel<<<grid(hi - lo), 128, 0, st>>>(G_, order, lo, hi, at, rat, slack,
-                                                      arc_delay, test_rat);
-    otg::count_launch();
-  }
-  if (cudaGetLastError() != cudaSuccess) return OTG_ERR_CUDA;
   return OTG_OK;
+}
+
+otg_status otg_prop_status(const void* workspace, otg_stream_t stream) {
+  if (!workspace) return OTG_ERR_INVALID;
+  otg::GridCtl h;
+  if (cudaMemcpyAsync(&h, workspace, sizeof(h), cudaMemcpyDeviceToHost, (cudaStream_t)stream) !=
+          cudaSuccess ||
+      cudaStreamSynchronize((cudaStream_t)stream) != cudaSuccess) {
+    cudaGetLastError();
+    return OTG_ERR_CUDA;
+  }
+  return (otg_status)h.status;
 }
 
 }  // extern "C"

@@ -12,7 +12,8 @@ writes into `dirpath`:
                         scaled by 0.9, so the MIN and MAX corners differ.
   design.v              a random gate DAG: 64 primary inputs and outputs,
                         fanin 1..2, sources drawn with a geometric bias
-                        towards recent signals (a skewed fanout), 5% flops on
+                        towards recent signals (a skewed fanout; the mean
+                        look-back is max(50, gates/100)), 5% flops on
                         one clock port; outputs left without a sink are
                         gathered by extra NAND2 gates until 64 remain.
   design.spef           one RC tree per net: the net's pins plus internal
@@ -182,9 +183,13 @@ def netlist(rng, gates, n_pi=64, n_po=64, dff_frac=0.05):
     fanout = {s: 0 for s in signals}
     glist = []
 
+    # geometric bias towards recent signals (a skewed fanout); the mean
+    # look-back grows with the design, so the logic depth stays in the
+    # hundreds of levels instead of growing with the gate count
+    p_back = min(0.02, 100.0 / max(gates, 1))
+
     def pick():
-        # geometric bias towards recent signals: a skewed fanout
-        back = min(int(rng.geometric(0.02)), len(signals))
+        back = min(int(rng.geometric(p_back)), len(signals))
         s = signals[-back]
         fanout[s] += 1
         return s

@@ -5,8 +5,8 @@
 
 The graph is flat: pins, arcs (net arcs onto RC nodes of the RcBatch's
 forest, cell arcs with a timing record per split), timing records, look-up
-tables, timing tests and primary-input/-output assertions.  Levels come
-from otg_levelize over the graph's fanin CSR.
+tables, timing tests and primary-input/-output assertions.  The pin order
+comes from otg_levelize over the graph's fanin CSR.
 """
 import ctypes
 
@@ -85,10 +85,10 @@ class TimingGraph:
         order, ends, _ = lb.result()
         assert len(order) == P, "the timing graph has a cycle"
         self.order = t(order, np.int32)
-        self.level_ends = np.ascontiguousarray(ends, np.int32)
+        self.level_ends = t(ends, np.int32)
         self.num_levels = len(ends) - 1
         ws = ctypes.c_size_t()
-        check("otg_prop_workspace_size", lib().otg_prop_workspace_size(A, len(test_arc),
+        check("otg_prop_workspace_size", lib().otg_prop_workspace_size(P, A, len(test_arc),
                                                                        ctypes.byref(ws)))
         self.workspace = torch.empty(max(ws.value, 256), dtype=torch.uint8, device=device)
         self.out = {k: torch.empty(P, NC, dtype=torch.float32, device=device)
@@ -102,14 +102,18 @@ class TimingGraph:
         o = self.out
         check("otg_propagate", lib().otg_propagate(
             ctypes.byref(self.graph), ctypes.byref(rc), _ptr(self.order),
-            self.level_ends.ctypes.data, self.num_levels, _ptr(o["at"]), _ptr(o["slew"]),
+            _ptr(o["at"]), _ptr(o["slew"]),
             _ptr(o["rat"]), _ptr(o["slack"]), _ptr(self.workspace), self.workspace.numel(),
             _stream(stream)))
         return self
 
+    def check(self, stream=None):
+        """Synchronizes; raises if a bounded wait of the last propagation
+        gave up (OTG_ERR_TIMEOUT)."""
+        check("otg_prop_status", lib().otg_prop_status(_ptr(self.workspace), _stream(stream)))
+
     def result(self):
-        import torch
-        torch.cuda.synchronize()
+        self.check()
         return {k: v.cpu().numpy() for k, v in self.out.items()}
 
 
