@@ -614,16 +614,20 @@ def run_spef():
 
 
 def pin_err(got, ref):
-    """Worst |got - ref| / (1e-5 |ref| + 1e-5) over pins and quantities
-    (inf where one side has a value the other lacks)."""
+    """Worst |got - ref| / (1e-5 s + 1e-5) over pins and quantities ([4,4]:
+    at, slew, rat, slack by corner), s = |ref| for at and slew and
+    max(|ref|, |ref at|) for rat and slack, differences of path-length
+    quantities (inf where one side has a value the other lacks)."""
     worst = 0.0
     for name, r in ref.items():
         g = got[name]
         m = ~np.isnan(r)
         if not np.array_equal(m, ~np.isnan(g)):
             return float("inf")
+        scale = np.abs(r)
+        scale[2:] = np.maximum(scale[2:], np.nan_to_num(np.abs(r[0])))
         if m.any():
-            worst = max(worst, float(np.max(np.abs(g[m] - r[m]) / (1e-5 * np.abs(r[m]) + 1e-5))))
+            worst = max(worst, float(np.max(np.abs(g[m] - r[m]) / (1e-5 * scale[m] + 1e-5))))
     return worst
 
 
@@ -681,7 +685,7 @@ def run_full_update(dump=None):
                            f"{graph.A} arcs, {graph.num_levels} levels",
                "gpu_ms": rc_ms + prop_ms, "rc_pass_ms": rc_ms, "propagation_ms": prop_ms,
                "timed": f"median of {FU_REPS}", "spef_read_ms": 1e3 * t_spef,
-               "levels": graph.num_levels, "launches_per_propagation": 1}
+               "levels": graph.num_levels, "launches_per_propagation": 2}
         exe = os.path.join(ROOT, "oracle", "_ref", "ot_run_ref")
         if os.path.exists(exe):
             ours = {n: np.stack([res[k][i] for k in ("at", "slew", "rat", "slack")])

@@ -373,9 +373,10 @@ otg_status otg_prop_workspace_size(int32_t num_pins, int32_t num_arcs, int32_t n
                                    size_t* bytes);
 /* order (device, num_pins entries) is otg_levelize's output over the
  * graph's fanin CSR: every pin after all of its fanout pins.  Writes at,
- * slew, rat, slack [P][4].  lut_meta must be 16-byte aligned, the
- * workspace 256-byte aligned.  One cooperative launch, dataflow-scheduled
- * (per-pin ready flags, bounded waits); asynchronous.  otg_prop_status
+ * slew, rat, slack [P][4].  lut_meta and the four outputs must be 16-byte
+ * aligned, the workspace 256-byte aligned.  A fill launch, then one
+ * cooperative launch, dataflow-scheduled (a pin polls the values it reads
+ * from its fanins, bounded waits); asynchronous.  otg_prop_status
  * synchronizes the stream and returns OTG_ERR_TIMEOUT if a wait gave up. */
 otg_status otg_propagate(const otg_prop_graph* graph, const otg_prop_rc* rc,
                          const int32_t* order, float* at, float* slew, float* rat, float* slack,

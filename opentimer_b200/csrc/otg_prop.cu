@@ -18,18 +18,27 @@
 // Schedule: one cooperative launch, a warp per pin, dataflow instead of
 // level barriers.  Pins are numbered in level order (otg_levelize: every
 // pin after all of its fanouts); the forward pass takes them last level
-// first, warp w the items w, w+W, w+2W, ...  A pin waits (bounded) on the
-// ready flag of each fanin, computes, and raises its own flag.  Because a
-// pin depends only on lower-numbered items and each warp works through its
-// items in order, the lowest unfinished item always has every input ready:
-// the schedule cannot deadlock while all CTAs are resident, which the
-// cooperative launch guarantees.  One grid barrier separates the forward
-// pass from the backward pass, which runs the same way first level first.
+// first, warp w the items w, w+W, w+2W, ...  A pin waits (bounded) until
+// the values it reads from its fanins are there, computes, and stores its
+// own.  Because a pin depends only on lower-numbered items and each warp
+// works through its items in order, the lowest unfinished item always has
+// every input ready: the schedule cannot deadlock while all CTAs are
+// resident, which the cooperative launch guarantees.  One grid barrier
+// separates the forward pass from the backward pass, which runs the same
+// way first level first.
+//
+// Readiness is carried by the values themselves: a fill kernel sets every
+// arrival time and slew to kPending, a NaN payload that no stored value
+// carries (an empty value is stored as the canonical NaN), and the forward
+// pass does the same to each pin's required time before the barrier.  A
+// reader polls exactly the words it needs with relaxed loads, each word is
+// written once, so no fence or flag sits on the critical path.
+//
 // Inside a warp the lanes split a pin's (arc, split, from-transition,
 // to-transition) combinations and reduce with shuffles; min/max reductions
 // are order-free, so the lane split does not change a value.  Values that
-// other warps wrote in the launch are read with __ldcg (L2); the graph and
-// the library are read-only for the launch and go through __ldg.
+// other warps wrote after the barrier are read with __ldcg (L2); the graph
+// and the library are read-only for the launch and go through __ldg.
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
@@ -145,23 +154,34 @@ __device__ __forceinline__ int rc_slot(const G& G_, int arc) {
   return __ldg(G_.rc.nodes_start + net) + __ldg(G_.rc.node2bfs + node);
 }
 
-__device__ __forceinline__ int ld_acquire(const int* p) {
-  int v;
-  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+constexpr unsigned kPending = 0x7fbadbadu;  // "not yet computed"
+constexpr unsigned kEmpty = 0x7fffffffu;    // the stored empty value
+
+__device__ __forceinline__ float canon(float x) { return none(x) ? __uint_as_float(kEmpty) : x; }
+
+__device__ __forceinline__ float ld_relaxed(const float* p) {
+  float v;
+  asm volatile("ld.relaxed.gpu.global.f32 %0, [%1];" : "=f"(v) : "l"(p) : "memory");
   return v;
 }
 
-__device__ __forceinline__ void st_release(int* p, int v) {
-  asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+__device__ __forceinline__ void st_relaxed4(float* p, float a, float b, float c, float d) {
+  asm volatile("st.relaxed.gpu.global.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(p), "f"(a), "f"(b),
+               "f"(c), "f"(d)
+               : "memory");
 }
 
-// Bounded wait for a ready flag; false when this or another wait gave up.
-__device__ bool wait_ready(const int* flag, GridCtl* c) {
-  if (ld_acquire(flag)) return true;
+// Bounded wait until *p holds a computed value, returned in out; false
+// when this or another wait gave up.  The first polls spin (each is an L2
+// round trip), later ones sleep.
+__device__ bool wait_value(const float* p, float& out, GridCtl* c) {
+  out = ld_relaxed(p);
+  if (__float_as_uint(out) != kPending) return true;
   const unsigned long long t0 = gtime();
-  for (;;) {
-    __nanosleep(32);
-    if (ld_acquire(flag)) return true;
+  for (int k = 0;; ++k) {
+    if (k >= 64) __nanosleep(64);
+    out = ld_relaxed(p);
+    if (__float_as_uint(out) != kPending) return true;
     if (*(volatile int*)&c->abort) return false;
     if (gtime() - t0 > kGridWaitNs) {
       atomicExch(&c->abort, 1);
@@ -181,19 +201,12 @@ __device__ __forceinline__ float relax_bwd(int el, float cur, float v) {
   return el == MIN_ ? fmaxf(cur, v) : fminf(cur, v);
 }
 
-// Writes of this warp visible GPU-wide, then the pin's ready flag.
-__device__ __forceinline__ void publish(int* flag, int lane) {
-  __threadfence();
-  __syncwarp();
-  if (lane == 0) st_release(flag, 1);
-}
-
 // Forward at pin v (one warp): Timer::_fprop_slew, _fprop_delay, _fprop_at
 // and _fprop_test.  Lane j of a pass takes fanin arc j/8 and the combination
 // (el, frf, trf) = bits (2, 1, 0) of j; its slew and arrival candidates go to
 // output corner (el, trf).  Returns false if a wait gave up.
-__device__ bool fprop_warp(const G& G_, int v, int lane, float* at, float* slew, float* arc_delay,
-                           float* test_rat, int* fready, GridCtl* ctl) {
+__device__ bool fprop_warp(const G& G_, int v, int lane, float* at, float* slew, float* rat,
+                           float* arc_delay, float* test_rat, GridCtl* ctl) {
   const otg_prop_graph& g = G_.g;
   const int el = (lane >> 2) & 1, frf = (lane >> 1) & 1, trf = lane & 1;
   const int c_out = 2 * el + trf;
@@ -228,12 +241,12 @@ __device__ bool fprop_warp(const G& G_, int v, int lane, float* at, float* slew,
       if (net >= 0 && t >= 0)
         load = __ldg(G_.rc.load + 4 * (size_t)__ldg(G_.rc.nodes_start + net) + c_out);
     }
-    if (!wait_ready(fready + u, ctl)) {
+    float si, fa;
+    if (!wait_value(slew + 4 * u + 2 * el + frf, si, ctl) ||
+        !wait_value(at + 4 * u + 2 * el + frf, fa, ctl)) {
       ok = false;
       break;
     }
-    const float si = __ldcg(slew + 4 * u + 2 * el + frf);
-    const float fa = __ldcg(at + 4 * u + 2 * el + frf);
     if (kind == 0) {
       // sign(si) * sqrt(si^2 + impulse) at the sink (FlatRct::slew)
       if (s >= 0 && !none(si)) {
@@ -259,13 +272,21 @@ __device__ bool fprop_warp(const G& G_, int v, int lane, float* at, float* slew,
     sl = relax_fwd(el, sl, __shfl_xor_sync(FULL, sl, m));
     a = relax_fwd(el, a, __shfl_xor_sync(FULL, a, m));
   }
-  // corner c's result sits in lane 4 * (c >> 1) + (c & 1)
-  float slc[4];
+  // corner c's result sits in lane 4 * (c >> 1) + (c & 1); lane 0 stores
+  // the pin's slew and arrival time, which releases its readers, and marks
+  // its required time pending for the backward pass (the arc delays and
+  // test RATs are read only after the grid barrier)
+  float slc[4], atc[4];
 #pragma unroll
-  for (int c = 0; c < 4; ++c) slc[c] = __shfl_sync(FULL, sl, 4 * (c >> 1) + (c & 1));
-  if (lane < 8 && frf == 0) {
-    slew[4 * v + c_out] = sl;
-    at[4 * v + c_out] = a;
+  for (int c = 0; c < 4; ++c) {
+    slc[c] = canon(__shfl_sync(FULL, sl, 4 * (c >> 1) + (c & 1)));
+    atc[c] = canon(__shfl_sync(FULL, a, 4 * (c >> 1) + (c & 1)));
+  }
+  if (lane == 0) {
+    st_relaxed4(slew + 4 * v, slc[0], slc[1], slc[2], slc[3]);
+    st_relaxed4(at + 4 * v, atc[0], atc[1], atc[2], atc[3]);
+    const float p = __uint_as_float(kPending);
+    reinterpret_cast<float4*>(rat)[v] = make_float4(p, p, p, p);
   }
   // timing tests constrained at v (Test::_fprop_rat): lane j of a pass takes
   // test j/4 and output corner j%4
@@ -283,12 +304,12 @@ __device__ bool fprop_warp(const G& G_, int v, int lane, float* at, float* slew,
       const float csl = slc[2 * tel + rf];
       if (!(rrf == FALL_ && edge != 2) && !none(csl)) {
         const Lut lc = timing_lut(G_, t, 2, rrf, rf);
-        if (!wait_ready(fready + u, ctl)) {
+        float rat_at, rsl;
+        if (!wait_value(at + 4 * u + 2 * fel + rrf, rat_at, ctl) ||
+            !wait_value(slew + 4 * u + 2 * fel + rrf, rsl, ctl)) {
           ok = false;
           break;
         }
-        const float rat_at = __ldcg(at + 4 * u + 2 * fel + rrf);
-        const float rsl = __ldcg(slew + 4 * u + 2 * fel + rrf);
         if (!none(rat_at) && !none(rsl)) {
           const float related = tel == MIN_ ? rat_at : __fadd_rn(rat_at, g.period);
           const float cons = timing_value(G_, lc, rsl, csl);
@@ -299,10 +320,7 @@ __device__ bool fprop_warp(const G& G_, int v, int lane, float* at, float* slew,
     }
     test_rat[4 * (size_t)test + (j & 3)] = val;
   }
-  ok = __all_sync(FULL, ok);
-  if (!ok) return false;
-  publish(fready + v, lane);
-  return true;
+  return __all_sync(FULL, ok);
 }
 
 // Backward at pin v (one warp): Timer::_bprop_rat and the slack.  Lanes
@@ -310,8 +328,7 @@ __device__ bool fprop_warp(const G& G_, int v, int lane, float* at, float* slew,
 // arcs (8 combinations each); every candidate lands in a 4-corner register
 // set reduced over the whole warp.
 __device__ bool bprop_warp(const G& G_, int v, int lane, const float* at, float* rat, float* slack,
-                           const float* arc_delay, const float* test_rat, int* bready,
-                           GridCtl* ctl) {
+                           const float* arc_delay, const float* test_rat, GridCtl* ctl) {
   const otg_prop_graph& g = G_.g;
   float r[4];
 #pragma unroll
@@ -343,24 +360,26 @@ __device__ bool bprop_warp(const G& G_, int v, int lane, const float* at, float*
         }
       }
       if (mode != 0) {
-        if (!wait_ready(bready + w, ctl)) {
+        // the fanout's required time this combination reads
+        const int wc = mode == 1 ? 2 * el + trf : (mode == 2 ? trf : 2 + trf);
+        float wr;
+        if (!wait_value(rat + 4 * w + wc, wr, ctl)) {
           ok = false;
           break;
         }
         if (mode == 1) {
           tc = 2 * el + frf;
-          const float wr = __ldcg(rat + 4 * w + 2 * el + trf);
           const float dl = __ldcg(d + 4 * el + 2 * frf + trf);
           if (!none(wr) && !none(dl)) cand = __fsub_rn(wr, dl);
         } else if (mode == 2) {  // hold-like: w's MIN slack moves v's MAX rat
           tc = 2 * MAX_ + frf;
           const float a = __ldcg(at + 4 * v + 2 * MAX_ + frf);
-          const float wa = __ldcg(at + 4 * w + trf), wr = __ldcg(rat + 4 * w + trf);
+          const float wa = __ldcg(at + 4 * w + trf);
           if (!none(a) && !none(wa) && !none(wr)) cand = __fadd_rn(a, __fsub_rn(wa, wr));
         } else {  // setup-like: w's MAX slack moves v's MIN rat
           tc = 2 * MIN_ + frf;
           const float a = __ldcg(at + 4 * v + 2 * MIN_ + frf);
-          const float wa = __ldcg(at + 4 * w + 2 + trf), wr = __ldcg(rat + 4 * w + 2 + trf);
+          const float wa = __ldcg(at + 4 * w + 2 + trf);
           if (!none(a) && !none(wa) && !none(wr)) cand = __fsub_rn(a, __fsub_rn(wr, wa));
         }
       }
@@ -375,18 +394,29 @@ __device__ bool bprop_warp(const G& G_, int v, int lane, const float* at, float*
   for (int c = 0; c < 4; ++c)
 #pragma unroll
     for (int m = 1; m < 32; m <<= 1) r[c] = relax_bwd(c >> 1, r[c], __shfl_xor_sync(FULL, r[c], m));
-  if (lane < 4) {
-    float rc = r[0];
+  if (lane == 0) {
+    st_relaxed4(rat + 4 * v, canon(r[0]), canon(r[1]), canon(r[2]), canon(r[3]));
+    const float4 a4 = __ldcg(reinterpret_cast<const float4*>(at) + v);
+    const float a[4] = {a4.x, a4.y, a4.z, a4.w};
+    float sk[4];
 #pragma unroll
-    for (int c = 1; c < 4; ++c)
-      if (lane == c) rc = r[c];
-    rat[4 * v + lane] = rc;
-    const float a = __ldcg(at + 4 * v + lane);
-    slack[4 * v + lane] = (none(a) || none(rc)) ? nanf("")
-                          : (lane < 2 ? __fsub_rn(a, rc) : __fsub_rn(rc, a));
+    for (int c = 0; c < 4; ++c)
+      sk[c] = (none(a[c]) || none(r[c])) ? __uint_as_float(kEmpty)
+              : (c < 2 ? __fsub_rn(a[c], r[c]) : __fsub_rn(r[c], a[c]));
+    reinterpret_cast<float4*>(slack)[v] = make_float4(sk[0], sk[1], sk[2], sk[3]);
   }
-  publish(bready + v, lane);
   return true;
+}
+
+// Marks every arrival time and slew pending and clears the control block.
+__global__ void prop_init_kernel(float4* at, float4* slew, int num_pins, GridCtl* ctl) {
+  const int i0 = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i0 == 0) *ctl = GridCtl{0u, 0u, 0, 0};
+  const float p = __uint_as_float(kPending);
+  for (int i = i0; i < num_pins; i += gridDim.x * blockDim.x) {
+    at[i] = make_float4(p, p, p, p);
+    slew[i] = make_float4(p, p, p, p);
+  }
 }
 
 // The whole propagation in one cooperative launch; warp w of W takes items
@@ -394,19 +424,18 @@ __device__ bool bprop_warp(const G& G_, int v, int lane, const float* at, float*
 __global__ void __launch_bounds__(256) prop_kernel(G G_, const int* order, int num_pins,
                                                    float* at, float* slew, float* rat,
                                                    float* slack, float* arc_delay,
-                                                   float* test_rat, int* fready, int* bready,
-                                                   GridCtl* ctl) {
+                                                   float* test_rat, GridCtl* ctl) {
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int W = (gridDim.x * blockDim.x) >> 5;
   bool ok = true;
   for (int j = warp; ok && j < num_pins; j += W)
-    ok = fprop_warp(G_, __ldg(order + num_pins - 1 - j), lane, at, slew, arc_delay, test_rat,
-                    fready, ctl);
+    ok = fprop_warp(G_, __ldg(order + num_pins - 1 - j), lane, at, slew, rat, arc_delay, test_rat,
+                    ctl);
   // the barrier also lets every CTA leave together when a wait gave up
   if (!grid_barrier(ctl) || !ok) return;
   for (int j = warp; ok && j < num_pins; j += W)
-    ok = bprop_warp(G_, __ldg(order + j), lane, at, rat, slack, arc_delay, test_rat, bready, ctl);
+    ok = bprop_warp(G_, __ldg(order + j), lane, at, rat, slack, arc_delay, test_rat, ctl);
 }
 
 size_t align256p(size_t x) { return (x + 255) & ~(size_t)255; }
@@ -425,8 +454,7 @@ extern "C" {
 otg_status otg_prop_workspace_size(int32_t num_pins, int32_t num_arcs, int32_t num_tests,
                                    size_t* bytes) {
   if (!bytes || num_pins < 0 || num_arcs < 0 || num_tests < 0) return OTG_ERR_INVALID;
-  *bytes = 256 + otg::align256p(8 * (size_t)num_pins) + otg::align256p(32 * (size_t)num_arcs) +
-           otg::align256p(16 * (size_t)num_tests);
+  *bytes = 256 + otg::align256p(32 * (size_t)num_arcs) + otg::align256p(16 * (size_t)num_tests);
   return OTG_OK;
 }
 
@@ -435,25 +463,23 @@ otg_status otg_propagate(const otg_prop_graph* g, const otg_prop_rc* rc, const i
                          size_t workspace_bytes, otg_stream_t stream) {
   if (!g || !rc || !order || !at || !slew || !rat || !slack || !workspace || g->num_pins < 0)
     return OTG_ERR_INVALID;
-  if (((uintptr_t)g->lut_meta & 15) != 0 || ((uintptr_t)workspace & 255) != 0)
-    return OTG_ERR_INVALID;  // lut_meta rows are read as int4
+  // lut_meta rows and the per-pin [4] rows are read and written as 16-byte vectors
+  if ((((uintptr_t)g->lut_meta | (uintptr_t)at | (uintptr_t)slew | (uintptr_t)rat |
+        (uintptr_t)slack) & 15) != 0 || ((uintptr_t)workspace & 255) != 0)
+    return OTG_ERR_INVALID;
   size_t need = 0;
   otg_prop_workspace_size(g->num_pins, g->num_arcs, g->num_tests, &need);
   if (workspace_bytes < need) return OTG_ERR_WORKSPACE;
   const int P = g->num_pins;
   char* ws = (char*)workspace;
   otg::GridCtl* ctl = (otg::GridCtl*)ws;
-  int* fready = (int*)(ws + 256);
-  int* bready = fready + P;
-  const size_t head = 256 + otg::align256p(8 * (size_t)P);
-  float* arc_delay = (float*)(ws + head);
-  float* test_rat = (float*)(ws + head + otg::align256p(32 * (size_t)g->num_arcs));
+  float* arc_delay = (float*)(ws + 256);
+  float* test_rat = (float*)(ws + 256 + otg::align256p(32 * (size_t)g->num_arcs));
   cudaStream_t st = (cudaStream_t)stream;
-  // the control block and the ready flags start at zero
-  if (cudaMemsetAsync(ws, 0, head, st) != cudaSuccess) {
-    cudaGetLastError();
-    return OTG_ERR_CUDA;
-  }
+  otg::prop_init_kernel<<<std::max(1, std::min(1184, (P + 255) / 256)), 256, 0, st>>>(
+      (float4*)at, (float4*)slew, P, ctl);
+  otg::count_launch();
+  if (cudaGetLastError() != cudaSuccess) return OTG_ERR_CUDA;
   if (P == 0) return OTG_OK;
   int dev = 0;
   cudaGetDevice(&dev);
@@ -468,8 +494,8 @@ otg_status otg_propagate(const otg_prop_graph* g, const otg_prop_rc* rc, const i
   const int grid = std::max(1, std::min(d.sms * std::max(d.occ, 1), (P + 7) / 8));
   otg::G G_{*g, *rc};
   int num_pins = P;
-  void* args[] = {&G_,  (void*)&order, &num_pins, &at,     &slew,   &rat,
-                  &slack, &arc_delay,  &test_rat, &fready, &bready, &ctl};
+  void* args[] = {&G_,    (void*)&order, &num_pins, &at,       &slew,
+                  &rat,   &slack,        &arc_delay, &test_rat, &ctl};
   const cudaError_t e =
       cudaLaunchCooperativeKernel((const void*)otg::prop_kernel, dim3(grid), dim3(256), args, 0, st);
   otg::count_launch();

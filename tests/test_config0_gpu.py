@@ -9,8 +9,10 @@ libotg in oracle/_ref/ot_run_otg.
 * load/delay/ldelay/impulse of every RC node, 4 corners: within the RC
   tolerance (1e-5 relative, floor 1e-6 x the net's max |value|).
 * arrival time, slew, required time and slack of every pin, 4 corners:
-  |ours - ref| <= 1e-5 |ref| + 1e-5 (library time unit: ns), NaN where
-  the reference has none.  Each of the design's thousands of timing arcs
+  |ours - ref| <= 1e-5 s + 1e-5 (library time unit: ns), NaN where the
+  reference has none; s = |ref| for arrival time and slew, max(|ref|,
+  |ref at|) for required time and slack, which are differences of
+  path-length quantities.  Each of the design's thousands of timing arcs
   turns the RC values into delays through the same NLDM tables, so the
   RC differences carry over at the same relative size.
 """
@@ -81,8 +83,11 @@ def pins_ok(got, ref):
         g = got[k]
         assert np.array_equal(np.isnan(g), np.isnan(r)), k
         m = ~np.isnan(r)
+        # [at x4, slew x4, rat x4, slack x4]
+        scale = np.abs(r)
+        scale[8:] = np.maximum(scale[8:], np.tile(np.nan_to_num(np.abs(r[:4])), 2))
         if m.any():
-            tol = PIN_RTOL * np.abs(r[m]) + PIN_ATOL
+            tol = PIN_RTOL * scale[m] + PIN_ATOL
             worst = max(worst, float(np.max(np.abs(g[m] - r[m]) / tol)))
     return worst
 
