@@ -191,6 +191,26 @@ __device__ bool wait_value(const float* p, float& out, GridCtl* c) {
   }
 }
 
+// wait_value for two words at once: both loads in flight per poll.
+__device__ bool wait_values(const float* p, const float* q, float& x, float& y, GridCtl* c) {
+  x = ld_relaxed(p);
+  y = ld_relaxed(q);
+  if (__float_as_uint(x) != kPending && __float_as_uint(y) != kPending) return true;
+  const unsigned long long t0 = gtime();
+  for (int k = 0;; ++k) {
+    if (k >= 64) __nanosleep(64);
+    if (__float_as_uint(x) == kPending) x = ld_relaxed(p);
+    if (__float_as_uint(y) == kPending) y = ld_relaxed(q);
+    if (__float_as_uint(x) != kPending && __float_as_uint(y) != kPending) return true;
+    if (*(volatile int*)&c->abort) return false;
+    if (gtime() - t0 > kGridWaitNs) {
+      atomicExch(&c->abort, 1);
+      atomicCAS(&c->status, 0, (int)OTG_ERR_TIMEOUT);
+      return false;
+    }
+  }
+}
+
 // Order-free relax of Pin::_relax_slew/_relax_at (MIN keeps the smallest,
 // MAX the largest) and Pin::_relax_rat (the other way round); NaN is the
 // empty value and loses to any number.
@@ -242,8 +262,7 @@ __device__ bool fprop_warp(const G& G_, int v, int lane, float* at, float* slew,
         load = __ldg(G_.rc.load + 4 * (size_t)__ldg(G_.rc.nodes_start + net) + c_out);
     }
     float si, fa;
-    if (!wait_value(slew + 4 * u + 2 * el + frf, si, ctl) ||
-        !wait_value(at + 4 * u + 2 * el + frf, fa, ctl)) {
+    if (!wait_values(slew + 4 * u + 2 * el + frf, at + 4 * u + 2 * el + frf, si, fa, ctl)) {
       ok = false;
       break;
     }
@@ -305,8 +324,8 @@ __device__ bool fprop_warp(const G& G_, int v, int lane, float* at, float* slew,
       if (!(rrf == FALL_ && edge != 2) && !none(csl)) {
         const Lut lc = timing_lut(G_, t, 2, rrf, rf);
         float rat_at, rsl;
-        if (!wait_value(at + 4 * u + 2 * fel + rrf, rat_at, ctl) ||
-            !wait_value(slew + 4 * u + 2 * fel + rrf, rsl, ctl)) {
+        if (!wait_values(at + 4 * u + 2 * fel + rrf, slew + 4 * u + 2 * fel + rrf, rat_at, rsl,
+                         ctl)) {
           ok = false;
           break;
         }

@@ -82,6 +82,7 @@ class TimingGraph:
                            t(frontier0, np.int32))
         lb.run()
         lb.check()
+        self.levelizer = lb  # re-run after a topology change (otg_levelize)
         order, ends, _ = lb.result()
         assert len(order) == P, "the timing graph has a cycle"
         self.order = t(order, np.int32)
