@@ -359,6 +359,8 @@ typedef struct otg_prop_graph {
                                   constrained-pin slew first; -1: no template) */
   const float* lut_data;       /* per LUT: index_1[n1], index_2[n2], values[n1*n2] */
   float period;                /* clock period of the timing tests (NaN: no clock) */
+  int32_t num_lut_data;        /* floats in lut_data (0: unknown; the tables are then
+                                  read from global memory, not staged on chip) */
 } otg_prop_graph;
 
 typedef struct otg_prop_rc {   /* outputs of otg_rc_timing for the design's nets */

@@ -9,13 +9,17 @@
 //                of its fanins (warp-aggregated atomics: lanes that hit the
 //                same pin combine into one atomicSub); the pin whose counter
 //                reaches zero sets its bit in the "ready" bitmap
-//   compact(k+1) the ready bitmap is split into per-CTA word ranges; each CTA
-//                counts its bits, and after a grid barrier writes its pins in
-//                ascending index order at its offset -- so every level after
-//                the seed comes out sorted by pin index, deterministically --
-//                then expands them into the other bitmap.
+//   compact(k+1) the ready bitmap is split into per-CTA word ranges of C
+//                words.  The expansion that sets a pin's bit also counts it
+//                for its range, so after ONE grid barrier every CTA knows its
+//                offset (the counts of the ranges before it), writes its pins
+//                in ascending index order there -- every level after the seed
+//                comes out sorted by pin index, deterministically -- and
+//                expands them into the other bitmap.  The range counts rotate
+//                through three buffers: read in level k, filled for k+1,
+//                cleared for k+2.
 //
-// Two grid barriers per level.  The barrier is a sense-counting barrier on
+// One grid barrier per level.  The barrier is a sense-counting barrier on
 // global memory whose waits are bounded by %globaltimer: a wait that runs
 // past the limit raises an abort flag that every other wait also watches,
 // so the kernel always returns and the host sees OTG_ERR_TIMEOUT.
@@ -39,7 +43,7 @@ using LvCtl = GridCtl;
 // their bit in `bm`.  Lanes of a warp that target the same pin combine.
 __device__ __forceinline__ void expand_pin(int u, bool active, const int* fanin_start,
                                            const int* fanin, int* cnt, unsigned* bm, int n,
-                                           const int* level) {
+                                           const int* level, int* rcount, int C) {
   int e = active ? fanin_start[u] : 0;
   const int e1 = active ? fanin_start[u + 1] : 0;
   while (__any_sync(FULL, e < e1)) {
@@ -53,7 +57,10 @@ __device__ __forceinline__ void expand_pin(int u, bool active, const int* fanin_
       const int old = atomicSub(&cnt[v], k);
       // a seed pin (level 0) is never emitted twice, even if the caller's
       // out_deg disagrees with the fanin lists
-      if (old > 0 && old - k <= 0 && level[v] < 0) atomicOr(&bm[v >> 5], 1u << (v & 31));
+      if (old > 0 && old - k <= 0 && level[v] < 0) {
+        atomicOr(&bm[v >> 5], 1u << (v & 31));
+        atomicAdd(&rcount[(v >> 5) / C], 1);
+      }
     }
     e += has ? 1 : 0;
   }
@@ -65,6 +72,7 @@ __global__ void __launch_bounds__(LT) levelize_kernel(int n, const int* fanin_st
                                                       int* order, int* level, int* level_ends,
                                                       int* counts, LvCtl* ctl, int* cnt,
                                                       unsigned* bm0, unsigned* bm1, int* blk) {
+  // blk: three rotating [G] buffers of per-range ready counts
   __shared__ int wsum[LT / 32];
   __shared__ int s_total, s_off;
   const int G = gridDim.x, b = blockIdx.x, tid = threadIdx.x;
@@ -77,6 +85,8 @@ __global__ void __launch_bounds__(LT) levelize_kernel(int n, const int* fanin_st
     level[v] = -1;
   }
   for (int i = gtid; i < nw; i += gstride) bm0[i] = bm1[i] = 0u;
+  for (int i = gtid; i < 3 * G; i += gstride) blk[i] = 0;
+  const int C = max(1, (nw + G - 1) / G);  // bitmap words per CTA range
   if (!grid_barrier(ctl)) return;
   for (int k = gtid; k < first_size; k += gstride) {
     const int v = frontier0[k];
@@ -97,32 +107,23 @@ __global__ void __launch_bounds__(LT) levelize_kernel(int n, const int* fanin_st
   for (int k0 = b * LT; k0 < first_size; k0 += gstride) {
     const int k = k0 + tid;
     const bool act = k < first_size && (unsigned)order[k] < (unsigned)n;
-    expand_pin(act ? order[k] : 0, act, fanin_start, fanin, cnt, bm0, n, level);
+    expand_pin(act ? order[k] : 0, act, fanin_start, fanin, cnt, bm0, n, level, blk + G, C);
   }
   unsigned* cur = bm0;
   unsigned* nxt = bm1;
   int emitted = first_size;
   int L = 1;
-  const int w0 = (int)((long long)nw * b / G), w1 = (int)((long long)nw * (b + 1) / G);
+  const int w0 = min(nw, b * C), w1 = min(nw, (b + 1) * C);
   while (true) {
     if (!grid_barrier(ctl)) return;
-    // phase 1: count own ready bits
-    int c = 0;
-    for (int i = w0 + tid; i < w1; i += LT) c += __popc(cur[i]);
-    for (int d = 16; d >= 1; d >>= 1) c += __shfl_xor_sync(FULL, c, d);
-    if (lane == 0) wsum[w] = c;
-    __syncthreads();
-    if (tid == 0) {
-      int s = 0;
-      for (int i = 0; i < LT / 32; ++i) s += wsum[i];
-      blk[b] = s;
-    }
-    if (!grid_barrier(ctl)) return;
-    // phase 2: offset of this CTA, level total
+    int* rc_now = blk + (L % 3) * G;         // counts of this level's ranges
+    int* rc_next = blk + ((L + 1) % 3) * G;  // filled by this level's expansion
+    if (tid == 0) blk[((L + 2) % 3) * G + b] = 0;  // read a level ago, filled next level
+    // offset of this CTA, level total
     if (tid < 32) {
       int before = 0, total = 0;
       for (int i = lane; i < G; i += 32) {
-        const int x = blk[i];
+        const int x = __ldcg(rc_now + i);
         total += x;
         if (i < b) before += x;
       }
@@ -157,8 +158,6 @@ __global__ void __launch_bounds__(LT) levelize_kernel(int n, const int* fanin_st
       __syncthreads();
       int pos = run + wb + x - pc;
       unsigned bits = word;
-      int pins[32];
-      int np = 0;
       while (bits) {
         const int bit = __ffs(bits) - 1;
         bits &= bits - 1;
@@ -170,19 +169,17 @@ __global__ void __launch_bounds__(LT) levelize_kernel(int n, const int* fanin_st
         }
         ++pos;
         level[v] = L;
-        pins[np++] = v;
       }
       if (i < w1) cur[i] = 0u;  // ready for reuse two levels on
-      // expand: one pin per lane per step
-      int maxp = np;
-      for (int d = 16; d >= 1; d >>= 1) maxp = max(maxp, __shfl_xor_sync(FULL, maxp, d));
-      for (int k = 0; k < maxp; ++k) {
-        const bool act = k < np;
-        int u = 0;
-#pragma unroll
-        for (int q = 0; q < 32; ++q)
-          if (q == k) u = pins[q];
-        expand_pin(act ? u : 0, act, fanin_start, fanin, cnt, nxt, n, level);
+      __syncthreads();  // the tile's slice of `order` is visible to the CTA
+      // expand the tile's pins, one per thread (a word's pins would
+      // otherwise go one after another through their atomics)
+      const int tn = min(tt, n - run);
+      for (int k0 = 0; k0 < tn; k0 += LT) {
+        const int k = k0 + tid;
+        const bool act = k < tn;
+        expand_pin(act ? order[run + k] : 0, act, fanin_start, fanin, cnt, nxt, n, level,
+                   rc_next, C);
       }
       run += tt;
     }
@@ -237,7 +234,7 @@ LvWs lv_ws(int n, int G) {
   const size_t nw = ((size_t)n + 31) / 32 + 1;
   l.bm0 = o; o = align256(o + 4 * nw);
   l.bm1 = o; o = align256(o + 4 * nw);
-  l.blk = o; o = align256(o + 4 * (size_t)G);
+  l.blk = o; o = align256(o + 12 * (size_t)G);  // three rotating [G] count buffers
   l.total = o;
   return l;
 }

@@ -67,11 +67,13 @@ __device__ float interpolate(float x, float x1, float x2, float y1, float y2) {
   return __fadd_rn(y1, __fmul_rn(__fsub_rn(x, x1), slope));
 }
 
+// Table reads go through a generic pointer: shared memory when the
+// library is staged on chip, else global memory (cached in L1).
 __device__ int lower_bound(const float* a, int n, float v) {
   int lo = 0, hi = n;
   while (lo < hi) {
     const int mid = (lo + hi) >> 1;
-    if (__ldg(a + mid) < v) lo = mid + 1; else hi = mid;
+    if (a[mid] < v) lo = mid + 1; else hi = mid;
   }
   return lo;
 }
@@ -98,18 +100,15 @@ __device__ float lut_eval(const Lut& m, const float* data, float v1, float v2) {
   const float* i2 = i1 + n1;
   const float* tb = i2 + n2;
   if (n1 < 1 || n2 < 1) return nanf("");
-  if (n1 == 1 && n2 == 1) return __ldg(tb);
+  if (n1 == 1 && n2 == 1) return tb[0];
   const int a1 = max(1, min(lower_bound(i1, n1, v1), n1 - 1));
   const int a2 = max(1, min(lower_bound(i2, n2, v2), n2 - 1));
-  if (n1 == 1)
-    return interpolate(v2, __ldg(i2 + a2 - 1), __ldg(i2 + a2), __ldg(tb + a2 - 1), __ldg(tb + a2));
-  const float x1 = __ldg(i1 + a1 - 1), x2 = __ldg(i1 + a1);
-  if (n2 == 1) return interpolate(v1, x1, x2, __ldg(tb + (a1 - 1) * n2), __ldg(tb + a1 * n2));
-  const float lo = interpolate(v1, x1, x2, __ldg(tb + (a1 - 1) * n2 + a2 - 1),
-                               __ldg(tb + a1 * n2 + a2 - 1));
-  const float hi = interpolate(v1, x1, x2, __ldg(tb + (a1 - 1) * n2 + a2),
-                               __ldg(tb + a1 * n2 + a2));
-  return interpolate(v2, __ldg(i2 + a2 - 1), __ldg(i2 + a2), lo, hi);
+  if (n1 == 1) return interpolate(v2, i2[a2 - 1], i2[a2], tb[a2 - 1], tb[a2]);
+  const float x1 = i1[a1 - 1], x2 = i1[a1];
+  if (n2 == 1) return interpolate(v1, x1, x2, tb[(a1 - 1) * n2], tb[a1 * n2]);
+  const float lo = interpolate(v1, x1, x2, tb[(a1 - 1) * n2 + a2 - 1], tb[a1 * n2 + a2 - 1]);
+  const float hi = interpolate(v1, x1, x2, tb[(a1 - 1) * n2 + a2], tb[a1 * n2 + a2]);
+  return interpolate(v2, i2[a2 - 1], i2[a2], lo, hi);
 }
 
 // timing record: [sense, edge, constraint, lut x6]
@@ -136,14 +135,24 @@ __device__ Lut timing_lut(const G& G_, int t, int which, int irf, int orf) {
 
 // The query itself; (a, b) = (slew, load) for delay and slew, (related
 // slew, constrained slew) for constraint.
-__device__ float timing_value(const G& G_, const Lut& m, float a, float b) {
+// Where the tables are read: the staged copy (floats [0, n)) for a table
+// that lies inside it, global memory otherwise.
+struct LutSrc {
+  const float* smem;
+  int n;
+  const float* gmem;
+};
+
+__device__ float timing_value(const LutSrc& src, const Lut& m, float a, float b) {
   if (m.n1 < 0) return nanf("");
+  const bool staged = m.off >= 0 && m.off + m.n1 + m.n2 + m.n1 * m.n2 <= src.n;
+  const float* lutd = staged ? src.smem : src.gmem;
   if (m.var < 0) {  // no template: a scalar only
-    if (m.n1 == 1 && m.n2 == 1) return __ldg(G_.g.lut_data + m.off + 2);
+    if (m.n1 == 1 && m.n2 == 1) return lutd[m.off + 2];
     return nanf("");
   }
   // var 0: (slew | related) first; var 1: (load | constrained) first
-  return m.var == 0 ? lut_eval(m, G_.g.lut_data, a, b) : lut_eval(m, G_.g.lut_data, b, a);
+  return m.var == 0 ? lut_eval(m, lutd, a, b) : lut_eval(m, lutd, b, a);
 }
 
 // RC node of a net arc's sink: global BFS slot (-1: none)
@@ -225,8 +234,9 @@ __device__ __forceinline__ float relax_bwd(int el, float cur, float v) {
 // and _fprop_test.  Lane j of a pass takes fanin arc j/8 and the combination
 // (el, frf, trf) = bits (2, 1, 0) of j; its slew and arrival candidates go to
 // output corner (el, trf).  Returns false if a wait gave up.
-__device__ bool fprop_warp(const G& G_, int v, int lane, float* at, float* slew, float* rat,
-                           float* arc_delay, float* test_rat, GridCtl* ctl) {
+__device__ bool fprop_warp(const G& G_, const LutSrc& lutd, int v, int lane, float* at,
+                           float* slew, float* rat, float* arc_delay, float* test_rat,
+                           GridCtl* ctl) {
   const otg_prop_graph& g = G_.g;
   const int el = (lane >> 2) & 1, frf = (lane >> 1) & 1, trf = lane & 1;
   const int c_out = 2 * el + trf;
@@ -253,18 +263,55 @@ __device__ bool fprop_warp(const G& G_, int v, int lane, float* at, float* slew,
         imp = __ldg(G_.rc.impulse + 4 * (size_t)s + c_out);
         d = __ldg(G_.rc.delay + 4 * (size_t)s + c_out);
       }
-    } else {
+    }
+    // A cell arc out of a pin whose only fanin is a net arc (a gate's input
+    // pin) reads through it: the lane waits on the net's driver and derives
+    // the input pin's slew and arrival time at (el, frf) exactly as that
+    // pin's own warp does (one candidate relaxed against the assertion).
+    // The input pin still stores its own values; this only shortens the
+    // chain of waits.
+    int src = u;
+    bool thru = false;
+    float t_imp = 0.0f, t_d = nanf(""), t_psl = nanf(""), t_pat = nanf("");
+    int t_s = -1;
+    if (kind != 0) {
       const int t = __ldg(g.arc_timing + 2 * arc + el);
       ls = timing_lut(G_, t, 1, frf, trf);
       ld = timing_lut(G_, t, 0, frf, trf);
       const int net = __ldg(g.arc_net + arc);
       if (net >= 0 && t >= 0)
         load = __ldg(G_.rc.load + 4 * (size_t)__ldg(G_.rc.nodes_start + net) + c_out);
+      const int uf0 = __ldg(g.fanin_start + u);
+      if (__ldg(g.fanin_start + u + 1) - uf0 == 1) {
+        const int a0 = __ldg(g.fanin + uf0);
+        if (__ldg(g.arc_kind + a0) == 0) {
+          const int c_in = 2 * el + frf;
+          thru = true;
+          src = __ldg(g.arc_from + a0);
+          t_s = rc_slot(G_, a0);
+          if (t_s >= 0) {
+            t_imp = __ldg(G_.rc.impulse + 4 * (size_t)t_s + c_in);
+            t_d = __ldg(G_.rc.delay + 4 * (size_t)t_s + c_in);
+          }
+          t_psl = __ldg(g.pi_slew + 4 * u + c_in);
+          t_pat = __ldg(g.pi_at + 4 * u + c_in);
+        }
+      }
     }
     float si, fa;
-    if (!wait_values(slew + 4 * u + 2 * el + frf, at + 4 * u + 2 * el + frf, si, fa, ctl)) {
+    if (!wait_values(slew + 4 * src + 2 * el + frf, at + 4 * src + 2 * el + frf, si, fa, ctl)) {
       ok = false;
       break;
+    }
+    if (thru) {
+      float so_u = nanf(""), at_u = nanf("");
+      if (t_s >= 0 && !none(si)) {
+        const float r = sqrtf(__fadd_rn(__fmul_rn(si, si), t_imp));
+        so_u = si < 0.0f ? -r : r;
+      }
+      if (!none(fa) && !none(t_d)) at_u = __fadd_rn(t_d, fa);
+      si = relax_fwd(el, t_psl, so_u);
+      fa = relax_fwd(el, t_pat, at_u);
     }
     if (kind == 0) {
       // sign(si) * sqrt(si^2 + impulse) at the sink (FlatRct::slew)
@@ -273,8 +320,8 @@ __device__ bool fprop_warp(const G& G_, int v, int lane, float* at, float* slew,
         so = si < 0.0f ? -r : r;
       }
     } else if (!none(si)) {
-      so = timing_value(G_, ls, si, load);
-      d = timing_value(G_, ld, si, load);
+      so = timing_value(lutd, ls, si, load);
+      d = timing_value(lutd, ld, si, load);
     } else {
       d = nanf("");
     }
@@ -331,7 +378,7 @@ __device__ bool fprop_warp(const G& G_, int v, int lane, float* at, float* slew,
         }
         if (!none(rat_at) && !none(rsl)) {
           const float related = tel == MIN_ ? rat_at : __fadd_rn(rat_at, g.period);
-          const float cons = timing_value(G_, lc, rsl, csl);
+          const float cons = timing_value(lutd, lc, rsl, csl);
           if (!none(cons))
             val = tel == MIN_ ? __fadd_rn(cons, related) : __fsub_rn(related, cons);
         }
@@ -443,14 +490,20 @@ __global__ void prop_init_kernel(float4* at, float4* slew, int num_pins, GridCtl
 __global__ void __launch_bounds__(256) prop_kernel(G G_, const int* order, int num_pins,
                                                    float* at, float* slew, float* rat,
                                                    float* slack, float* arc_delay,
-                                                   float* test_rat, GridCtl* ctl) {
+                                                   float* test_rat, GridCtl* ctl, int lut_smem) {
+  // the library's tables, staged on chip when the caller gave their size
+  // and they fit (lut_smem floats)
+  extern __shared__ float s_lut[];
+  for (int i = threadIdx.x; i < lut_smem; i += blockDim.x) s_lut[i] = __ldg(G_.g.lut_data + i);
+  __syncthreads();
+  const LutSrc lutd{s_lut, lut_smem, G_.g.lut_data};
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int W = (gridDim.x * blockDim.x) >> 5;
   bool ok = true;
   for (int j = warp; ok && j < num_pins; j += W)
-    ok = fprop_warp(G_, __ldg(order + num_pins - 1 - j), lane, at, slew, rat, arc_delay, test_rat,
-                    ctl);
+    ok = fprop_warp(G_, lutd, __ldg(order + num_pins - 1 - j), lane, at, slew, rat, arc_delay,
+                    test_rat, ctl);
   // the barrier also lets every CTA leave together when a wait gave up
   if (!grid_barrier(ctl) || !ok) return;
   for (int j = warp; ok && j < num_pins; j += W)
@@ -459,8 +512,13 @@ __global__ void __launch_bounds__(256) prop_kernel(G G_, const int* order, int n
 
 size_t align256p(size_t x) { return (x + 255) & ~(size_t)255; }
 
+// Tables up to this many floats are staged in shared memory (32 KB per
+// CTA keeps five 256-thread CTAs per SM).
+constexpr int kLutSmemFloats = 8192;
+
 struct PropDev {
-  int sms = 0, occ = 0;
+  int sms = 0;
+  int occ[2] = {0, 0};  // CTAs per SM without / with the staged tables
   bool init = false;
 };
 PropDev g_pdev[64];
@@ -505,18 +563,24 @@ otg_status otg_propagate(const otg_prop_graph* g, const otg_prop_rc* rc, const i
   otg::PropDev& d = otg::g_pdev[dev & 63];
   if (!d.init) {
     cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d.occ, otg::prop_kernel, 256, 0);
+    cudaFuncSetAttribute(otg::prop_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         4 * otg::kLutSmemFloats);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d.occ[0], otg::prop_kernel, 256, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d.occ[1], otg::prop_kernel, 256,
+                                                  4 * otg::kLutSmemFloats);
     d.init = true;
   }
+  int lut_smem = g->num_lut_data > 0 && g->num_lut_data <= otg::kLutSmemFloats ? g->num_lut_data : 0;
+  const int occ = lut_smem ? d.occ[1] : d.occ[0];
   // every CTA resident (the schedule and the barrier rely on it), no more
   // warps than pins
-  const int grid = std::max(1, std::min(d.sms * std::max(d.occ, 1), (P + 7) / 8));
+  const int grid = std::max(1, std::min(d.sms * std::max(occ, 1), (P + 7) / 8));
   otg::G G_{*g, *rc};
   int num_pins = P;
-  void* args[] = {&G_,    (void*)&order, &num_pins, &at,       &slew,
-                  &rat,   &slack,        &arc_delay, &test_rat, &ctl};
-  const cudaError_t e =
-      cudaLaunchCooperativeKernel((const void*)otg::prop_kernel, dim3(grid), dim3(256), args, 0, st);
+  void* args[] = {&G_,  (void*)&order, &num_pins,  &at,  &slew,    &rat,
+                  &slack, &arc_delay,  &test_rat,  &ctl, &lut_smem};
+  const cudaError_t e = cudaLaunchCooperativeKernel(
+      (const void*)otg::prop_kernel, dim3(grid), dim3(256), args, 4 * (size_t)lut_smem, st);
   otg::count_launch();
   if (e != cudaSuccess) {
     cudaGetLastError();

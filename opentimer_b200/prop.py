@@ -23,7 +23,8 @@ class PropGraph(ctypes.Structure):
         (k, ctypes.c_void_p) for k in
         ["arc_from", "arc_to", "arc_kind", "arc_timing", "arc_net", "arc_node", "fanin_start",
          "fanin", "fanout_start", "fanout", "test_arc", "test_start", "test_of_pin", "pi_at",
-         "pi_slew", "po_rat", "timing", "lut_meta", "lut_data"]] + [("period", ctypes.c_float)]
+         "pi_slew", "po_rat", "timing", "lut_meta", "lut_data"]] + [
+        ("period", ctypes.c_float), ("num_lut_data", ctypes.c_int32)]
 
 
 class PropRc(ctypes.Structure):
@@ -72,7 +73,7 @@ class TimingGraph:
                                   "arc_node", "fanin_start", "fanin", "fanout_start", "fanout",
                                   "test_arc", "test_start", "test_of_pin", "pi_at", "pi_slew",
                                   "po_rat", "timing", "lut_meta", "lut_data"]],
-                               float(a["period"]))
+                               float(a["period"]), int(np.size(a["lut_data"])))
         # levels over the pin graph: a pin's level is its longest path to a pin
         # without fanout (otg_levelize, the reference's frontier rule)
         fin_src = np.asarray(a["arc_from"], np.int32)[fanin]
