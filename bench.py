@@ -273,7 +273,11 @@ def run_ours(args, world, rank, local):
 
     # ---- workload (per rank: its own 1M nets -> weak scaling)
     tuning, tune_s = None, 0.0
-    if not args.no_autotune:
+    if args.tuning:  # a saved tuning (a profiler run replays the timed run's choice)
+        src = args.tuning
+        tuning = json.load(open(src)) if os.path.exists(src) else json.loads(src)
+        otg.set_tuning(tuning)
+    elif not args.no_autotune:
         tuning, tune_s = autotune_on(SEED + 100 + rank, min(TUNE_NETS, args.nets), args.min_nodes,
                                      args.max_nodes, dev)
     ns_np = rank_nets(rank, args.nets, args.min_nodes, args.max_nodes)
@@ -330,7 +334,8 @@ def run_ours(args, world, rank, local):
                    "num_nets_per_gpu": N, "total_nodes_per_gpu": V, "sinks_per_gpu": S,
                    "l2": "inputs and outputs (>60 GB) far exceed L2; no flush needed",
                    "tuning": tuning or "default",
-                   "autotune": (f"otg_rc_autotune on {min(TUNE_NETS, args.nets)} nets of the same "
+                   "autotune": ("given (--tuning)" if args.tuning else
+                                f"otg_rc_autotune on {min(TUNE_NETS, args.nets)} nets of the same "
                                 f"distribution (another seed), {tune_s:.1f} s, before warm-up")
                    if tuning else "off",
                    "parallelism": f"replicas x{world} (nets shard with no collective)"},
@@ -759,6 +764,8 @@ def main():
     ap.add_argument("--no-incremental", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--tuning", default=None,
+                    help="RC-pass tuning to apply instead of autotuning (JSON or a JSON file)")
     ap.add_argument("--no-spef", action="store_true")
     ap.add_argument("--no-full-update", action="store_true")
     # smaller cases (profiling); the defaults are the benchmark workload

@@ -43,9 +43,11 @@ def _csr(keys, n):
 class TimingGraph:
     """arrays: arc_from, arc_to, arc_kind, arc_timing [A,2], arc_net,
     arc_node, test_arc, pi_at, pi_slew, po_rat [P,4], timing [R,9],
-    lut_meta [L,4], lut_data, period; num_pins."""
+    lut_meta [L,4], lut_data, period; num_pins.  order: a pin order to use
+    instead of levelizing (every pin after all of its fanouts); it is not
+    checked, and one that breaks the rule ends in OTG_ERR_TIMEOUT."""
 
-    def __init__(self, arrays, device="cuda"):
+    def __init__(self, arrays, device="cuda", order=None):
         import torch
         a = arrays
         P = int(a["num_pins"])
@@ -74,6 +76,16 @@ class TimingGraph:
                                   "test_arc", "test_start", "test_of_pin", "pi_at", "pi_slew",
                                   "po_rat", "timing", "lut_meta", "lut_data"]],
                                float(a["period"]), int(np.size(a["lut_data"])))
+        ws = ctypes.c_size_t()
+        check("otg_prop_workspace_size", lib().otg_prop_workspace_size(P, A, len(test_arc),
+                                                                       ctypes.byref(ws)))
+        self.workspace = torch.empty(max(ws.value, 256), dtype=torch.uint8, device=device)
+        self.out = {k: torch.empty(P, NC, dtype=torch.float32, device=device)
+                    for k in ("at", "slew", "rat", "slack")}
+        if order is not None:
+            assert len(order) == P
+            self.order, self.levelizer, self.num_levels = t(order, np.int32), None, None
+            return
         # levels over the pin graph: a pin's level is its longest path to a pin
         # without fanout (otg_levelize, the reference's frontier rule)
         fin_src = np.asarray(a["arc_from"], np.int32)[fanin]
@@ -89,12 +101,6 @@ class TimingGraph:
         self.order = t(order, np.int32)
         self.level_ends = t(ends, np.int32)
         self.num_levels = len(ends) - 1
-        ws = ctypes.c_size_t()
-        check("otg_prop_workspace_size", lib().otg_prop_workspace_size(P, A, len(test_arc),
-                                                                       ctypes.byref(ws)))
-        self.workspace = torch.empty(max(ws.value, 256), dtype=torch.uint8, device=device)
-        self.out = {k: torch.empty(P, NC, dtype=torch.float32, device=device)
-                    for k in ("at", "slew", "rat", "slack")}
 
     def propagate(self, batch, stream=None):
         """Forward and backward propagation on the RC outputs of `batch`

@@ -193,3 +193,45 @@ def test_own_graph_matches_reference_timer(design, tmp_path):
     w_cpu = compare(names, out, ref_cpu)
     print(f"own graph: err/tol vs reference GPU path {w_gpu}, vs CPU path {w_cpu}")
     assert max(w_gpu.values()) <= 1.0 and max(w_cpu.values()) <= 1.0
+
+
+def _chain_graph(cyclic):
+    """Two pins joined by net arcs without RC nodes: 0 -> 1, plus 1 -> 0
+    when cyclic.  Pin 0 carries PI assertions."""
+    arcs = [(0, 1), (1, 0)] if cyclic else [(0, 1)]
+    A = len(arcs)
+    nan4 = np.full((2, 4), np.nan, np.float32)
+    pi_at, pi_slew = nan4.copy(), nan4.copy()
+    pi_at[0], pi_slew[0] = 1.0, 2.0
+    return dict(num_pins=2, arc_from=np.array([f for f, _ in arcs], np.int32),
+                arc_to=np.array([t for _, t in arcs], np.int32), arc_kind=np.zeros(A, np.int32),
+                arc_timing=np.full((A, 2), -1, np.int32), arc_net=np.full(A, -1, np.int32),
+                arc_node=np.full(A, -1, np.int32), test_arc=np.zeros(0, np.int32),
+                pi_at=pi_at, pi_slew=pi_slew, po_rat=nan4.copy(),
+                timing=np.zeros((0, 9), np.int32), lut_meta=np.zeros((0, 4), np.int32),
+                lut_data=np.zeros(0, np.float32), period=np.nan)
+
+
+def test_bounded_wait_gives_up_on_a_cycle(cuda):
+    """A pin order that breaks the dataflow rule (here a two-pin cycle, so
+    each pin waits on the other) ends every wait after the 2 s limit with
+    OTG_ERR_TIMEOUT; the context stays usable for the next propagation."""
+    import time
+    import torch
+    from opentimer_b200.prop import TimingGraph
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()  # noqa: E731
+    batch = otg.RcBatch(t(np.array([0, 2], np.int32)), t(np.array([[0, 1]], np.int32)),
+                        t(np.zeros(1, np.int32)), t(np.ones(1, np.float32)),
+                        t(np.ones((2, 4), np.float32)))
+    batch.run()
+    batch.check()
+    g = TimingGraph(_chain_graph(True), order=np.array([1, 0], np.int32))
+    t0 = time.time()
+    g.propagate(batch)
+    with pytest.raises(otg.OtgError) as e:
+        g.check()
+    assert e.value.code == 6  # OTG_ERR_TIMEOUT
+    assert time.time() - t0 < 30
+    out = TimingGraph(_chain_graph(False)).propagate(batch).result()
+    assert np.all(out["at"][0] == 1.0) and np.all(out["slew"][0] == 2.0)
+    assert np.all(np.isnan(out["at"][1]))  # a net arc without an RC node carries nothing
