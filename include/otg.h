@@ -112,6 +112,27 @@ otg_status otg_rc_timing_subset(const otg_rc_forest* forest, int32_t max_net_nod
                                 int32_t max_listed, void* workspace, size_t workspace_bytes,
                                 otg_stream_t stream);
 
+/*
+ * otg_rc_move_nets -- copies whole nets from forest src into forest dst on
+ * the device: every net i of dst with src_net[i] >= 0 receives net
+ * src_net[i] of src (root, edges, res and cap; with copy_outputs also
+ * node2bfs, pid, load, delay, ldelay and impulse).  Nets with src_net[i] < 0
+ * are left alone.  A size mismatch or an out-of-range src_net entry skips
+ * that net and sets *status (device memory, caller-zeroed) to
+ * OTG_ERR_INVALID.  Asynchronous; src_net is device memory [dst nets].
+ *
+ * The relayout step of incremental SPEF ingestion.  The reference
+ * re-attaches each changed net's parasitics (Timer::_read_spef,
+ * ot/timer/spef.cpp:40-53) and re-times on the next update_timing; here
+ * the unchanged nets move into the new layout with their results, the
+ * changed nets' inputs move in from a staging forest, and
+ * otg_rc_timing_subset re-times only those.  No reference counterpart as
+ * one call.
+ */
+otg_status otg_rc_move_nets(const otg_rc_forest* src, const otg_rc_forest* dst,
+                            const int32_t* src_net, int32_t copy_outputs, int32_t* status,
+                            otg_stream_t stream);
+
 /* Synchronizes `stream` and returns the first device-side error recorded in
  * `workspace` by the last otg_rc_timing call (OTG_OK if none); *bad_net (if
  * non-NULL) gets the offending net index or -1. */
@@ -338,8 +359,9 @@ typedef struct otg_prop_graph {
   const int32_t* arc_timing;   /* [A][2] cell arcs: timing record per split (-1 none) */
   const int32_t* arc_net;      /* [A] net arcs: the forest net; cell arcs: the net the
                                   arc drives (its load), -1 none (load 0) */
-  const int32_t* arc_node;     /* [A] net arcs: the sink's global RC node index
-                                  (nodes_start[net] + local id), -1 not in the tree */
+  const int32_t* arc_node;     /* [A] net arcs: the sink's local RC node id in its net
+                                  (unchanged when nets move, otg_rc_move_nets), -1 not
+                                  in the tree */
   const int32_t* fanin_start;  /* [P+1] CSR of the arcs into each pin */
   const int32_t* fanin;
   const int32_t* fanout_start; /* [P+1] CSR of the arcs out of each pin */

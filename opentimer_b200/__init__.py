@@ -158,6 +158,72 @@ class RcBatch:
         code, net = self.status(stream)
         if code != 0:
             raise OtgError(f"otg_rc_timing (net {net})", code)
+        moved = getattr(self, "_move_status", None)
+        if moved is not None and int(moved.item()) != 0:
+            raise OtgError("otg_rc_move_nets", int(moved.item()))
+
+    def replace_nets(self, nets, nodes_start, edges, roots, res, cap, stream=None):
+        """Incremental SPEF ingestion: a new batch in which the forest nets
+        `nets` (distinct indices) carry new RC trees, given as a forest of
+        len(nets) nets in the constructor's layout (numpy arrays or CUDA
+        tensors), while every other net keeps its tree AND its results,
+        moved into the new layout on the device (otg_rc_move_nets).  Only
+        the replaced nets are re-timed (otg_rc_timing_subset), so the
+        result equals a full pass over the new forest.  This batch must
+        have run; sink arrays are not carried over."""
+        import torch
+        assert self.sinks_start is None, "sink arrays are not carried over"
+        dev = self.cap.device
+        nets = np.asarray(nets, np.int64).reshape(-1)
+        K, N = len(nets), self.num_nets
+        assert len(np.unique(nets)) == K, "a net is replaced twice"
+        assert K == 0 or (nets.min() >= 0 and nets.max() < N)
+
+        def t(a, dt):
+            if torch.is_tensor(a):
+                return a.to(dev).contiguous()
+            return torch.from_numpy(np.ascontiguousarray(a, dt)).to(dev)
+        host = lambda a: a.cpu().numpy() if torch.is_tensor(a) else np.asarray(a)  # noqa: E731
+        sub = [t(nodes_start, np.int32), t(edges, np.int32), t(roots, np.int32),
+               t(res, np.float32), t(cap, np.float32)]
+        sizes = host(self.nodes_start).astype(np.int64)
+        sizes = sizes[1:] - sizes[:-1]
+        sub_sizes = np.diff(host(nodes_start).astype(np.int64))
+        assert len(sub_sizes) == K
+        sizes[nets] = sub_sizes
+        ns_new = np.zeros(N + 1, np.int64)
+        np.cumsum(sizes, out=ns_new[1:])
+        assert ns_new[-1] < 2 ** 31, "32-bit node offsets"
+        V, E = int(ns_new[-1]), int(ns_new[-1]) - N
+        new = RcBatch(t(ns_new, np.int32), torch.empty((E, 2), dtype=torch.int32, device=dev),
+                      torch.empty(N, dtype=torch.int32, device=dev),
+                      torch.empty(E, dtype=torch.float32, device=dev),
+                      torch.empty((V, NC), dtype=torch.float32, device=dev),
+                      max_net_nodes=int(sizes.max()) if N else 1)
+        status = torch.zeros(1, dtype=torch.int32, device=dev)
+        keep = np.arange(N, dtype=np.int32)
+        keep[nets] = -1
+        put = np.full(N, -1, np.int32)
+        put[nets] = np.arange(K, dtype=np.int32)
+        keep_d, put_d = t(keep, np.int32), t(put, np.int32)
+        s = _stream(stream)
+        check("otg_rc_move_nets", lib().otg_rc_move_nets(
+            ctypes.byref(self._forest), ctypes.byref(new._forest), _ptr(keep_d), 1, _ptr(status), s))
+        staging = RcForest(K, int(host(nodes_start)[-1]) if K else 0,
+                           *[x.data_ptr() for x in sub], *([None] * 10))
+        check("otg_rc_move_nets", lib().otg_rc_move_nets(
+            ctypes.byref(staging), ctypes.byref(new._forest), _ptr(put_d), 0, _ptr(status), s))
+        net_list = t(nets, np.int32)
+        num = torch.tensor([K], dtype=torch.int32, device=dev)
+        if K:
+            check("otg_rc_timing_subset", lib().otg_rc_timing_subset(
+                ctypes.byref(new._forest), new.max_net_nodes, _ptr(net_list), _ptr(num), K,
+                _ptr(new.workspace), new.workspace.numel(), s))
+        else:  # nothing re-timed: clear the status word the moves leave alone
+            new.workspace.zero_()
+        # the staging tensors live until the stream has used them
+        new._move_status, new._keep = status, (sub, keep_d, put_d, net_list, num)
+        return new
 
 
 def rc_timing(nodes_start, edges, roots, res, cap, **kw):

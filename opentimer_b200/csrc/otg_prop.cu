@@ -155,12 +155,13 @@ __device__ float timing_value(const LutSrc& src, const Lut& m, float a, float b)
   return m.var == 0 ? lut_eval(m, lutd, a, b) : lut_eval(m, lutd, b, a);
 }
 
-// RC node of a net arc's sink: global BFS slot (-1: none)
+// RC node of a net arc's sink (arc_node: its local id in the net) as a
+// global BFS slot (-1: none)
 __device__ __forceinline__ int rc_slot(const G& G_, int arc) {
   const int node = __ldg(G_.g.arc_node + arc);
   if (node < 0) return -1;
-  const int net = __ldg(G_.g.arc_net + arc);
-  return __ldg(G_.rc.nodes_start + net) + __ldg(G_.rc.node2bfs + node);
+  const int b = __ldg(G_.rc.nodes_start + __ldg(G_.g.arc_net + arc));
+  return b + __ldg(G_.rc.node2bfs + b + node);
 }
 
 constexpr unsigned kPending = 0x7fbadbadu;  // "not yet computed"

@@ -286,6 +286,21 @@ def spef(rng, nets):
     return "\n".join(out) + "\n"
 
 
+def change_spef(design, path, frac=0.01, seed=0):
+    """Writes a TAU15-style change SPEF: new random RC trees (same pins,
+    new internal nodes, topology, R and C) for a seeded fraction of the
+    design's nets (`design` as filled by write_design's keep).  Returns the
+    changed net names, in file order."""
+    rng = np.random.default_rng(seed)
+    names = sorted(design["nets"])
+    k = max(1, int(round(frac * len(names))))
+    chosen = sorted(rng.choice(len(names), size=k, replace=False).tolist())
+    nets = {names[i]: design["nets"][names[i]] for i in chosen}
+    with open(path, "w") as f:
+        f.write(spef(rng, nets))
+    return [names[i] for i in chosen]
+
+
 def write_design(dirpath, seed=2024, gates=2000, keep=None):
     """Writes the design files; returns a summary.  With `keep` (a dict), it
     also receives the in-memory design for timing_graph/pin_caps."""

@@ -115,6 +115,14 @@ class TimingGraph:
             _stream(stream)))
         return self
 
+    def set_arc_nodes(self, arcs, nodes):
+        """New sink node ids (local to their nets) for some net arcs, as
+        after an incremental SPEF replaced their nets' trees."""
+        import torch
+        arcs = torch.as_tensor(np.asarray(arcs, np.int64), device=self.dev["arc_node"].device)
+        self.dev["arc_node"][arcs] = torch.as_tensor(np.asarray(nodes, np.int32),
+                                                     device=arcs.device)
+
     def check(self, stream=None):
         """Synchronizes; raises if a bounded wait of the last propagation
         gave up (OTG_ERR_TIMEOUT)."""
@@ -128,8 +136,8 @@ class TimingGraph:
 def rc_inputs(spef, pin_caps):
     """Flat RC inputs from read_spef's output plus each non-root pin's cap
     (pin_caps: name -> [4]), as the flat path adds them (ot/timer/
-    net.cpp:433-446).  Returns (cap [V,4], node_of {(net, pin name):
-    global node})."""
+    net.cpp:433-446).  Returns (cap [V,4], node_of {(net, pin name): the
+    pin's local node id in the net})."""
     ns, ps = spef["nodes_start"], spef["pins_start"]
     cap = spef["cap"].copy()
     node_of = {}
@@ -140,10 +148,39 @@ def rc_inputs(spef, pin_caps):
             node = int(spef["pin_node"][q])
             if node < 0:
                 continue
-            node_of[(i, names[q])] = b + node
+            node_of[(i, names[q])] = node
             if node != spef["roots"][i] and names[q] in pin_caps:
                 cap[b + node] = cap[b + node] + np.asarray(pin_caps[names[q]], np.float32)
     return cap, node_of
+
+
+def change_nets(spef_change, net_index, pin_caps):
+    """Reads a change SPEF (read_spef output) against a design whose forest
+    nets are named by net_index {name: forest net}.  Returns (nets, forest,
+    node_of): the forest indices of the nets it names (unknown names are
+    skipped, as Timer::_read_spef does, ot/timer/spef.cpp:40-53), their new
+    trees as a forest in file order (nodes_start, edges, roots, res, cap
+    with the pin caps added) for RcBatch.replace_nets, and node_of
+    {(forest net, pin name): local node} for the arcs into them."""
+    f = spef_change
+    cap, node_local = rc_inputs(f, pin_caps)
+    ns = f["nodes_start"]
+    keep = [i for i, n in enumerate(f["net_names"]) if n in net_index]
+    nets = np.array([net_index[f["net_names"][i]] for i in keep], np.int64)
+    sizes = np.array([ns[i + 1] - ns[i] for i in keep], np.int64)
+    sub_ns = np.zeros(len(keep) + 1, np.int64)
+    np.cumsum(sizes, out=sub_ns[1:])
+    node_rows = np.concatenate([np.arange(ns[i], ns[i + 1]) for i in keep]) if keep else \
+        np.zeros(0, np.int64)
+    edge_rows = np.concatenate([np.arange(ns[i] - i, ns[i + 1] - i - 1) for i in keep]) if keep \
+        else np.zeros(0, np.int64)
+    forest = (sub_ns.astype(np.int32), f["edges"][edge_rows].copy(),
+              np.asarray(f["roots"])[keep].astype(np.int32), f["res"][edge_rows].copy(),
+              cap[node_rows].copy())
+    back = {i: k for k, i in enumerate(keep)}
+    node_of = {(int(nets[back[i]]), pin): node for (i, pin), node in node_local.items()
+               if i in back}
+    return nets, forest, node_of
 
 
 def attach_nets(arrays, pin_names, pin_net_names, spef, node_of):

@@ -148,12 +148,22 @@ static void dump_graph(ot::Timer& timer, const char* path) {
 }
 
 int main(int argc, char** argv) {
-  if (argc != 4 && argc != 5) {
-    std::fprintf(stderr, "usage: %s <dir> cpu|cuda <out> [graph]\n", argv[0]);
+  if (argc < 4) {
+    std::fprintf(stderr, "usage: %s <dir> cpu|cuda <out> [graph] [change=<spef>]...\n",
+                 argv[0]);
     return 2;
   }
   const std::string dir = argv[1];
   const bool cuda = std::string(argv[2]) == "cuda";
+  // optional: a graph dump path, and change SPEFs applied after the first
+  // update (read_spef + update_timing, as the TAU15 ops files do)
+  const char* graph_path = nullptr;
+  std::vector<std::string> changes;
+  for (int a = 4; a < argc; ++a) {
+    const std::string s = argv[a];
+    if (s.rfind("change=", 0) == 0) changes.push_back(s.substr(7));
+    else graph_path = argv[a];
+  }
   ot::Timer timer;
   timer.read_celllib(dir + "/early.lib", ot::MIN)
       .read_celllib(dir + "/late.lib", ot::MAX)
@@ -166,6 +176,14 @@ int main(int argc, char** argv) {
   const double secs =
       std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   std::printf("update_timing_s %.6f\n", secs);
+  if (!changes.empty()) {
+    const auto t1 = std::chrono::steady_clock::now();
+    for (const auto& c : changes) timer.read_spef(c);
+    timer.update_timing();
+    const double s2 =
+        std::chrono::duration<double>(std::chrono::steady_clock::now() - t1).count();
+    std::printf("incremental_update_timing_s %.6f\n", s2);
+  }
 
   FILE* f = std::fopen(argv[3], "w");
   if (!f) return 3;
@@ -237,6 +255,6 @@ int main(int argc, char** argv) {
     }
   }
   std::fclose(f);
-  if (argc == 5) dump_graph(timer, argv[4]);
+  if (graph_path) dump_graph(timer, graph_path);
   return 0;
 }

@@ -89,7 +89,7 @@ def our_timing(d, G, pin_cap):
         for q in range(ps[i], ps[i + 1]):
             node = int(f["pin_node"][q])
             name = f["pin_names"][q]
-            node_of[(i, name)] = int(ns[i]) + node
+            node_of[(i, name)] = node  # local id in the net
             if node != f["roots"][i]:
                 cap[int(ns[i]) + node] += pin_cap[name]
     t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()  # noqa: E731
