@@ -35,6 +35,7 @@ TUNE_NETS = 50_000
 SPEF_NETS = 20_000
 FU_GATES = 50_000
 FU_REPS = 5
+FU_CHANGE = 0.01  # fraction of the nets a change SPEF re-draws
 # incremental sizing loop
 INC_GATES, INC_ITERS, INC_FRAC, INC_PLAIN_ITERS, INC_CHECK = 200_000, 1000, 0.005, 20, True
 # serving
@@ -738,6 +739,79 @@ def run_full_update(dump=None):
                     # the reference's own two paths against each other, same tolerance
                     out["pins_err_over_tol_reference_cuda_vs_cpu"] = pin_err(ref["cuda"][1],
                                                                              ref["cpu"][1])
+        out["incremental_spef"] = _incremental_spef(d, keep, f, caps, batch, graph, arrays, names)
+    return out
+
+
+def _incremental_spef(d, keep, f0, caps, batch, graph, arrays, names):
+    """A change SPEF (TAU15 change_*.spef style) re-drawing FU_CHANGE of the
+    design's nets, applied to the device-resident design: the host reads
+    the file and maps its nets and pins, then RcBatch.replace_nets moves
+    the unchanged nets with their results into the new layout, re-times
+    the changed nets, and the propagation runs again.  The reference
+    Timer's read_spef + update_timing on the same change (oracle/_ref, CPU
+    path) is timed beside it, and every pin is compared."""
+    import subprocess
+    import torch
+    from opentimer_b200 import designgen
+    from opentimer_b200.prop import change_nets
+    from opentimer_b200.spef import read_spef
+    path = os.path.join(d, "change.spef")
+    changed = designgen.change_spef(keep, path, frac=FU_CHANGE, seed=SEED + 31)
+    t0 = time.perf_counter()
+    fc = read_spef(path, r_scale=np.float32(1e-3))
+    index = {n: i for i, n in enumerate(f0["net_names"])}
+    nets, forest, node_of = change_nets(fc, index, caps)
+    # net arcs into the changed nets get their sinks' new local ids
+    arc_net = graph.dev["arc_net"].cpu().numpy()
+    sel = np.nonzero((np.asarray(arrays["arc_kind"]) == 0) & np.isin(arc_net, nets))[0]
+    nodes = [node_of.get((int(arc_net[k]), names[int(arrays["arc_to"][k])]), -1) for k in sel]
+    host_ms = 1e3 * (time.perf_counter() - t0)
+    forest_d = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in forest]
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    mv_t, pr_t = [], []
+    for r in range(3 + FU_REPS):
+        torch.cuda.synchronize()
+        ev[0].record()
+        b1 = batch.replace_nets(nets, *forest_d)
+        graph.set_arc_nodes(sel, nodes)
+        ev[1].record()
+        graph.propagate(b1)
+        ev[2].record()
+        torch.cuda.synchronize()
+        if r >= 3:
+            mv_t.append(ev[0].elapsed_time(ev[1]))
+            pr_t.append(ev[1].elapsed_time(ev[2]))
+    b1.check()
+    res = graph.result()
+    res["rat"] = np.where(np.isnan(res["at"]), np.nan, res["rat"])
+    mv_ms, pr_ms = float(np.median(mv_t)), float(np.median(pr_t))
+    out = {"workload": f"change SPEF re-drawing {len(changed)} of {len(index)} nets "
+                       f"({int(np.diff(forest[0]).sum())} nodes)",
+           "host_read_and_map_ms": host_ms, "replace_nets_ms": mv_ms, "propagation_ms": pr_ms,
+           "total_ms": host_ms + mv_ms + pr_ms, "timed": f"median of {FU_REPS} (device parts)",
+           "replace_nets": "relayout (otg_rc_move_nets) + subset RC pass on the changed nets"}
+    exe = os.path.join(ROOT, "oracle", "_ref", "ot_run_ref")
+    if os.path.exists(exe):
+        ref_out = os.path.join(d, "ref_change.txt")
+        p = subprocess.run([exe, d, "cpu", ref_out, f"change={path}"], capture_output=True,
+                           text=True, timeout=600)
+        secs = [float(x.split()[1]) for x in p.stdout.splitlines()
+                if x.startswith("incremental_update_timing_s")]
+        if p.returncode == 0 and secs:
+            pins = {}
+            with open(ref_out) as fh:
+                for line in fh:
+                    if line.startswith("P "):
+                        tk = line.split()
+                        pins[tk[1]] = np.array([float(x) for x in tk[2:]]).reshape(4, 4)
+            ours = {n: np.stack([res[k][i] for k in ("at", "slew", "rat", "slack")])
+                    for i, n in enumerate(names)}
+            out["reference"] = {"read_spef_and_update_timing_ms": 1e3 * secs[0], "path": "CPU",
+                                "threads": os.cpu_count(),
+                                "what": "the reference Timer (oracle/_ref): read_spef(change) + "
+                                        "update_timing, dirty nets only"}
+            out["pins_err_over_tol_vs_reference_cpu"] = pin_err(ours, pins)
     return out
 
 
