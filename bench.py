@@ -361,10 +361,12 @@ def run_ours(args, world, rank, local):
         line["incremental"] = run_incremental()
     if world == 1 and not args.no_serving:
         line["serving"] = run_serving()
+    # reference runs of the other sections belong to the CPU-baseline leg
+    base = line.get("cpu_baseline")
     if rank == 0 and not args.no_spef:
-        line["spef_ingest"] = run_spef()
+        line["spef_ingest"] = run_spef(base)
     if world == 1 and not args.no_full_update:
-        line["full_update"] = run_full_update()
+        line["full_update"] = run_full_update(baseline=base if rank == 0 else None)
     return line
 
 
@@ -576,11 +578,13 @@ def run_serving():
     return out
 
 
-def run_spef():
+def run_spef(baseline=None):
     """SPEF ingestion: a seeded 20k-net SPEF (2..512 nodes per net, ~1.8M
     nodes) read into the flat RC layout by otg_spef_read (all host threads,
-    and one), against the reference's SPEF parser plus the flat id rule
-    (oracle/_ref, one thread, as the reference reads SPEF)."""
+    and one).  With `baseline` (the CPU-baseline leg's dict), the
+    reference's SPEF parser plus the flat id rule (oracle/_ref, one thread,
+    as the reference reads SPEF) is timed on the same file into
+    baseline["spef_ingest"]."""
     import tempfile
     from opentimer_b200 import synth_forest_host, workloads
     from opentimer_b200.spef import read_spef
@@ -603,20 +607,21 @@ def run_spef():
         got = read_spef(path, names=False)
         same = bool(np.array_equal(got["edges"], forest["edges"]) and
                     np.array_equal(got["roots"], forest["roots"]))
-        ref = None
-        if os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libotref.so")):
+        if baseline is not None and os.path.exists(os.path.join(ROOT, "oracle", "_ref",
+                                                               "libotref.so")):
             sys.path.insert(0, os.path.join(ROOT, "oracle"))
             import oracle as O
             L = O.ref_lib()
             n, v = ctypes.c_int(), ctypes.c_int()
             t_ref = best(lambda: L.otref_spef_load(path.encode(), ctypes.byref(n),
                                                    ctypes.byref(v)), reps=1)
-            ref = {"nodes_per_s": V / t_ref, "threads": 1,
-                   "what": "the reference's SPEF parser (PEGTL) + the flat id rule"}
+            baseline["spef_ingest"] = {
+                "value": V / t_ref, "unit": "nodes/s", "cores": 1, "kind": "reference",
+                "sample": f"the same {mb:.0f} MB file, one pass",
+                "what": "the reference's SPEF parser (PEGTL) + the flat id rule"}
     return {"workload": f"{SPEF_NETS} nets, {V} nodes, {mb:.0f} MB of SPEF text",
             "nodes_per_s": V / t_all, "threads": os.cpu_count(),
-            "single_thread_nodes_per_s": V / t_one, "ids_round_trip": same,
-            "reference": ref}
+            "single_thread_nodes_per_s": V / t_one, "ids_round_trip": same}
 
 
 def pin_err(got, ref):
@@ -637,15 +642,16 @@ def pin_err(got, ref):
     return worst
 
 
-def run_full_update(dump=None):
+def run_full_update(dump=None, baseline=None):
     """A full timing update on the GPU for a seeded gate-level design
     (designgen: 4-cell library with 7x7 NLDM tables, a random DAG with 5%
     flops, one RC tree per net): SPEF read into the flat layout, the fused
     RC pass, and levelized propagation of slew/delay/arrival/required time
-    and slack over the design's timing graph.  The reference Timer's own
-    update_timing on the same files (oracle/_ref/ot_run_ref, its CPU path,
-    all host threads) is timed beside it, and every pin's results are
-    compared."""
+    and slack over the design's timing graph.  With `baseline` (the
+    CPU-baseline leg's dict), the reference Timer's own update_timing on the
+    same files (oracle/_ref/ot_run_ref: its CPU path on all host threads,
+    and its CUDA path) is timed into baseline["full_update"], and every
+    pin's results are checked against it."""
     import subprocess
     import tempfile
     import torch
@@ -704,7 +710,7 @@ def run_full_update(dump=None):
                "timed": f"median of {FU_REPS}", "spef_read_ms": 1e3 * t_spef,
                "levels": graph.num_levels, "launches_per_propagation": 2}
         exe = os.path.join(ROOT, "oracle", "_ref", "ot_run_ref")
-        if os.path.exists(exe):
+        if baseline is not None and os.path.exists(exe):
             ours = {n: np.stack([res[k][i] for k in ("at", "slew", "rat", "slack")])
                     for i, n in enumerate(names)}
             ref = {}
@@ -727,30 +733,34 @@ def run_full_update(dump=None):
                 dump.update(names=names, ours=ours, ref={k: v[1] for k, v in ref.items()},
                             order=graph.order.cpu().numpy(),
                             level_ends=graph.level_ends.cpu().numpy())
+            b = {}
             if "cpu" in ref:
-                out["reference"] = {"update_timing_ms": ref["cpu"][0], "path": "CPU",
-                                    "threads": os.cpu_count(),
-                                    "what": "the reference Timer's update_timing (oracle/_ref)"}
-                out["pins_err_over_tol_vs_reference_cpu"] = pin_err(ours, ref["cpu"][1])
+                b.update(value=ref["cpu"][0], unit="ms per update_timing", cores=os.cpu_count(),
+                         kind="reference", sample="the same design files, one full update",
+                         what="the reference Timer's update_timing (oracle/_ref), CPU path")
+                b["ours_pins_err_over_tol"] = pin_err(ours, ref["cpu"][1])
             if "cuda" in ref:
-                out["reference_cuda_update_timing_ms"] = ref["cuda"][0]
-                out["pins_err_over_tol_vs_reference_cuda"] = pin_err(ours, ref["cuda"][1])
+                b["reference_cuda_path_ms"] = ref["cuda"][0]
+                b["ours_pins_err_over_tol_vs_cuda_path"] = pin_err(ours, ref["cuda"][1])
                 if "cpu" in ref:
                     # the reference's own two paths against each other, same tolerance
-                    out["pins_err_over_tol_reference_cuda_vs_cpu"] = pin_err(ref["cuda"][1],
-                                                                             ref["cpu"][1])
-        out["incremental_spef"] = _incremental_spef(d, keep, f, caps, batch, graph, arrays, names)
+                    b["reference_cuda_vs_cpu_pins_err_over_tol"] = pin_err(ref["cuda"][1],
+                                                                           ref["cpu"][1])
+            baseline["full_update"] = b
+        out["incremental_spef"] = _incremental_spef(d, keep, f, caps, batch, graph, arrays, names,
+                                                    baseline)
     return out
 
 
-def _incremental_spef(d, keep, f0, caps, batch, graph, arrays, names):
+def _incremental_spef(d, keep, f0, caps, batch, graph, arrays, names, baseline=None):
     """A change SPEF (TAU15 change_*.spef style) re-drawing FU_CHANGE of the
     design's nets, applied to the device-resident design: the host reads
     the file and maps its nets and pins, then RcBatch.replace_nets moves
     the unchanged nets with their results into the new layout, re-times
-    the changed nets, and the propagation runs again.  The reference
-    Timer's read_spef + update_timing on the same change (oracle/_ref, CPU
-    path) is timed beside it, and every pin is compared."""
+    the changed nets, and the propagation runs again.  With `baseline`, the
+    reference Timer's read_spef + update_timing on the same change
+    (oracle/_ref, CPU path) is timed into baseline["incremental_spef"] and
+    every pin is checked against it."""
     import subprocess
     import torch
     from opentimer_b200 import designgen
@@ -758,13 +768,15 @@ def _incremental_spef(d, keep, f0, caps, batch, graph, arrays, names):
     from opentimer_b200.spef import read_spef
     path = os.path.join(d, "change.spef")
     changed = designgen.change_spef(keep, path, frac=FU_CHANGE, seed=SEED + 31)
+    # design state kept between changes, as the Timer keeps its net map
+    index = {n: i for i, n in enumerate(f0["net_names"])}
+    arc_net = graph.dev["arc_net"].cpu().numpy()
+    net_arc = np.asarray(arrays["arc_kind"]) == 0
     t0 = time.perf_counter()
     fc = read_spef(path, r_scale=np.float32(1e-3))
-    index = {n: i for i, n in enumerate(f0["net_names"])}
     nets, forest, node_of = change_nets(fc, index, caps)
     # net arcs into the changed nets get their sinks' new local ids
-    arc_net = graph.dev["arc_net"].cpu().numpy()
-    sel = np.nonzero((np.asarray(arrays["arc_kind"]) == 0) & np.isin(arc_net, nets))[0]
+    sel = np.nonzero(net_arc & np.isin(arc_net, nets))[0]
     nodes = [node_of.get((int(arc_net[k]), names[int(arrays["arc_to"][k])]), -1) for k in sel]
     host_ms = 1e3 * (time.perf_counter() - t0)
     forest_d = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in forest]
@@ -792,7 +804,7 @@ def _incremental_spef(d, keep, f0, caps, batch, graph, arrays, names):
            "total_ms": host_ms + mv_ms + pr_ms, "timed": f"median of {FU_REPS} (device parts)",
            "replace_nets": "relayout (otg_rc_move_nets) + subset RC pass on the changed nets"}
     exe = os.path.join(ROOT, "oracle", "_ref", "ot_run_ref")
-    if os.path.exists(exe):
+    if baseline is not None and os.path.exists(exe):
         ref_out = os.path.join(d, "ref_change.txt")
         p = subprocess.run([exe, d, "cpu", ref_out, f"change={path}"], capture_output=True,
                            text=True, timeout=600)
@@ -807,11 +819,12 @@ def _incremental_spef(d, keep, f0, caps, batch, graph, arrays, names):
                         pins[tk[1]] = np.array([float(x) for x in tk[2:]]).reshape(4, 4)
             ours = {n: np.stack([res[k][i] for k in ("at", "slew", "rat", "slack")])
                     for i, n in enumerate(names)}
-            out["reference"] = {"read_spef_and_update_timing_ms": 1e3 * secs[0], "path": "CPU",
-                                "threads": os.cpu_count(),
-                                "what": "the reference Timer (oracle/_ref): read_spef(change) + "
-                                        "update_timing, dirty nets only"}
-            out["pins_err_over_tol_vs_reference_cpu"] = pin_err(ours, pins)
+            baseline["incremental_spef"] = {
+                "value": 1e3 * secs[0], "unit": "ms per change", "cores": os.cpu_count(),
+                "kind": "reference", "sample": "the same change SPEF, one application",
+                "what": "the reference Timer (oracle/_ref): read_spef(change) + update_timing, "
+                        "CPU path, dirty nets only",
+                "ours_pins_err_over_tol": pin_err(ours, pins)}
     return out
 
 
