@@ -363,6 +363,8 @@ def run_ours(args, world, rank, local):
         line["serving"] = run_serving()
     # reference runs of the other sections belong to the CPU-baseline leg
     base = line.get("cpu_baseline")
+    if base is not None and lv:
+        base["levelize"] = levelize_baseline(lv)
     if rank == 0 and not args.no_spef:
         line["spef_ingest"] = run_spef(base)
     if world == 1 and not args.no_full_update:
@@ -438,10 +440,50 @@ def run_levelize(args, world, dev):
     L, emitted = [int(x) for x in lb.counts.tolist()]
     n, E = len(od), len(fi)
     lv_bytes = 12 * E + 16 * n
+    # the same through host arrays (otg_levelize_host: copies in, levelize,
+    # copies out), as a Timer hands its CSR over
+    otg.levelize_host(fs, fi, od, f0)
+    t0 = time.perf_counter()
+    otg.levelize_host(fs, fi, od, f0)
+    host_ms = 1e3 * (time.perf_counter() - t0)
     return {"edges_per_s": world * E / (ms / 1e3), "ms": ms, "pins": n, "edges": E,
             "levels": L, "emitted": emitted, "us_per_level": 1e3 * ms / max(L, 1),
+            "host_path_ms": host_ms,
             "hbm_gbs": lv_bytes / (ms / 1e3) / 1e9,
             "workload": f"pin DAG {n} pins, {E} edges, {L} levels (seeded)"}
+
+
+def levelize_baseline(ours):
+    """The levelization workload (the same seeded pin DAG) through the
+    reference's own toposort_compute_cuda loop (oracle/_ref: its
+    toposort_advance kernel, one launch and one blocking copy per level,
+    with its allocations and copies, as the Timer calls it) and through the
+    oracle's restatement of the frontier Kahn on one host core.  Both are
+    checked against our levels."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from opentimer_b200 import workloads
+    fs, fi, od, f0 = workloads.pin_dag(SEED, LV_PINS, LV_EDGES, LV_LEVELS)
+    n = len(od)
+    out = {"unit": "ms per levelization", "kind": "reference",
+           "ours_device_ms": ours["ms"]}
+    t0 = time.perf_counter()
+    order, ends, _ = O.levelize(n, fs, fi, od, f0)
+    out["port_cpu_ms"] = 1e3 * (time.perf_counter() - t0)
+    out["port_cpu_cores"] = 1
+    out["levels_match_port"] = bool(len(ends) - 1 == ours["levels"])
+    if O.ref_available():
+        O.ref_toposort_gpu(n, fs, fi, od, f0)  # warm-up (context, module load)
+        t0 = time.perf_counter()
+        fr, rends = O.ref_toposort_gpu(n, fs, fi, od, f0)
+        out["value"] = 1e3 * (time.perf_counter() - t0)
+        out["what"] = ("the reference's toposort_compute_cuda loop on the B200 (oracle/_ref), "
+                       "host arrays in and out, as the Timer calls it")
+        out["levels_match_reference"] = bool(
+            len(rends) == len(ends) and all(
+                np.array_equal(np.sort(fr[rends[k]:rends[k + 1]]), np.sort(order[ends[k]:ends[k + 1]]))
+                for k in range(len(ends) - 1)))
+    return out
 
 
 def _pct(lat, q):

@@ -202,3 +202,47 @@ def attach_nets(arrays, pin_names, pin_net_names, spef, node_of):
     out = dict(arrays)
     out["arc_net"], out["arc_node"] = arc_net, arc_node
     return out
+
+
+def _main():
+    """python -m opentimer_b200.prop [--gates N] [--seed S] [--reps R]: a
+    seeded design (designgen) through the SPEF reader, the RC pass,
+    levelization and R propagations on cuda:0; prints one JSON line with
+    the CUDA-event times (the last propagation's)."""
+    import argparse
+    import json
+    import os
+    import tempfile
+    import torch
+    from . import RcBatch, designgen
+    from .spef import read_spef
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gates", type=int, default=10000)
+    ap.add_argument("--seed", type=int, default=77)
+    ap.add_argument("--reps", type=int, default=3)
+    args = ap.parse_args()
+    with tempfile.TemporaryDirectory() as d:
+        keep = {}
+        designgen.write_design(d, seed=args.seed, gates=args.gates, keep=keep)
+        arrays, names, nets = designgen.timing_graph(keep)
+        f = read_spef(os.path.join(d, "design.spef"), r_scale=np.float32(1e-3))
+    cap, node_of = rc_inputs(f, designgen.pin_caps(keep))
+    g = TimingGraph(attach_nets(arrays, names, nets, f, node_of))
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()  # noqa: E731
+    b = RcBatch(t(f["nodes_start"]), t(f["edges"].copy()), t(f["roots"]), t(f["res"]), t(cap))
+    b.run()
+    b.check()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    for _ in range(max(args.reps, 1)):
+        ev[0].record()
+        g.propagate(b)
+        ev[1].record()
+    g.check()
+    out = g.result()
+    print(json.dumps({"gates": args.gates, "pins": g.P, "arcs": g.A, "levels": g.num_levels,
+                      "propagation_ms": ev[0].elapsed_time(ev[1]),
+                      "pins_with_slack": int(np.isfinite(out["slack"]).any(axis=1).sum())}))
+
+
+if __name__ == "__main__":
+    _main()
