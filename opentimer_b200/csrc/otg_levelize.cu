@@ -6,9 +6,12 @@
 //
 //   level 0      = the caller's seed (pins without candidate fanout)
 //   expand(k)    every pin of level k decrements the fanout counter of each
-//                of its fanins (warp-aggregated atomics: lanes that hit the
-//                same pin combine into one atomicSub); the pin whose counter
-//                reaches zero sets its bit in the "ready" bitmap
+//                of its fanins, edge-parallel: a block scan over the pins'
+//                fanin counts hands one edge to each thread, so all of a
+//                chunk's decrements are in flight at once (warp-aggregated
+//                atomics: lanes that hit the same pin combine into one
+//                atomicSub); the pin whose counter reaches zero sets its bit
+//                in the "ready" bitmap
 //   compact(k+1) the ready bitmap is split into per-CTA word ranges of C
 //                words.  The expansion that sets a pin's bit also counts it
 //                for its range, so after ONE grid barrier every CTA knows its
@@ -39,8 +42,28 @@ constexpr unsigned FULL = 0xffffffffu;
 constexpr int LT = 512;                              // threads per CTA
 using LvCtl = GridCtl;
 
-// Decrement the fanout counters of u's fanins; pins that become ready set
-// their bit in `bm`.  Lanes of a warp that target the same pin combine.
+// One fanin edge per lane (target v, ok = a valid pin): decrement v's
+// fanout counter; the pin whose counter reaches zero sets its bit in `bm`
+// and counts for its range.  Lanes of a warp that target the same pin
+// combine into one atomicSub.  Every lane of the warp must call it.
+__device__ __forceinline__ void decrement(int v, bool ok, int* cnt, unsigned* bm, const int* level,
+                                          int* rcount, int C) {
+  const int lane = threadIdx.x & 31;
+  const unsigned peers = __match_any_sync(FULL, ok ? v : -2 - lane);
+  if (ok && (__ffs(peers) - 1 == lane)) {
+    const int k = __popc(peers);
+    const int old = atomicSub(&cnt[v], k);
+    // a seed pin (level 0) is never emitted twice, even if the caller's
+    // out_deg disagrees with the fanin lists
+    if (old > 0 && old - k <= 0 && level[v] < 0) {
+      atomicOr(&bm[v >> 5], 1u << (v & 31));
+      atomicAdd(&rcount[(v >> 5) / C], 1);
+    }
+  }
+}
+
+// Decrement the fanout counters of u's fanins, one edge per lane per step
+// (the seed level).
 __device__ __forceinline__ void expand_pin(int u, bool active, const int* fanin_start,
                                            const int* fanin, int* cnt, unsigned* bm, int n,
                                            const int* level, int* rcount, int C) {
@@ -49,19 +72,7 @@ __device__ __forceinline__ void expand_pin(int u, bool active, const int* fanin_
   while (__any_sync(FULL, e < e1)) {
     const bool has = e < e1;
     const int v = has ? fanin[e] : -1;
-    const bool ok = has && (unsigned)v < (unsigned)n;
-    const unsigned peers = __match_any_sync(FULL, ok ? v : -2 - (int)(threadIdx.x & 31));
-    const int lane = threadIdx.x & 31;
-    if (ok && (__ffs(peers) - 1 == lane)) {
-      const int k = __popc(peers);
-      const int old = atomicSub(&cnt[v], k);
-      // a seed pin (level 0) is never emitted twice, even if the caller's
-      // out_deg disagrees with the fanin lists
-      if (old > 0 && old - k <= 0 && level[v] < 0) {
-        atomicOr(&bm[v >> 5], 1u << (v & 31));
-        atomicAdd(&rcount[(v >> 5) / C], 1);
-      }
-    }
+    decrement(v, has && (unsigned)v < (unsigned)n, cnt, bm, level, rcount, C);
     e += has ? 1 : 0;
   }
 }
@@ -74,6 +85,8 @@ __global__ void __launch_bounds__(LT) levelize_kernel(int n, const int* fanin_st
                                                       unsigned* bm0, unsigned* bm1, int* blk) {
   // blk: three rotating [G] buffers of per-range ready counts
   __shared__ int wsum[LT / 32];
+  __shared__ int red_t[LT / 32], red_b[LT / 32];
+  __shared__ int s_estart[LT], s_e0[LT];
   __shared__ int s_total, s_off;
   const int G = gridDim.x, b = blockIdx.x, tid = threadIdx.x;
   const int gtid = b * LT + tid, gstride = G * LT;
@@ -119,10 +132,16 @@ __global__ void __launch_bounds__(LT) levelize_kernel(int n, const int* fanin_st
     int* rc_now = blk + (L % 3) * G;         // counts of this level's ranges
     int* rc_next = blk + ((L + 1) % 3) * G;  // filled by this level's expansion
     if (tid == 0) blk[((L + 2) % 3) * G + b] = 0;  // read a level ago, filled next level
-    // offset of this CTA, level total
-    if (tid < 32) {
+    // the first tile's bitmap words load while the counts are summed
+    unsigned word0[2];
+#pragma unroll
+    for (int j = 0; j < 2; ++j)
+      word0[j] = w0 + 2 * tid + j < w1 ? __ldcg(cur + w0 + 2 * tid + j) : 0u;
+    // offset of this CTA and level total: every thread reads at most a few
+    // counts (independent loads), then a block reduction
+    {
       int before = 0, total = 0;
-      for (int i = lane; i < G; i += 32) {
+      for (int i = tid; i < G; i += LT) {
         const int x = __ldcg(rc_now + i);
         total += x;
         if (i < b) before += x;
@@ -131,17 +150,28 @@ __global__ void __launch_bounds__(LT) levelize_kernel(int n, const int* fanin_st
         total += __shfl_xor_sync(FULL, total, d);
         before += __shfl_xor_sync(FULL, before, d);
       }
-      if (lane == 0) { s_total = total; s_off = before; }
+      if (lane == 0) { red_t[w] = total; red_b[w] = before; }
+      __syncthreads();
+      if (tid == 0) {
+        int t = 0, o = 0;
+        for (int k = 0; k < LT / 32; ++k) { t += red_t[k]; o += red_b[k]; }
+        s_total = t;
+        s_off = o;
+      }
+      __syncthreads();
     }
-    __syncthreads();
     const int total = s_total;
     if (total == 0) break;
     int run = emitted + s_off;
-    // write own pins in ascending order, tile by tile, and expand them
-    for (int t0 = w0; t0 < w1; t0 += LT) {
-      const int i = t0 + tid;
-      const unsigned word = i < w1 ? cur[i] : 0u;
-      const int pc = __popc(word);
+    // write own pins in ascending order, tile by tile (two bitmap words per
+    // thread), and expand them
+    for (int t0 = w0; t0 < w1; t0 += 2 * LT) {
+      const int i = t0 + 2 * tid;
+      unsigned wd[2];
+#pragma unroll
+      for (int j = 0; j < 2; ++j)
+        wd[j] = t0 == w0 ? word0[j] : (i + j < w1 ? __ldcg(cur + i + j) : 0u);
+      const int pc = __popc(wd[0]) + __popc(wd[1]);
       // block exclusive scan of pc
       int x = pc;
       for (int d = 1; d < 32; d <<= 1) {
@@ -157,29 +187,70 @@ __global__ void __launch_bounds__(LT) levelize_kernel(int n, const int* fanin_st
       }
       __syncthreads();
       int pos = run + wb + x - pc;
-      unsigned bits = word;
-      while (bits) {
-        const int bit = __ffs(bits) - 1;
-        bits &= bits - 1;
-        const int v = (i << 5) + bit;
-        if (pos < n) {
-          order[pos] = v;
-        } else {
-          atomicCAS(&ctl->status, 0, (int)OTG_ERR_INVALID);  // duplicate seeds
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        unsigned bits = wd[j];
+        while (bits) {
+          const int bit = __ffs(bits) - 1;
+          bits &= bits - 1;
+          const int v = ((i + j) << 5) + bit;
+          if (pos < n) {
+            order[pos] = v;
+          } else {
+            atomicCAS(&ctl->status, 0, (int)OTG_ERR_INVALID);  // duplicate seeds
+          }
+          ++pos;
+          level[v] = L;
         }
-        ++pos;
-        level[v] = L;
+        if (i + j < w1) cur[i + j] = 0u;  // ready for reuse two levels on
       }
-      if (i < w1) cur[i] = 0u;  // ready for reuse two levels on
       __syncthreads();  // the tile's slice of `order` is visible to the CTA
-      // expand the tile's pins, one per thread (a word's pins would
-      // otherwise go one after another through their atomics)
+      // expand the tile's pins edge-parallel: LT pins at a time, their fanin
+      // edges spread one per thread, so every decrement of a chunk is in
+      // flight at once instead of one edge after another per pin
       const int tn = min(tt, n - run);
-      for (int k0 = 0; k0 < tn; k0 += LT) {
-        const int k = k0 + tid;
-        const bool act = k < tn;
-        expand_pin(act ? order[run + k] : 0, act, fanin_start, fanin, cnt, nxt, n, level,
-                   rc_next, C);
+      for (int c0 = 0; c0 < tn; c0 += LT) {
+        const int k = c0 + tid;
+        int e0 = 0, deg = 0;
+        if (k < tn) {
+          const int u = order[run + k];
+          if ((unsigned)u < (unsigned)n) {
+            e0 = fanin_start[u];
+            deg = fanin_start[u + 1] - e0;
+          }
+        }
+        // block exclusive scan of the degrees
+        int y = deg;
+        for (int d = 1; d < 32; d <<= 1) {
+          const int z = __shfl_up_sync(FULL, y, d);
+          if (lane >= d) y += z;
+        }
+        if (lane == 31) wsum[w] = y;
+        __syncthreads();
+        int eb = 0, etot = 0;
+        for (int u = 0; u < LT / 32; ++u) {
+          if (u < w) eb += wsum[u];
+          etot += wsum[u];
+        }
+        s_estart[tid] = eb + y - deg;
+        s_e0[tid] = e0;
+        __syncthreads();
+        const int np = min(LT, tn - c0);
+        for (int q0 = 0; q0 < etot; q0 += LT) {
+          const int q = q0 + tid;
+          int v = -1;
+          if (q < etot) {
+            // the pin owning edge q: the last one whose start is <= q
+            int lo = 0, hi = np - 1;
+            while (lo < hi) {
+              const int mid = (lo + hi + 1) >> 1;
+              if (s_estart[mid] <= q) lo = mid; else hi = mid - 1;
+            }
+            v = fanin[s_e0[lo] + (q - s_estart[lo])];
+          }
+          decrement(v, (unsigned)v < (unsigned)n, cnt, nxt, level, rc_next, C);
+        }
+        __syncthreads();  // s_estart / s_e0 / wsum are reused
       }
       run += tt;
     }
