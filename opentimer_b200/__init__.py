@@ -209,10 +209,12 @@ class RcBatch:
         s = _stream(stream)
         check("otg_rc_move_nets", lib().otg_rc_move_nets(
             ctypes.byref(self._forest), ctypes.byref(new._forest), _ptr(keep_d), 1, _ptr(status), s))
-        staging = RcForest(K, int(host(nodes_start)[-1]) if K else 0,
-                           *[x.data_ptr() for x in sub], *([None] * 10))
-        check("otg_rc_move_nets", lib().otg_rc_move_nets(
-            ctypes.byref(staging), ctypes.byref(new._forest), _ptr(put_d), 0, _ptr(status), s))
+        if K:
+            staging = RcForest(K, int(host(nodes_start)[-1]), *[x.data_ptr() for x in sub],
+                               *([None] * 10))
+            check("otg_rc_move_nets", lib().otg_rc_move_nets(
+                ctypes.byref(staging), ctypes.byref(new._forest), _ptr(put_d), 0, _ptr(status),
+                s))
         net_list = t(nets, np.int32)
         num = torch.tensor([K], dtype=torch.int32, device=dev)
         if K:

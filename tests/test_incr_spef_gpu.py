@@ -175,3 +175,36 @@ def test_incremental_update_matches_reference_timer(design):
             if m.any():
                 worst = max(worst, float(np.max(np.abs(gq[m] - r[m]) / (1e-5 * scale[m] + 1e-5))))
         assert worst <= 1.0, worst
+
+
+def test_empty_change_and_bad_move(cuda):
+    """Replacing no net keeps every result bit for bit; a move whose source
+    net index is out of range is skipped and reported (OTG_ERR_INVALID),
+    never read."""
+    import ctypes
+    import torch
+    from opentimer_b200 import synth_forest, workloads
+    from opentimer_b200._lib import lib
+    ns = torch.from_numpy(workloads.net_sizes(9, 300, 2, 300)).cuda()
+    g = synth_forest(9, ns, with_sinks=False)
+    b0 = otg.RcBatch(ns, g["edges"], g["roots"], g["res"], g["cap"])
+    b0.run()
+    b0.check()
+    empty = (np.zeros(1, np.int32), np.zeros((0, 2), np.int32), np.zeros(0, np.int32),
+             np.zeros(0, np.float32), np.zeros((0, 4), np.float32))
+    b1 = b0.replace_nets([], *empty)
+    b1.check()
+    for k in ("nodes_start", "edges", "node2bfs", "pid", "load", "delay", "ldelay", "impulse"):
+        assert torch.equal(getattr(b0, k), getattr(b1, k)), k
+    # a source index past the source forest: skipped and flagged
+    bad = torch.full((b0.num_nets,), -1, dtype=torch.int32, device="cuda")
+    bad[0] = b0.num_nets + 5
+    status = torch.zeros(1, dtype=torch.int32, device="cuda")
+    before = b1.load.clone()
+    code = lib().otg_rc_move_nets(ctypes.byref(b0._forest), ctypes.byref(b1._forest),
+                                  ctypes.c_void_p(bad.data_ptr()), 1,
+                                  ctypes.c_void_p(status.data_ptr()),
+                                  ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+    torch.cuda.synchronize()
+    assert code == 0 and int(status.item()) == 1  # OTG_ERR_INVALID
+    assert torch.equal(before, b1.load)
