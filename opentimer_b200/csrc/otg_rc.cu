@@ -883,12 +883,15 @@ __device__ void rc_net_block(const RcArgs& a, int net, char* ws, int n, int* sh,
 
   // ---- B: Elmore, one corner pair at a time (corners 2cp, 2cp+1), with
   // exact fixed-point sums (see fx_scale).  The maximum term of every sweep
-  // is gathered in the loop before it (smx) to set its scale.
+  // is gathered in the loop before it (smx) to set its scale.  The pair's
+  // caps are read from HBM once, in id order, into Y by preorder; after the
+  // load sweep they move to the unused half of each Ip slot, where the
+  // ldelay sweep reads them last (and overwrites them in place).
   const float2* cap2 = (const float2*)a.cap;
+  float2* capI = (float2*)Ip;  // cap of preorder slot i at capI[2 * i]
   for (int cp = 0; cp < 2; ++cp) {
     float2* out;
     float up[2], dn[2], m[2];
-    auto capx = [&](int i) { return cap2[2 * (size_t)(b + (int)nap[i]) + cp]; };
     auto scale = [&](int k) {
       fx_scale(__uint_as_float(smx[2 * k]), n, up[0], dn[0]);
       fx_scale(__uint_as_float(smx[2 * k + 1]), n, up[1], dn[1]);
@@ -896,12 +899,16 @@ __device__ void rc_net_block(const RcArgs& a, int net, char* ws, int n, int* sh,
     if (tid < 8) smx[tid] = 0u;
     __syncthreads();
     m[0] = m[1] = 0.f;
-    for (int i = tid; i < n; i += T) max2_accumulate(capx(i), m);
+    for (int j = tid; j < n; j += T) {
+      const float2 c = cap2[2 * (size_t)(b + j) + cp];
+      Y[(int)pre[j]] = c;
+      max2_accumulate(c, m);
+    }
     max2_commit(m, smx + 0);
     __syncthreads();
     // load (up): cap summed over the subtree
     scale(0);
-    up_scan_fx<T, K>(n, capx, up, Ip, shl);
+    up_scan_fx<T, K>(n, [&](int i) { return Y[i]; }, up, Ip, shl);
     m[0] = m[1] = 0.f;
     for (int i = tid; i < n; i += T) {
       const float2 v = up_range_fx(Ip, i, i + (int)size[i] - 1, dn);
@@ -912,6 +919,8 @@ __device__ void rc_net_block(const RcArgs& a, int net, char* ws, int n, int* sh,
     __syncthreads();
     out = (float2*)a.load;
     for (int r = tid; r < n; r += T) out[2 * (size_t)(b + r) + cp] = X[pre[nas[r]]];
+    for (int i = tid; i < n; i += T) capI[2 * i] = Y[i];  // Ip is free until the ldelay sweep
+    __syncthreads();
     PHASE(8);
     // delay (down): +pres*load entering a node, - leaving it
     scale(1);
@@ -935,14 +944,15 @@ __device__ void rc_net_block(const RcArgs& a, int net, char* ws, int n, int* sh,
       const int i = (int)pre[nas[r]];
       const float2 d = Y[i];
       out[2 * (size_t)(b + r) + cp] = d;
-      max2_accumulate(f2mul(capx(i), d), m);
+      max2_accumulate(f2mul(capI[2 * i], d), m);
     }
     max2_commit(m, smx + 4);
     __syncthreads();
     PHASE(9);
     // ldelay (up): cap*delay over the subtree
     scale(2);
-    up_scan_fx<T, K>(n, [&](int i) { return f2mul(capx(i), Y[i]); }, up, Ip, shl);
+    // each thread reads its own slots' caps before it writes their sums
+    up_scan_fx<T, K>(n, [&](int i) { return f2mul(capI[2 * i], Y[i]); }, up, Ip, shl);
     m[0] = m[1] = 0.f;
     for (int i = tid; i < n; i += T) {
       const float2 v = up_range_fx(Ip, i, i + (int)size[i] - 1, dn);
