@@ -339,6 +339,10 @@ otg_status otg_spef_pins(const otg_spef* spef, int32_t* pins_start, int32_t* pin
                          int8_t* pin_dir, int8_t* pin_port);
 const char* otg_spef_net_name(const otg_spef* spef, int32_t net);
 const char* otg_spef_pin_name(const otg_spef* spef, int32_t net, int32_t k);
+/* Every net name, then every pin name (net order, *CONN order), each
+ * NUL-terminated, into buf (*bytes: its size in, the size used out).  With
+ * buf NULL it only sets *bytes.  OTG_ERR_WORKSPACE if buf is too small. */
+otg_status otg_spef_names(const otg_spef* spef, char* buf, size_t* bytes);
 void otg_spef_free(otg_spef* spef);
 
 /*

@@ -472,6 +472,31 @@ const char* otg_spef_pin_name(const otg_spef* s, int32_t net, int32_t k) {
   return p[k].name.c_str();
 }
 
+otg_status otg_spef_names(const otg_spef* s, char* buf, size_t* bytes) {
+  if (!s || !bytes) return OTG_ERR_INVALID;
+  size_t need = 0;
+  for (const auto& n : s->nets) {
+    need += n.name.size() + 1;
+    for (const auto& p : n.pins) need += p.name.size() + 1;
+  }
+  if (!buf) {
+    *bytes = need;
+    return OTG_OK;
+  }
+  if (*bytes < need) return OTG_ERR_WORKSPACE;
+  char* o = buf;
+  auto put = [&](const std::string& x) {
+    std::memcpy(o, x.data(), x.size());
+    o += x.size();
+    *o++ = '\0';
+  };
+  for (const auto& n : s->nets) put(n.name);
+  for (const auto& n : s->nets)
+    for (const auto& p : n.pins) put(p.name);
+  *bytes = need;
+  return OTG_OK;
+}
+
 void otg_spef_free(otg_spef* s) { delete s; }
 
 }  // extern "C"

@@ -138,20 +138,33 @@ def rc_inputs(spef, pin_caps):
     (pin_caps: name -> [4]), as the flat path adds them (ot/timer/
     net.cpp:433-446).  Returns (cap [V,4], node_of {(net, pin name): the
     pin's local node id in the net})."""
-    ns, ps = spef["nodes_start"], spef["pins_start"]
+    ns, ps = np.asarray(spef["nodes_start"]), np.asarray(spef["pins_start"])
     cap = spef["cap"].copy()
-    node_of = {}
     names = spef["pin_names"]
-    for i in range(len(ns) - 1):
-        b = int(ns[i])
-        for q in range(ps[i], ps[i + 1]):
-            node = int(spef["pin_node"][q])
-            if node < 0:
-                continue
-            node_of[(i, names[q])] = node
-            if node != spef["roots"][i] and names[q] in pin_caps:
-                cap[b + node] = cap[b + node] + np.asarray(pin_caps[names[q]], np.float32)
+    net = np.repeat(np.arange(len(ns) - 1), np.diff(ps))
+    node = np.asarray(spef["pin_node"], np.int64)
+    on = np.nonzero(node >= 0)[0]
+    node_of = dict(zip(zip(net[on].tolist(), [names[q] for q in on]), node[on].tolist()))
+    nonroot = on[node[on] != np.asarray(spef["roots"])[net[on]]]
+    rows, vals = [], []
+    for q in nonroot.tolist():
+        c = pin_caps.get(names[q])
+        if c is not None:
+            rows.append(int(ns[net[q]]) + int(node[q]))
+            vals.append(c)
+    if rows:  # float32 adds, in pin order (np.add.at is unbuffered)
+        np.add.at(cap, np.asarray(rows, np.int64), np.asarray(vals, np.float32))
     return cap, node_of
+
+
+def _ranges(starts, sizes):
+    """Concatenated aranges [starts[k], starts[k] + sizes[k])."""
+    sizes = np.asarray(sizes, np.int64)
+    total = int(sizes.sum())
+    off = np.zeros(len(sizes), np.int64)
+    np.cumsum(sizes[:-1], out=off[1:])
+    return np.arange(total, dtype=np.int64) - np.repeat(off, sizes) + \
+        np.repeat(np.asarray(starts, np.int64), sizes)
 
 
 def change_nets(spef_change, net_index, pin_caps):
@@ -164,22 +177,19 @@ def change_nets(spef_change, net_index, pin_caps):
     {(forest net, pin name): local node} for the arcs into them."""
     f = spef_change
     cap, node_local = rc_inputs(f, pin_caps)
-    ns = f["nodes_start"]
-    keep = [i for i, n in enumerate(f["net_names"]) if n in net_index]
-    nets = np.array([net_index[f["net_names"][i]] for i in keep], np.int64)
-    sizes = np.array([ns[i + 1] - ns[i] for i in keep], np.int64)
+    ns = np.asarray(f["nodes_start"], np.int64)
+    keep = np.array([i for i, n in enumerate(f["net_names"]) if n in net_index], np.int64)
+    nets = np.array([net_index[f["net_names"][i]] for i in keep.tolist()], np.int64)
+    sizes = ns[keep + 1] - ns[keep] if len(keep) else np.zeros(0, np.int64)
     sub_ns = np.zeros(len(keep) + 1, np.int64)
     np.cumsum(sizes, out=sub_ns[1:])
-    node_rows = np.concatenate([np.arange(ns[i], ns[i + 1]) for i in keep]) if keep else \
-        np.zeros(0, np.int64)
-    edge_rows = np.concatenate([np.arange(ns[i] - i, ns[i + 1] - i - 1) for i in keep]) if keep \
-        else np.zeros(0, np.int64)
+    node_rows = _ranges(ns[keep], sizes)
+    edge_rows = _ranges(ns[keep] - keep, sizes - 1)
     forest = (sub_ns.astype(np.int32), f["edges"][edge_rows].copy(),
               np.asarray(f["roots"])[keep].astype(np.int32), f["res"][edge_rows].copy(),
               cap[node_rows].copy())
-    back = {i: k for k, i in enumerate(keep)}
-    node_of = {(int(nets[back[i]]), pin): node for (i, pin), node in node_local.items()
-               if i in back}
+    back = dict(zip(keep.tolist(), nets.tolist()))
+    node_of = {(back[i], pin): node for (i, pin), node in node_local.items() if i in back}
     return nets, forest, node_of
 
 

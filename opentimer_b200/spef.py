@@ -38,11 +38,14 @@ def read_spef(path, threads=0, r_scale=1.0, c_scale=1.0, names=True):
                                                a("res"), a("cap"), a("net_flags")))
         check("otg_spef_pins", L.otg_spef_pins(h, a("pins_start"), a("pin_node"), a("pin_dir"),
                                                a("pin_port")))
-        if names:
-            out["net_names"] = [L.otg_spef_net_name(h, i).decode() for i in range(N)]
-            ps = out["pins_start"]
-            out["pin_names"] = [L.otg_spef_pin_name(h, i, k).decode()
-                                for i in range(N) for k in range(ps[i + 1] - ps[i])]
+        if names:  # all names in one call: nets, then pins in net order
+            size = ctypes.c_size_t()
+            check("otg_spef_names", L.otg_spef_names(h, None, ctypes.byref(size)))
+            buf = ctypes.create_string_buffer(max(size.value, 1))
+            check("otg_spef_names", L.otg_spef_names(h, buf, ctypes.byref(size)))
+            allnames = buf.raw[:size.value].decode().split("\0")[:-1] if size.value else []
+            out["net_names"] = allnames[:N]
+            out["pin_names"] = allnames[N:]
         return out
     finally:
         L.otg_spef_free(h)
