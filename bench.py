@@ -360,24 +360,36 @@ def run_ours(args, world, rank, local):
     if lv:
         line["levelize"] = lv
     if rank == 0 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(g, ns_np)
+        line["cpu_baseline"] = _section(cpu_baseline, g, ns_np)
     # the per-GPU incremental and serving loops (one GPU only)
     if world == 1 and not (args.no_incremental and args.no_serving):
         del batch, g
         torch.cuda.empty_cache()
     if world == 1 and not args.no_incremental:
-        line["incremental"] = run_incremental()
+        line["incremental"] = _section(run_incremental)
     if world == 1 and not args.no_serving:
-        line["serving"] = run_serving()
+        line["serving"] = _section(run_serving)
     # reference runs of the other sections belong to the CPU-baseline leg
     base = line.get("cpu_baseline")
     if base is not None and lv:
-        base["levelize"] = levelize_baseline(lv)
+        base["levelize"] = _section(levelize_baseline, lv)
     if rank == 0 and not args.no_spef:
-        line["spef_ingest"] = run_spef(base)
+        line["spef_ingest"] = _section(run_spef, base)
     if world == 1 and not args.no_full_update:
-        line["full_update"] = run_full_update(baseline=base if rank == 0 else None)
+        line["full_update"] = _section(run_full_update, baseline=base if rank == 0 else None)
     return line
+
+
+def _section(fn, *args, **kw):
+    """Runs a section after the headline measurement: a failure is reported
+    in the line ({"error": ...}, traceback on stderr) instead of losing the
+    headline numbers."""
+    try:
+        return fn(*args, **kw)
+    except Exception as e:  # noqa: BLE001 -- reported, not swallowed
+        import traceback
+        traceback.print_exc()
+        return {"error": f"{type(e).__name__}: {e}"}
 
 
 def run_e2e(args, world, g, ns_np, N, V, S, dev):
