@@ -757,6 +757,8 @@ def run_full_update(dump=None, baseline=None):
             torch.cuda.synchronize()
             ev[0].record()
             graph.levelizer.run()
+            if graph.fwd_levelizer is not None:  # the forward pass's order as well
+                graph.fwd_levelizer.run()
             ev[1].record()
             torch.cuda.synchronize()
             lv_t.append(ev[0].elapsed_time(ev[1]))

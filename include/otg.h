@@ -400,15 +400,20 @@ typedef struct otg_prop_rc {   /* outputs of otg_rc_timing for the design's nets
 otg_status otg_prop_workspace_size(int32_t num_pins, int32_t num_arcs, int32_t num_tests,
                                    size_t* bytes);
 /* order (device, num_pins entries) is otg_levelize's output over the
- * graph's fanin CSR: every pin after all of its fanout pins.  Writes at,
+ * graph's fanin CSR: every pin after all of its fanout pins; the backward
+ * pass takes it as is.  fwd_order (device, may be NULL) is the forward
+ * pass's order, every pin after all of its fanin pins (otg_levelize over
+ * the fanout CSR: by distance from the sources); NULL takes order
+ * reversed.  Any such orders give the same results.  Writes at,
  * slew, rat, slack [P][4].  lut_meta and the four outputs must be 16-byte
  * aligned, the workspace 256-byte aligned.  A fill launch, then one
  * cooperative launch, dataflow-scheduled (a pin polls the values it reads
  * from its fanins, bounded waits); asynchronous.  otg_prop_status
  * synchronizes the stream and returns OTG_ERR_TIMEOUT if a wait gave up. */
 otg_status otg_propagate(const otg_prop_graph* graph, const otg_prop_rc* rc,
-                         const int32_t* order, float* at, float* slew, float* rat, float* slack,
-                         void* workspace, size_t workspace_bytes, otg_stream_t stream);
+                         const int32_t* order, const int32_t* fwd_order, float* at, float* slew,
+                         float* rat, float* slack, void* workspace, size_t workspace_bytes,
+                         otg_stream_t stream);
 otg_status otg_prop_status(const void* workspace, otg_stream_t stream);
 
 /* Human-readable name of a status code. */

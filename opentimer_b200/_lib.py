@@ -134,7 +134,7 @@ def lib():
         L.otg_spef_pin_name.restype = ctypes.c_char_p
         L.otg_spef_free.argtypes = [P]
         L.otg_prop_workspace_size.argtypes = [I32, I32, I32, PS]
-        L.otg_propagate.argtypes = [P, P, P, P, P, P, P, P, S, P]
+        L.otg_propagate.argtypes = [P, P, P, P, P, P, P, P, P, S, P]
         L.otg_prop_status.argtypes = [P, P]
         L.otg_rc_move_nets.argtypes = [P, P, P, I32, P, P]
         L.otg_spef_names.argtypes = [P, P, PS]

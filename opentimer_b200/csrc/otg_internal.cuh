@@ -90,7 +90,7 @@ struct RcLayout {
 };
 
 // Sublist splitters of the Euler-tour ranking: about one arc in kSplit.
-constexpr int kSplit = 16;
+constexpr int kSplit = 8;
 
 // Radix digit of the block sort: 8 bits, 7 for 1024-thread CTAs (whose
 // 32 per-warp histograms would otherwise take 32 KB of shared memory).

@@ -488,7 +488,8 @@ __global__ void prop_init_kernel(float4* at, float4* slew, int num_pins, GridCtl
 
 // The whole propagation in one cooperative launch; warp w of W takes items
 // w, w + W, ... of each pass.
-__global__ void __launch_bounds__(256) prop_kernel(G G_, const int* order, int num_pins,
+__global__ void __launch_bounds__(256) prop_kernel(G G_, const int* order, const int* fwd_order,
+                                                   int num_pins,
                                                    float* at, float* slew, float* rat,
                                                    float* slack, float* arc_delay,
                                                    float* test_rat, GridCtl* ctl, int lut_smem) {
@@ -502,9 +503,10 @@ __global__ void __launch_bounds__(256) prop_kernel(G G_, const int* order, int n
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int W = (gridDim.x * blockDim.x) >> 5;
   bool ok = true;
-  for (int j = warp; ok && j < num_pins; j += W)
-    ok = fprop_warp(G_, lutd, __ldg(order + num_pins - 1 - j), lane, at, slew, rat, arc_delay,
-                    test_rat, ctl);
+  for (int j = warp; ok && j < num_pins; j += W) {
+    const int v = fwd_order ? __ldg(fwd_order + j) : __ldg(order + num_pins - 1 - j);
+    ok = fprop_warp(G_, lutd, v, lane, at, slew, rat, arc_delay, test_rat, ctl);
+  }
   // the barrier also lets every CTA leave together when a wait gave up
   if (!grid_barrier(ctl) || !ok) return;
   for (int j = warp; ok && j < num_pins; j += W)
@@ -537,8 +539,9 @@ otg_status otg_prop_workspace_size(int32_t num_pins, int32_t num_arcs, int32_t n
 }
 
 otg_status otg_propagate(const otg_prop_graph* g, const otg_prop_rc* rc, const int32_t* order,
-                         float* at, float* slew, float* rat, float* slack, void* workspace,
-                         size_t workspace_bytes, otg_stream_t stream) {
+                         const int32_t* fwd_order, float* at, float* slew, float* rat,
+                         float* slack, void* workspace, size_t workspace_bytes,
+                         otg_stream_t stream) {
   if (!g || !rc || !order || !at || !slew || !rat || !slack || !workspace || g->num_pins < 0)
     return OTG_ERR_INVALID;
   // lut_meta rows and the per-pin [4] rows are read and written as 16-byte vectors
@@ -578,8 +581,8 @@ otg_status otg_propagate(const otg_prop_graph* g, const otg_prop_rc* rc, const i
   const int grid = std::max(1, std::min(d.sms * std::max(occ, 1), (P + 7) / 8));
   otg::G G_{*g, *rc};
   int num_pins = P;
-  void* args[] = {&G_,  (void*)&order, &num_pins,  &at,  &slew,    &rat,
-                  &slack, &arc_delay,  &test_rat,  &ctl, &lut_smem};
+  void* args[] = {&G_,       (void*)&order, (void*)&fwd_order, &num_pins, &at,  &slew,
+                  &rat,      &slack,        &arc_delay,        &test_rat, &ctl, &lut_smem};
   const cudaError_t e = cudaLaunchCooperativeKernel(
       (const void*)otg::prop_kernel, dim3(grid), dim3(256), args, 4 * (size_t)lut_smem, st);
   otg::count_launch();
