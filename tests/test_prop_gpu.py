@@ -235,3 +235,31 @@ def test_bounded_wait_gives_up_on_a_cycle(cuda):
     out = TimingGraph(_chain_graph(False)).propagate(batch).result()
     assert np.all(out["at"][0] == 1.0) and np.all(out["slew"][0] == 2.0)
     assert np.all(np.isnan(out["at"][1]))  # a net arc without an RC node carries nothing
+
+
+def test_forward_order_from_sources_is_identical(design, tmp_path):
+    """The forward pass may take its pins by distance from the sources
+    (fwd_order, a second levelization) instead of the backward order
+    reversed: every pin's results are the same bits."""
+    import torch
+    from opentimer_b200 import designgen
+    from opentimer_b200.prop import TimingGraph, attach_nets, rc_inputs
+    from opentimer_b200.spef import read_spef
+    keep = {}
+    d = str(tmp_path)
+    designgen.write_design(d, seed=2024, gates=2000, keep=keep)
+    arrays, names, nets = designgen.timing_graph(keep)
+    f = read_spef(os.path.join(d, "design.spef"), r_scale=np.float32(1e-3))
+    cap, node_of = rc_inputs(f, designgen.pin_caps(keep))
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()  # noqa: E731
+    batch = otg.RcBatch(t(f["nodes_start"]), t(f["edges"].copy()), t(f["roots"]), t(f["res"]),
+                        t(cap))
+    batch.run()
+    batch.check()
+    att = attach_nets(arrays, names, nets, f, node_of)
+    a = TimingGraph(att, forward="sinks").propagate(batch).result()
+    gs = TimingGraph(att, forward="sources")
+    assert gs.fwd_order is not None
+    b = gs.propagate(batch).result()
+    for k in ("at", "slew", "rat", "slack"):
+        assert np.array_equal(a[k].view(np.uint32), b[k].view(np.uint32)), k
