@@ -148,14 +148,21 @@ __host__ __device__ inline RcLayout rc_layout(int n, int T, int K, int ib) {
   OTG_TAKE(hist, 4u * (1u << rc_radix_bits(T)) * W);
   const uint32_t endA = o;
   o = rA;
-  OTG_TAKE(X, 8u * N);
-  OTG_TAKE(Y, 8u * N);
-  OTG_TAKE(Ip, 16u * N);
+  OTG_TAKE(X, 8u * (N + N / 4u + 1u));  // padded slots, see rc_pad8
+  OTG_TAKE(Y, 8u * (N + N / 4u + 1u));
+  OTG_TAKE(Ip, 16u * (N + N / 8u + 1u));  // rc_pad16
 #undef OTG_TAKE
 #undef OTG_AL
   l.total = endA > o ? endA : o;
   return l;
 }
+
+// Padded slot indices of the Elmore arrays.  The scans give each thread K
+// consecutive slots, so for a given k a warp's lanes touch elements K
+// apart, several to a shared-memory bank; one spare element per 4 (8-byte
+// X, Y) and per 8 (16-byte Ip) spreads them over the banks.
+__host__ __device__ __forceinline__ int rc_pad8(int i) { return i + (i >> 2); }
+__host__ __device__ __forceinline__ int rc_pad16(int i) { return i + (i >> 3); }
 
 // Net-size classes: class c takes nets with nmax[c-1] < n <= nmax[c].
 struct RcClasses {

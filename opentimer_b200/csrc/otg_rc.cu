@@ -564,7 +564,7 @@ __device__ void up_scan_fx(int n, XF x, const float (&up)[2], longlong2* Ip, lon
     const long long b0 = carry[0] + wb[0] + ex[0], b1 = carry[1] + wb[1] + ex[1];
 #pragma unroll
     for (int k = 0; k < K; ++k)
-      if (q0 + k < n) Ip[q0 + k] = make_longlong2(b0 + loc[k][0], b1 + loc[k][1]);
+      if (q0 + k < n) Ip[rc_pad16(q0 + k)] = make_longlong2(b0 + loc[k][0], b1 + loc[k][1]);
     carry[0] += tt[0];
     carry[1] += tt[1];
     __syncthreads();
@@ -574,9 +574,9 @@ __device__ void up_scan_fx(int n, XF x, const float (&up)[2], longlong2* Ip, lon
 // Sum over preorder slots [lo, hi] of an up_scan_fx, back in fp32.
 __device__ __forceinline__ float2 up_range_fx(const longlong2* Ip, int lo, int hi,
                                               const float (&dn)[2]) {
-  longlong2 h = Ip[hi];
+  longlong2 h = Ip[rc_pad16(hi)];
   if (lo > 0) {
-    const longlong2 l = Ip[lo - 1];
+    const longlong2 l = Ip[rc_pad16(lo - 1)];
     h.x -= l.x;
     h.y -= l.y;
   }
@@ -888,7 +888,7 @@ __device__ void rc_net_block(const RcArgs& a, int net, char* ws, int n, int* sh,
   // load sweep they move to the unused half of each Ip slot, where the
   // ldelay sweep reads them last (and overwrites them in place).
   const float2* cap2 = (const float2*)a.cap;
-  float2* capI = (float2*)Ip;  // cap of preorder slot i at capI[2 * i]
+  float2* capI = (float2*)Ip;  // cap of preorder slot i at capI[2 * rc_pad16(i)]
   for (int cp = 0; cp < 2; ++cp) {
     float2* out;
     float up[2], dn[2], m[2];
@@ -901,50 +901,50 @@ __device__ void rc_net_block(const RcArgs& a, int net, char* ws, int n, int* sh,
     m[0] = m[1] = 0.f;
     for (int j = tid; j < n; j += T) {
       const float2 c = cap2[2 * (size_t)(b + j) + cp];
-      Y[(int)pre[j]] = c;
+      Y[rc_pad8((int)pre[j])] = c;
       max2_accumulate(c, m);
     }
     max2_commit(m, smx + 0);
     __syncthreads();
     // load (up): cap summed over the subtree
     scale(0);
-    up_scan_fx<T, K>(n, [&](int i) { return Y[i]; }, up, Ip, shl);
+    up_scan_fx<T, K>(n, [&](int i) { return Y[rc_pad8(i)]; }, up, Ip, shl);
     m[0] = m[1] = 0.f;
     for (int i = tid; i < n; i += T) {
       const float2 v = up_range_fx(Ip, i, i + (int)size[i] - 1, dn);
-      X[i] = v;
+      X[rc_pad8(i)] = v;
       max2_accumulate(f2scale(v, pres[i]), m);
     }
     max2_commit(m, smx + 2);
     __syncthreads();
     out = (float2*)a.load;
-    for (int r = tid; r < n; r += T) out[2 * (size_t)(b + r) + cp] = X[pre[nas[r]]];
-    for (int i = tid; i < n; i += T) capI[2 * i] = Y[i];  // Ip is free until the ldelay sweep
+    for (int r = tid; r < n; r += T) out[2 * (size_t)(b + r) + cp] = X[rc_pad8(pre[nas[r]])];
+    for (int i = tid; i < n; i += T) capI[2 * rc_pad16(i)] = Y[rc_pad8(i)];  // Ip is free until the ldelay sweep
     __syncthreads();
     PHASE(8);
     // delay (down): +pres*load entering a node, - leaving it
     scale(1);
-    if (tid == 0) Y[0] = make_float2(0.f, 0.f);
+    if (tid == 0) Y[rc_pad8(0)] = make_float2(0.f, 0.f);
     down_scan_fx<T, K>(
         A,
         [&](int p) {
           const int c = (int)code[p];
           const int i = (c > 0 ? c : -c) - 1;
-          return f2scale(X[i], c > 0 ? pres[i] : -pres[i]);
+          return f2scale(X[rc_pad8(i)], c > 0 ? pres[i] : -pres[i]);
         },
         up,
         [&](int p, long long v0, long long v1) {
           const int c = (int)code[p];
-          if (c > 0) Y[c - 1] = make_float2(from_fx(v0, dn[0]), from_fx(v1, dn[1]));
+          if (c > 0) Y[rc_pad8(c - 1)] = make_float2(from_fx(v0, dn[0]), from_fx(v1, dn[1]));
         },
         shl);
     m[0] = m[1] = 0.f;
     out = (float2*)a.delay;
     for (int r = tid; r < n; r += T) {
       const int i = (int)pre[nas[r]];
-      const float2 d = Y[i];
+      const float2 d = Y[rc_pad8(i)];
       out[2 * (size_t)(b + r) + cp] = d;
-      max2_accumulate(f2mul(capI[2 * i], d), m);
+      max2_accumulate(f2mul(capI[2 * rc_pad16(i)], d), m);
     }
     max2_commit(m, smx + 4);
     __syncthreads();
@@ -952,41 +952,41 @@ __device__ void rc_net_block(const RcArgs& a, int net, char* ws, int n, int* sh,
     // ldelay (up): cap*delay over the subtree
     scale(2);
     // each thread reads its own slots' caps before it writes their sums
-    up_scan_fx<T, K>(n, [&](int i) { return f2mul(capI[2 * i], Y[i]); }, up, Ip, shl);
+    up_scan_fx<T, K>(n, [&](int i) { return f2mul(capI[2 * rc_pad16(i)], Y[rc_pad8(i)]); }, up, Ip, shl);
     m[0] = m[1] = 0.f;
     for (int i = tid; i < n; i += T) {
       const float2 v = up_range_fx(Ip, i, i + (int)size[i] - 1, dn);
-      X[i] = v;
+      X[rc_pad8(i)] = v;
       max2_accumulate(f2scale(v, pres[i]), m);
     }
     max2_commit(m, smx + 6);
     __syncthreads();
     out = (float2*)a.ldelay;
-    for (int r = tid; r < n; r += T) out[2 * (size_t)(b + r) + cp] = X[pre[nas[r]]];
+    for (int r = tid; r < n; r += T) out[2 * (size_t)(b + r) + cp] = X[rc_pad8(pre[nas[r]])];
     PHASE(10);
     // beta (down) -> impulse = 2*beta - delay^2, kept where Ip was
     scale(3);
     float2* imp = (float2*)Ip;
-    if (tid == 0) imp[0] = make_float2(0.f, 0.f);
+    if (tid == 0) imp[2 * rc_pad16(0)] = make_float2(0.f, 0.f);
     down_scan_fx<T, K>(
         A,
         [&](int p) {
           const int c = (int)code[p];
           const int i = (c > 0 ? c : -c) - 1;
-          return f2scale(X[i], c > 0 ? pres[i] : -pres[i]);
+          return f2scale(X[rc_pad8(i)], c > 0 ? pres[i] : -pres[i]);
         },
         up,
         [&](int p, long long v0, long long v1) {
           const int c = (int)code[p];
           if (c > 0) {
-            const float2 d = Y[c - 1];
-            imp[c - 1] = make_float2(fmaf(-d.x, d.x, 2.0f * from_fx(v0, dn[0])),
+            const float2 d = Y[rc_pad8(c - 1)];
+            imp[2 * rc_pad16(c - 1)] = make_float2(fmaf(-d.x, d.x, 2.0f * from_fx(v0, dn[0])),
                                      fmaf(-d.y, d.y, 2.0f * from_fx(v1, dn[1])));
           }
         },
         shl);
     out = (float2*)a.impulse;
-    for (int r = tid; r < n; r += T) out[2 * (size_t)(b + r) + cp] = imp[pre[nas[r]]];
+    for (int r = tid; r < n; r += T) out[2 * (size_t)(b + r) + cp] = imp[2 * rc_pad16(pre[nas[r]])];
     if (a.sinks_start) {
       const int s0 = a.sinks_start[net], s1 = a.sinks_start[net + 1];
       const float2 si = ((const float2*)a.driver_slew)[2 * (size_t)net + cp];
@@ -994,7 +994,7 @@ __device__ void rc_net_block(const RcArgs& a, int net, char* ws, int n, int* sh,
       for (int k = s0 + tid; k < s1; k += T) {
         const int v = a.sink_nodes[k];
         if ((unsigned)v >= (unsigned)n) { report(a, OTG_ERR_INVALID, net); continue; }
-        const float2 iv = imp[pre[v]];
+        const float2 iv = imp[2 * rc_pad16(pre[v])];
         so[2 * (size_t)k + cp] = make_float2(sink_slew1(si.x, iv.x), sink_slew1(si.y, iv.y));
       }
     }

@@ -42,9 +42,11 @@ def run(g):
     return b, {k: getattr(b, k).cpu().numpy() for k in OUT}
 
 
-def random_tuning(rng):
+def random_tuning(rng, hi):
+    """A random valid table; hi: the largest net the block path holds in
+    shared memory (the default table's last bound)."""
     k = int(rng.integers(1, 7))
-    bounds = np.sort(rng.choice(np.arange(40, 4800), k, replace=False))
+    bounds = np.sort(rng.choice(np.arange(40, hi + 1), k, replace=False))
     shapes = [SHAPES[int(i)] for i in rng.integers(0, len(SHAPES), k)]
     return {"class_max": [int(x) for x in bounds], "class_threads": [s[0] for s in shapes],
             "class_items": [s[1] for s in shapes]}
@@ -53,10 +55,11 @@ def random_tuning(rng):
 def test_every_tuning_gives_identical_outputs(cuda, restore_tuning):
     g = forest(cuda)
     otg.set_tuning(None)
+    hi = otg.get_tuning()["class_max"][-1]
     _, ref = run(g)
     rng = np.random.default_rng(8)
     for _ in range(6):
-        t = random_tuning(rng)
+        t = random_tuning(rng, hi)
         otg.set_tuning(t)
         assert otg.get_tuning() == t
         _, got = run(g)
