@@ -867,17 +867,23 @@ __device__ void rc_net_block(const RcArgs& a, int net, char* ws, int n, int* sh,
     __syncthreads();
   }
   PHASE(6);
-  // ---- A8: topology outputs, parent resistance by preorder
+  // ---- A8: topology outputs, parent resistance by preorder (read in edge
+  // order, coalesced, and placed at the child's preorder slot).  From here
+  // on nas[r] holds the preorder slot of BFS slot r (bpre).
+  Ix* bpre = nas;
   for (int v = tid; v < n; v += T) a.node2bfs[b + v] = (int)slot[v];
   for (int r = tid; r < n; r += T) {
     const int v = (int)nas[r];
     a.pid[b + r] = r == 0 ? 0 : r - (int)slot[parent[v]];
+    bpre[r] = pre[v];
   }
+  if (tid == 0) pres[0] = 0.0f;
   for (int e = tid; e < m; e += T) {
     const int s = (int)es[e], t = (int)et[e];
-    a.edges[eb + e] = ((int)pedge[t] == e) ? make_int2(s, t) : make_int2(t, s);
+    const bool down = (int)pedge[t] == e;  // t is the child of edge e
+    a.edges[eb + e] = down ? make_int2(s, t) : make_int2(t, s);
+    pres[(int)pre[down ? t : s]] = a.res[eb + e];
   }
-  for (int i = tid; i < n; i += T) pres[i] = i == 0 ? 0.0f : a.res[eb + (int)pedge[nap[i]]];
   __syncthreads();
   PHASE(7);
 
@@ -918,7 +924,7 @@ __device__ void rc_net_block(const RcArgs& a, int net, char* ws, int n, int* sh,
     max2_commit(m, smx + 2);
     __syncthreads();
     out = (float2*)a.load;
-    for (int r = tid; r < n; r += T) out[2 * (size_t)(b + r) + cp] = X[rc_pad8(pre[nas[r]])];
+    for (int r = tid; r < n; r += T) out[2 * (size_t)(b + r) + cp] = X[rc_pad8(bpre[r])];
     for (int i = tid; i < n; i += T) capI[2 * rc_pad16(i)] = Y[rc_pad8(i)];  // Ip is free until the ldelay sweep
     __syncthreads();
     PHASE(8);
@@ -941,7 +947,7 @@ __device__ void rc_net_block(const RcArgs& a, int net, char* ws, int n, int* sh,
     m[0] = m[1] = 0.f;
     out = (float2*)a.delay;
     for (int r = tid; r < n; r += T) {
-      const int i = (int)pre[nas[r]];
+      const int i = (int)bpre[r];
       const float2 d = Y[rc_pad8(i)];
       out[2 * (size_t)(b + r) + cp] = d;
       max2_accumulate(f2mul(capI[2 * rc_pad16(i)], d), m);
@@ -962,7 +968,7 @@ __device__ void rc_net_block(const RcArgs& a, int net, char* ws, int n, int* sh,
     max2_commit(m, smx + 6);
     __syncthreads();
     out = (float2*)a.ldelay;
-    for (int r = tid; r < n; r += T) out[2 * (size_t)(b + r) + cp] = X[rc_pad8(pre[nas[r]])];
+    for (int r = tid; r < n; r += T) out[2 * (size_t)(b + r) + cp] = X[rc_pad8(bpre[r])];
     PHASE(10);
     // beta (down) -> impulse = 2*beta - delay^2, kept where Ip was
     scale(3);
@@ -986,7 +992,7 @@ __device__ void rc_net_block(const RcArgs& a, int net, char* ws, int n, int* sh,
         },
         shl);
     out = (float2*)a.impulse;
-    for (int r = tid; r < n; r += T) out[2 * (size_t)(b + r) + cp] = imp[2 * rc_pad16(pre[nas[r]])];
+    for (int r = tid; r < n; r += T) out[2 * (size_t)(b + r) + cp] = imp[2 * rc_pad16(bpre[r])];
     if (a.sinks_start) {
       const int s0 = a.sinks_start[net], s1 = a.sinks_start[net + 1];
       const float2 si = ((const float2*)a.driver_slew)[2 * (size_t)net + cp];
