@@ -44,14 +44,18 @@ __device__ inline bool grid_barrier(GridCtl* c) {
       __threadfence();
       atomicAdd(&c->gen, 1u);
     } else {
+      // the abort flag and the clock are read on every 8th poll only, so
+      // that a poll costs one round trip, not two
       const unsigned long long t0 = gtime();
-      while (vc->gen == gen) {
-        if (vc->abort) { ok = 0; break; }
-        if (gtime() - t0 > kGridWaitNs) {
-          atomicExch(&c->abort, 1);
-          atomicCAS(&c->status, 0, (int)OTG_ERR_TIMEOUT);
-          ok = 0;
-          break;
+      for (int k = 0; vc->gen == gen; ++k) {
+        if ((k & 7) == 7) {
+          if (vc->abort) { ok = 0; break; }
+          if (gtime() - t0 > kGridWaitNs) {
+            atomicExch(&c->abort, 1);
+            atomicCAS(&c->status, 0, (int)OTG_ERR_TIMEOUT);
+            ok = 0;
+            break;
+          }
         }
         __nanosleep(64);
       }

@@ -183,7 +183,8 @@ __device__ __forceinline__ void st_relaxed4(float* p, float a, float b, float c,
 
 // Bounded wait until *p holds a computed value, returned in out; false
 // when this or another wait gave up.  The first polls spin (each is an L2
-// round trip), later ones sleep.
+// round trip), later ones sleep.  The abort flag and the clock are read
+// on every 8th poll only, so that a poll costs one round trip, not two.
 __device__ bool wait_value(const float* p, float& out, GridCtl* c) {
   out = ld_relaxed(p);
   if (__float_as_uint(out) != kPending) return true;
@@ -192,6 +193,7 @@ __device__ bool wait_value(const float* p, float& out, GridCtl* c) {
     if (k >= 64) __nanosleep(64);
     out = ld_relaxed(p);
     if (__float_as_uint(out) != kPending) return true;
+    if ((k & 7) != 7) continue;
     if (*(volatile int*)&c->abort) return false;
     if (gtime() - t0 > kGridWaitNs) {
       atomicExch(&c->abort, 1);
@@ -212,6 +214,7 @@ __device__ bool wait_values(const float* p, const float* q, float& x, float& y, 
     if (__float_as_uint(x) == kPending) x = ld_relaxed(p);
     if (__float_as_uint(y) == kPending) y = ld_relaxed(q);
     if (__float_as_uint(x) != kPending && __float_as_uint(y) != kPending) return true;
+    if ((k & 7) != 7) continue;
     if (*(volatile int*)&c->abort) return false;
     if (gtime() - t0 > kGridWaitNs) {
       atomicExch(&c->abort, 1);
@@ -429,6 +432,16 @@ __device__ bool bprop_warp(const G& G_, int v, int lane, const float* at, float*
       if (mode != 0) {
         // the fanout's required time this combination reads
         const int wc = mode == 1 ? 2 * el + trf : (mode == 2 ? trf : 2 + trf);
+        // arc delays and arrival times are final since the forward pass, so
+        // they are loaded before the wait and arrive during it
+        float dl = nanf(""), a = nanf(""), wa = nanf("");
+        if (mode == 1) {
+          dl = __ldcg(d + 4 * el + 2 * frf + trf);
+        } else {
+          const int ael = mode == 2 ? MAX_ : MIN_, wel = mode == 2 ? MIN_ : MAX_;
+          a = __ldcg(at + 4 * v + 2 * ael + frf);
+          wa = __ldcg(at + 4 * w + 2 * wel + trf);
+        }
         float wr;
         if (!wait_value(rat + 4 * w + wc, wr, ctl)) {
           ok = false;
@@ -436,17 +449,12 @@ __device__ bool bprop_warp(const G& G_, int v, int lane, const float* at, float*
         }
         if (mode == 1) {
           tc = 2 * el + frf;
-          const float dl = __ldcg(d + 4 * el + 2 * frf + trf);
           if (!none(wr) && !none(dl)) cand = __fsub_rn(wr, dl);
         } else if (mode == 2) {  // hold-like: w's MIN slack moves v's MAX rat
           tc = 2 * MAX_ + frf;
-          const float a = __ldcg(at + 4 * v + 2 * MAX_ + frf);
-          const float wa = __ldcg(at + 4 * w + trf);
           if (!none(a) && !none(wa) && !none(wr)) cand = __fadd_rn(a, __fsub_rn(wa, wr));
         } else {  // setup-like: w's MAX slack moves v's MIN rat
           tc = 2 * MIN_ + frf;
-          const float a = __ldcg(at + 4 * v + 2 * MIN_ + frf);
-          const float wa = __ldcg(at + 4 * w + 2 + trf);
           if (!none(a) && !none(wa) && !none(wr)) cand = __fsub_rn(a, __fsub_rn(wr, wa));
         }
       }
