@@ -44,8 +44,9 @@ __device__ inline bool grid_barrier(GridCtl* c) {
       __threadfence();
       atomicAdd(&c->gen, 1u);
     } else {
-      // the abort flag and the clock are read on every 8th poll only, so
-      // that a poll costs one round trip, not two
+      // each poll is one L2 round trip: the abort flag and the clock are
+      // read on every 8th poll only, and no poll sleeps (a sleeping thread
+      // sees the release only after it wakes)
       const unsigned long long t0 = gtime();
       for (int k = 0; vc->gen == gen; ++k) {
         if ((k & 7) == 7) {
@@ -57,7 +58,6 @@ __device__ inline bool grid_barrier(GridCtl* c) {
             break;
           }
         }
-        __nanosleep(64);
       }
     }
     __threadfence();

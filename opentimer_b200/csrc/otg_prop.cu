@@ -182,15 +182,14 @@ __device__ __forceinline__ void st_relaxed4(float* p, float a, float b, float c,
 }
 
 // Bounded wait until *p holds a computed value, returned in out; false
-// when this or another wait gave up.  The first polls spin (each is an L2
-// round trip), later ones sleep.  The abort flag and the clock are read
-// on every 8th poll only, so that a poll costs one round trip, not two.
+// when this or another wait gave up.  Each poll is one L2 round trip: the
+// abort flag and the clock are read on every 8th poll only, and no poll
+// sleeps, since a sleeping warp sees a new value only after it wakes.
 __device__ bool wait_value(const float* p, float& out, GridCtl* c) {
   out = ld_relaxed(p);
   if (__float_as_uint(out) != kPending) return true;
   const unsigned long long t0 = gtime();
   for (int k = 0;; ++k) {
-    if (k >= 64) __nanosleep(64);
     out = ld_relaxed(p);
     if (__float_as_uint(out) != kPending) return true;
     if ((k & 7) != 7) continue;
@@ -210,7 +209,6 @@ __device__ bool wait_values(const float* p, const float* q, float& x, float& y, 
   if (__float_as_uint(x) != kPending && __float_as_uint(y) != kPending) return true;
   const unsigned long long t0 = gtime();
   for (int k = 0;; ++k) {
-    if (k >= 64) __nanosleep(64);
     if (__float_as_uint(x) == kPending) x = ld_relaxed(p);
     if (__float_as_uint(y) == kPending) y = ld_relaxed(q);
     if (__float_as_uint(x) != kPending && __float_as_uint(y) != kPending) return true;
