@@ -202,7 +202,8 @@ otg_status otg_rc_timing_noalloc(const otg_rc_forest* forest, int32_t max_net_no
 /*
  * ---- Device-resident designs and the incremental timing server ----------
  * (no counterpart in the reference, whose Timer recomputes dirty nets on the
- * CPU and whose GPU path is valid only for a first full update).
+ * CPU and whose CUDA path flattens and re-times every net of the design on
+ * each update; ot/timer/timer.cpp:929-966).
  *
  * A server owns designs whose RC state stays on the device.  A request is
  * an incremental change to one design -- node capacitance updates (a gate

@@ -254,7 +254,7 @@ def verilog(glist, ins, outs):
 def spef(rng, nets):
     """nets: {name: (driver_pin, driver_is_port, [(sink_pin, sink_is_port)])}"""
     out = ['*SPEF "IEEE 1481-1998"', '*DESIGN "top"', '*DATE "0"', '*VENDOR "otg"',
-           '*PROGRAM "config0_design"', '*VERSION "0"', '*DESIGN_FLOW "NETLIST_TYPE_VERILOG"',
+           '*PROGRAM "opentimer_b200 designgen"', '*VERSION "0"', '*DESIGN_FLOW "NETLIST_TYPE_VERILOG"',
            "*DIVIDER /", "*DELIMITER :", "*BUS_DELIMITER [ ]", "*T_UNIT 1 NS", "*C_UNIT 1 FF",
            "*R_UNIT 1 OHM", "*L_UNIT 1 HENRY", ""]
     for name in sorted(nets):

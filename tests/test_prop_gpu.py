@@ -15,7 +15,7 @@ import subprocess
 import numpy as np
 import pytest
 
-from opentimer_b200 import designgen as config0_design
+from opentimer_b200 import designgen
 import opentimer_b200 as otg
 
 pytestmark = pytest.mark.gpu
@@ -68,7 +68,7 @@ def design(tmp_path_factory, cuda):
     if not os.path.exists(EXE_REF):
         pytest.skip("the reference Timer harness (oracle/_ref) is not built")
     d = str(tmp_path_factory.mktemp("prop"))
-    config0_design.write_design(d, seed=2024, gates=2000)
+    designgen.write_design(d, seed=2024, gates=2000)
     graph = os.path.join(d, "graph.txt")
     ref_gpu, pin_cap = ref_run(d, "cuda", graph)
     ref_cpu, _ = ref_run(d, "cpu")

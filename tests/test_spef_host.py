@@ -9,7 +9,7 @@ import os
 import numpy as np
 import pytest
 
-from opentimer_b200 import designgen as config0_design
+from opentimer_b200 import designgen
 import oracle as O
 from opentimer_b200.spef import read_spef
 
@@ -41,7 +41,7 @@ def assert_same(path, **kw):
 
 
 def test_generated_design(tmp_path):
-    config0_design.write_design(str(tmp_path), seed=7, gates=800)
+    designgen.write_design(str(tmp_path), seed=7, gates=800)
     f = assert_same(tmp_path / "design.spef", threads=3)
     assert len(f["net_names"]) > 800
     # every pin of every net is a tree node; the root is one of them

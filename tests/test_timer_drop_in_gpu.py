@@ -23,7 +23,7 @@ import subprocess
 import numpy as np
 import pytest
 
-from opentimer_b200 import designgen as config0_design
+from opentimer_b200 import designgen
 
 pytestmark = pytest.mark.gpu
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
@@ -96,8 +96,8 @@ def pins_ok(got, ref):
 def runs(tmp_path_factory, cuda):
     if not (os.path.exists(EXE_REF) and os.path.exists(EXE_OTG)):
         pytest.skip("the reference Timer harness (oracle/_ref) is not built")
-    d = str(tmp_path_factory.mktemp("config0"))
-    info = config0_design.write_design(d, seed=2024, gates=2000)
+    d = str(tmp_path_factory.mktemp("design2k"))
+    info = designgen.write_design(d, seed=2024, gates=2000)
     return (dict(info, dir=d), run(EXE_REF, d, "cuda"), run(EXE_OTG, d, "cuda"),
             run(EXE_REF, d, "cpu"))
 
@@ -113,7 +113,7 @@ def test_rc_nodes_within_tolerance(runs):
     assert set(ours[1]) == set(ref[1]) == set(cpu[1])
     w_gpu = rc_ok(ours[1], ref[1])
     w_cpu = rc_ok(ours[1], cpu[1])
-    print(f"config 0 ({info}): RC err/tol vs reference GPU {w_gpu:.3g}, vs CPU {w_cpu:.3g}")
+    print(f"2k-gate design ({info}): RC err/tol vs reference GPU {w_gpu:.3g}, vs CPU {w_cpu:.3g}")
     assert w_gpu <= 1.0 and w_cpu <= 1.0
 
 
