@@ -2,7 +2,7 @@
  * otg_oracle.c -- CPU restatement of OpenTimer's RC-net timing and
  * timing-graph levelization.  TEST INFRASTRUCTURE ONLY.
  *
- * This file is the checker for the CUDA product path.  Only tests/,
+ * The CUDA product path is tested against this file.  Only tests/,
  * __graft_entry__.smoke() and bench.py's CPU-baseline leg may load it; the
  * product library never links, loads or calls it.
  *
