@@ -31,6 +31,7 @@
 #include <stdint.h>
 
 #include <algorithm>
+#include <climits>
 
 #include "../../include/otg.h"
 #include "otg_internal.cuh"
@@ -45,17 +46,18 @@ using LvCtl = GridCtl;
 // One fanin edge per lane (target v, ok = a valid pin): decrement v's
 // fanout counter; the pin whose counter reaches zero sets its bit in `bm`
 // and counts for its range.  Lanes of a warp that target the same pin
-// combine into one atomicSub.  Every lane of the warp must call it.
-__device__ __forceinline__ void decrement(int v, bool ok, int* cnt, unsigned* bm, const int* level,
-                                          int* rcount, int C) {
+// combine into one atomicSub.  Every lane of the warp must call it.  A
+// seed pin's counter starts at INT_MAX, so a seed is never emitted twice,
+// even if the caller's out_deg disagrees with the fanin lists, and no
+// other read is needed on this chain.
+__device__ __forceinline__ void decrement(int v, bool ok, int* cnt, unsigned* bm, int* rcount,
+                                          int C) {
   const int lane = threadIdx.x & 31;
   const unsigned peers = __match_any_sync(FULL, ok ? v : -2 - lane);
   if (ok && (__ffs(peers) - 1 == lane)) {
     const int k = __popc(peers);
     const int old = atomicSub(&cnt[v], k);
-    // a seed pin (level 0) is never emitted twice, even if the caller's
-    // out_deg disagrees with the fanin lists
-    if (old > 0 && old - k <= 0 && level[v] < 0) {
+    if (old > 0 && old - k <= 0) {
       atomicOr(&bm[v >> 5], 1u << (v & 31));
       atomicAdd(&rcount[(v >> 5) / C], 1);
     }
@@ -66,13 +68,13 @@ __device__ __forceinline__ void decrement(int v, bool ok, int* cnt, unsigned* bm
 // (the seed level).
 __device__ __forceinline__ void expand_pin(int u, bool active, const int* fanin_start,
                                            const int* fanin, int* cnt, unsigned* bm, int n,
-                                           const int* level, int* rcount, int C) {
+                                           int* rcount, int C) {
   int e = active ? fanin_start[u] : 0;
   const int e1 = active ? fanin_start[u + 1] : 0;
   while (__any_sync(FULL, e < e1)) {
     const bool has = e < e1;
     const int v = has ? fanin[e] : -1;
-    decrement(v, has && (unsigned)v < (unsigned)n, cnt, bm, level, rcount, C);
+    decrement(v, has && (unsigned)v < (unsigned)n, cnt, bm, rcount, C);
     e += has ? 1 : 0;
   }
 }
@@ -104,8 +106,12 @@ __global__ void __launch_bounds__(LT) levelize_kernel(int n, const int* fanin_st
   for (int k = gtid; k < first_size; k += gstride) {
     const int v = frontier0[k];
     order[k] = v;
-    if ((unsigned)v < (unsigned)n) level[v] = 0;
-    else atomicCAS(&ctl->status, 0, (int)OTG_ERR_INVALID);
+    if ((unsigned)v < (unsigned)n) {
+      level[v] = 0;
+      cnt[v] = INT_MAX;  // after the counters' fill (grid barrier above)
+    } else {
+      atomicCAS(&ctl->status, 0, (int)OTG_ERR_INVALID);
+    }
   }
   if (gtid == 0) {
     level_ends[0] = 0;
@@ -120,7 +126,7 @@ __global__ void __launch_bounds__(LT) levelize_kernel(int n, const int* fanin_st
   for (int k0 = b * LT; k0 < first_size; k0 += gstride) {
     const int k = k0 + tid;
     const bool act = k < first_size && (unsigned)order[k] < (unsigned)n;
-    expand_pin(act ? order[k] : 0, act, fanin_start, fanin, cnt, bm0, n, level, blk + G, C);
+    expand_pin(act ? order[k] : 0, act, fanin_start, fanin, cnt, bm0, n, blk + G, C);
   }
   unsigned* cur = bm0;
   unsigned* nxt = bm1;
@@ -248,7 +254,7 @@ __global__ void __launch_bounds__(LT) levelize_kernel(int n, const int* fanin_st
             }
             v = fanin[s_e0[lo] + (q - s_estart[lo])];
           }
-          decrement(v, (unsigned)v < (unsigned)n, cnt, nxt, level, rc_next, C);
+          decrement(v, (unsigned)v < (unsigned)n, cnt, nxt, rc_next, C);
         }
         __syncthreads();  // s_estart / s_e0 / wsum are reused
       }
