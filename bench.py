@@ -811,12 +811,12 @@ def run_full_update(dump=None, baseline=None):
                     b["reference_cuda_vs_cpu_pins_err_over_tol"] = pin_err(ref["cuda"][1],
                                                                            ref["cpu"][1])
             baseline["full_update"] = b
-        out["incremental_spef"] = _incremental_spef(d, keep, f, caps, batch, graph, arrays, names,
+        out["incremental_spef"] = _incremental_spef(d, keep, f, caps, batch, graph, names,
                                                     baseline)
     return out
 
 
-def _incremental_spef(d, keep, f0, caps, batch, graph, arrays, names, baseline=None):
+def _incremental_spef(d, keep, f0, caps, batch, graph, names, baseline=None):
     """A change SPEF (TAU15 change_*.spef style) re-drawing FU_CHANGE of the
     design's nets, applied to the device-resident design: the host reads
     the file and maps its nets and pins, then RcBatch.replace_nets moves
@@ -828,23 +828,19 @@ def _incremental_spef(d, keep, f0, caps, batch, graph, arrays, names, baseline=N
     import subprocess
     import torch
     from opentimer_b200 import designgen
-    from opentimer_b200.prop import change_nets
+    from opentimer_b200.prop import change_arcs, change_nets
     from opentimer_b200.spef import read_spef
     path = os.path.join(d, "change.spef")
     changed = designgen.change_spef(keep, path, frac=FU_CHANGE, seed=SEED + 31)
     # design state kept between changes, as the Timer keeps its net map
     index = {n: i for i, n in enumerate(f0["net_names"])}
-    arc_net = graph.dev["arc_net"].cpu().numpy()
-    net_arc = np.asarray(arrays["arc_kind"]) == 0
     host_t = []
     for _ in range(FU_REPS):  # the host part is repeatable: median of FU_REPS
         t0 = time.perf_counter()
         fc = read_spef(path, r_scale=np.float32(1e-3))
         nets, forest, node_of = change_nets(fc, index, caps)
         # net arcs into the changed nets get their sinks' new local ids
-        sel = np.nonzero(net_arc & np.isin(arc_net, nets))[0]
-        nodes = [node_of.get((int(arc_net[k]), names[int(arrays["arc_to"][k])]), -1)
-                 for k in sel]
+        sel, nodes = change_arcs(graph.net_arcs, graph.arc_to, names, nets, node_of)
         host_t.append(1e3 * (time.perf_counter() - t0))
     host_ms = float(np.median(host_t))
     forest_d = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in forest]

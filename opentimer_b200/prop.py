@@ -10,6 +10,8 @@ comes from otg_levelize over the graph's fanin CSR.
 """
 import ctypes
 
+from itertools import compress
+
 import numpy as np
 
 from . import LevelizeBatch, _ptr, _stream, check, lib
@@ -72,6 +74,9 @@ class TimingGraph:
         t = lambda x, dt: torch.from_numpy(  # noqa: E731
             np.ascontiguousarray(x, dt).reshape(-1) if np.size(x) else np.zeros(1, dt)).to(device)
         self.dev = {k: t(v, np.int32) for k, v in host.items()}
+        # what the host side of an incremental change reads
+        self.arc_to = np.asarray(a["arc_to"], np.int32)
+        self.net_arcs = net_arc_index(a["arc_kind"], a["arc_net"])
         for k in ("pi_at", "pi_slew", "po_rat", "lut_data"):
             self.dev[k] = t(a[k], np.float32)
         self.graph = PropGraph(P, A, len(test_arc),
@@ -135,6 +140,15 @@ class TimingGraph:
             _stream(stream)))
         return self
 
+    def change_nets(self, nets, node_of, pin_names):
+        """After RcBatch.replace_nets(nets, ...) with change_nets' output:
+        points the net arcs into those nets at their sinks' new local ids.
+        Returns (arcs, nodes)."""
+        arcs, nodes = change_arcs(self.net_arcs, self.arc_to, pin_names, nets, node_of)
+        if len(arcs):
+            self.set_arc_nodes(arcs, nodes)
+        return arcs, nodes
+
     def set_arc_nodes(self, arcs, nodes):
         """New sink node ids (local to their nets) for some net arcs, as
         after an incremental SPEF replaced their nets' trees."""
@@ -153,26 +167,34 @@ class TimingGraph:
         return {k: v.cpu().numpy() for k, v in self.out.items()}
 
 
-def rc_inputs(spef, pin_caps):
+def rc_inputs(spef, pin_caps, net_ids=None):
     """Flat RC inputs from read_spef's output plus each non-root pin's cap
     (pin_caps: name -> [4]), as the flat path adds them (ot/timer/
     net.cpp:433-446).  Returns (cap [V,4], node_of {(net, pin name): the
-    pin's local node id in the net})."""
-    ns, ps = np.asarray(spef["nodes_start"]), np.asarray(spef["pins_start"])
+    pin's local node id in the net}).  With net_ids (an index per net of
+    the file, -1 for none), node_of is keyed by those indices and leaves
+    out the nets without one."""
+    ns, ps = np.asarray(spef["nodes_start"], np.int64), np.asarray(spef["pins_start"])
     cap = spef["cap"].copy()
     names = spef["pin_names"]
     net = np.repeat(np.arange(len(ns) - 1), np.diff(ps))
     node = np.asarray(spef["pin_node"], np.int64)
     on = np.nonzero(node >= 0)[0]
-    node_of = dict(zip(zip(net[on].tolist(), [names[q] for q in on]), node[on].tolist()))
-    nonroot = on[node[on] != np.asarray(spef["roots"])[net[on]]]
-    rows, vals = [], []
-    for q in nonroot.tolist():
-        c = pin_caps.get(names[q])
-        if c is not None:
-            rows.append(int(ns[net[q]]) + int(node[q]))
-            vals.append(c)
-    if rows:  # float32 adds, in pin order (np.add.at is unbuffered)
+    on_names = [names[q] for q in on.tolist()]
+    if net_ids is None:
+        node_of = dict(zip(zip(net[on].tolist(), on_names), node[on].tolist()))
+    else:
+        key = np.asarray(net_ids, np.int64)[net[on]]
+        m = key >= 0
+        node_of = dict(zip(zip(key[m].tolist(), compress(on_names, m.tolist())),
+                           node[on][m].tolist()))
+    nonroot = node[on] != np.asarray(spef["roots"])[net[on]]
+    get = pin_caps.get
+    found = [(r, c) for r, c in zip((ns[net[on]] + node[on])[nonroot].tolist(),
+                                    (get(nm) for nm, k in zip(on_names, nonroot.tolist()) if k))
+             if c is not None]
+    if found:  # float32 adds, in pin order (np.add.at is unbuffered)
+        rows, vals = zip(*found)
         np.add.at(cap, np.asarray(rows, np.int64), np.asarray(vals, np.float32))
     return cap, node_of
 
@@ -196,10 +218,12 @@ def change_nets(spef_change, net_index, pin_caps):
     with the pin caps added) for RcBatch.replace_nets, and node_of
     {(forest net, pin name): local node} for the arcs into them."""
     f = spef_change
-    cap, node_local = rc_inputs(f, pin_caps)
     ns = np.asarray(f["nodes_start"], np.int64)
     keep = np.array([i for i, n in enumerate(f["net_names"]) if n in net_index], np.int64)
     nets = np.array([net_index[f["net_names"][i]] for i in keep.tolist()], np.int64)
+    net_ids = np.full(len(ns) - 1, -1, np.int64)
+    net_ids[keep] = nets
+    cap, node_of = rc_inputs(f, pin_caps, net_ids)
     sizes = ns[keep + 1] - ns[keep] if len(keep) else np.zeros(0, np.int64)
     sub_ns = np.zeros(len(keep) + 1, np.int64)
     np.cumsum(sizes, out=sub_ns[1:])
@@ -208,9 +232,36 @@ def change_nets(spef_change, net_index, pin_caps):
     forest = (sub_ns.astype(np.int32), f["edges"][edge_rows].copy(),
               np.asarray(f["roots"])[keep].astype(np.int32), f["res"][edge_rows].copy(),
               cap[node_rows].copy())
-    back = dict(zip(keep.tolist(), nets.tolist()))
-    node_of = {(back[i], pin): node for (i, pin), node in node_local.items() if i in back}
     return nets, forest, node_of
+
+
+def net_arc_index(arc_kind, arc_net):
+    """The graph's net arcs grouped by their forest net, for change_arcs:
+    (arcs, nets), both sorted by net (arcs ascending within a net)."""
+    arc_net = np.asarray(arc_net)
+    na = np.nonzero((np.asarray(arc_kind) == 0) & (arc_net >= 0))[0]
+    by = np.argsort(arc_net[na], kind="stable")
+    return na[by], arc_net[na][by]
+
+
+def change_arcs(index, arc_to, pin_names, nets, node_of):
+    """The net arcs into the nets a change SPEF replaced (`nets`, forest
+    indices), ascending, and their sinks' new local ids from change_nets'
+    node_of (-1: the sink is not in the new tree): (arcs, nodes) for
+    TimingGraph.set_arc_nodes.  index is net_arc_index's output and arc_to
+    the graph's per-arc sink pins, both kept with the design."""
+    arcs_by_net, net_of = index
+    nets = np.asarray(nets, np.int64)
+    if len(nets) == 0:
+        return np.zeros(0, np.int64), []
+    lo = np.searchsorted(net_of, nets, side="left")
+    hi = np.searchsorted(net_of, nets, side="right")
+    rows = _ranges(lo, hi - lo)
+    by_id = np.argsort(arcs_by_net[rows], kind="stable")
+    arcs, arc_nets = arcs_by_net[rows][by_id], net_of[rows][by_id]
+    get = node_of.get
+    return arcs, [get((i, pin_names[t]), -1)
+                  for i, t in zip(arc_nets.tolist(), np.asarray(arc_to)[arcs].tolist())]
 
 
 def attach_nets(arrays, pin_names, pin_net_names, spef, node_of):

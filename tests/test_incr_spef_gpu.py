@@ -136,7 +136,9 @@ def test_incremental_update_matches_reference_timer(design):
             arcs.append(k)
             nodes.append(node_of_c.get((i, pin_names[int(arrays["arc_to"][k])]), -1))
     assert arcs
-    g.set_arc_nodes(arcs, nodes)
+    # the graph's own mapping (what a caller uses) agrees and applies it
+    got_arcs, got_nodes = g.change_nets(nets, node_of_c, pin_names)
+    assert got_arcs.tolist() == arcs and got_nodes == nodes
     out = g.propagate(b1).result()
     out["rat"] = np.where(np.isnan(out["at"]), np.nan, out["rat"])
     # RC at every pin node, all nets (changed and moved)
