@@ -188,13 +188,14 @@ def rc_inputs(spef, pin_caps, net_ids=None):
         m = key >= 0
         node_of = dict(zip(zip(key[m].tolist(), compress(on_names, m.tolist())),
                            node[on][m].tolist()))
-    nonroot = node[on] != np.asarray(spef["roots"])[net[on]]
-    get = pin_caps.get
-    found = [(r, c) for r, c in zip((ns[net[on]] + node[on])[nonroot].tolist(),
-                                    (get(nm) for nm, k in zip(on_names, nonroot.tolist()) if k))
-             if c is not None]
-    if found:  # float32 adds, in pin order (np.add.at is unbuffered)
-        rows, vals = zip(*found)
+    nonroot = (node[on] != np.asarray(spef["roots"])[net[on]]).tolist()
+    rows, vals = [], []
+    for row, name, add in zip((ns[net[on]] + node[on]).tolist(), on_names, nonroot):
+        c = pin_caps.get(name) if add else None
+        if c is not None:
+            rows.append(row)
+            vals.append(c)
+    if rows:  # float32 adds, in pin order (np.add.at is unbuffered)
         np.add.at(cap, np.asarray(rows, np.int64), np.asarray(vals, np.float32))
     return cap, node_of
 
