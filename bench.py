@@ -157,6 +157,27 @@ def rank_nets(rank, nets, lo, hi):
     return workloads.net_sizes(SEED + rank, nets, lo, hi)
 
 
+def load_workloads():
+    """opentimer_b200/workloads.py as a standalone module (numpy only), so
+    the reference arm sizes the workload without loading the package and
+    its library."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location(
+        "otg_workloads", os.path.join(ROOT, "opentimer_b200", "workloads.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def headline_config(nets, total_nodes, lo, hi, world):
+    """The `config` of the headline line, the same dict in both arms."""
+    return {"workload": f"batched Elmore: {nets} RC nets/GPU, log-uniform {lo}..{hi} nodes, "
+                        "70% random recursive trees / 30% chains, 4 corners, sink slews",
+            "num_nets_per_gpu": nets, "total_nodes_per_gpu": total_nodes, "seed": SEED,
+            "l2": "inputs and outputs (>60 GB) far exceed L2; no flush needed",
+            "parallelism": f"replicas x{world} (nets shard with no collective)"}
+
+
 def load_peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -213,40 +234,59 @@ def calibrate_cpu(make_forest, ns, threads):
 # ------------------------------------------------------------------ main
 
 def run_reference(args, world, rank):
-    """--impl reference: the reference's CPU path, rank 0 only."""
+    """--impl reference: the reference's own CPU path (Rct::update_rc_timing
+    in a Cpp-Taskflow parallel_for over all host threads, oracle/_ref) on
+    the headline workload, rank 0 only.  Each timed step takes its own
+    1/steps of the workload's nets, so the timed steps together cover all
+    of its nets once; warm-up steps repeat the first slices.  Inputs come
+    from the oracle's host generator (bit-identical to the device
+    generator), built outside the timed region; the product library is not
+    loaded in this arm."""
     if rank != 0:
         return
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
-    import opentimer_b200 as otg
-    ns_full = otg.workloads.net_sizes(SEED, NUM_NETS)
+    wl = load_workloads()
+    ns_full = wl.net_sizes(SEED, args.nets, args.min_nodes, args.max_nodes).astype(np.int64)
+    N, V_full = args.nets, int(ns_full[-1])
     threads = os.cpu_count() or 1
-    # the same nets, generated on the host (bit-identical to the device generator)
-    def make(k):
-        ns = ns_full[:k + 1].copy()
-        g = otg.synth_forest_host(SEED, ns)
-        return O.Forest(ns, g["edges"], g["roots"], g["res"], g["cap"])
-    rate = calibrate_cpu(make, ns_full, threads)
-    # each step ~ (20 s / steps) of CPU work, so the whole run stays within minutes
-    k = sample_nets_for_budget(ns_full, 20.0 / max(1, args.steps + args.warmup), rate)
-    f = make(k)
-    times = []
+    steps = max(1, args.steps)
+    cuts = [int(round(N * k / steps)) for k in range(steps + 1)]
+    kind = "reference" if O.ref_available() else "port"
+    times, nodes = [], 0
     for i in range(args.warmup + args.steps):
-        dt, kind, cores = time_reference_cpu(f, threads)
+        k = (i - args.warmup) % steps if i >= args.warmup else i % steps
+        a, b = cuts[k], cuts[k + 1]
+        f, _, _ = O.synth_forest(SEED, ns_full[a:b + 1], first_net=a, threads=threads)
+        if kind == "reference":
+            t0 = time.perf_counter()
+            st, _ = O.ref_rct_update(f, threads, readback=False)
+            dt = time.perf_counter() - t0
+            if st != 0:
+                raise RuntimeError("reference CPU path failed")
+        else:
+            t0 = time.perf_counter()
+            O.elmore_cpu_f32(f)
+            dt = time.perf_counter() - t0
         if i >= args.warmup:
             times.append(dt)
-    V = f.total_nodes
-    ms = 1e3 * statistics.mean(times)
-    value = V / (ms / 1e3)
+            nodes += f.total_nodes
+        del f
+    total = sum(times)
+    value = nodes / total
+    cores = threads if kind == "reference" else 1
     line = {
         "metric": METRIC, "value": value, "unit": "nodes/s", "impl": "reference",
-        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * total / len(times),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic (seeded; same generator as the GPU arm, host copy)",
-        "config": {"workload": "batched Elmore, log-uniform 2..4096-node RC nets (sample)",
-                   "num_nets": k, "total_nodes": V, "sample_of_num_nets": NUM_NETS},
+        "data": "synthetic (seeded; the GPU arm's generator restated on the host)",
+        "config": headline_config(N, V_full, args.min_nodes, args.max_nodes, world),
         "cpu_baseline": {"value": value, "unit": "nodes/s", "cores": cores, "kind": kind,
-                         "sample": f"first {k} of {NUM_NETS} nets ({V} nodes) per step"},
+                         "sample": f"each timed step one 1/{steps} slice of the {N} nets; the "
+                                   f"{args.steps} timed steps cover {nodes} of {V_full} nodes; "
+                                   "Rct built and timed per net as Net::_update_rc_timing "
+                                   "does, results left in the Rct nodes"},
         "e2e": {"value": value, "unit": "nodes/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -317,6 +357,9 @@ def run_ours(args, world, rank, local):
     ms = ev0.elapsed_time(ev1) / args.steps
     ms = max_over_ranks(world, ms)
     batch.check(stream)
+    # the timed run's own outputs, checked on a sample of its nets
+    parity = _section(check_headline_outputs, batch, ns_np, SEED + rank) \
+        if not args.no_parity else None
     value = world * V / (ms / 1e3)
     peak, peak_kind = load_peaks()
     abytes = algorithmic_bytes(N, V, S)
@@ -325,7 +368,7 @@ def run_ours(args, world, rank, local):
     # ---- end to end through the host C ABI (pinned host buffers)
     e2e = None
     if not args.no_e2e:
-        e2e = run_e2e(args, world, g, ns_np, N, V, S, dev)
+        e2e = run_e2e(args, world, g, ns_np, N, V, S, dev, batch)
 
     # ---- levelization (5M pins, 12M edges, 200 levels)
     lv = run_levelize(args, world, dev) if not args.no_levelize else None
@@ -335,17 +378,13 @@ def run_ours(args, world, rank, local):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded, generated on the device)",
-        "config": {"workload": f"batched Elmore: {N} RC nets/GPU, log-uniform "
-                               f"{args.min_nodes}..{args.max_nodes} nodes, 70% random recursive "
-                               "trees / 30% chains, 4 corners, sink slews",
-                   "num_nets_per_gpu": N, "total_nodes_per_gpu": V, "sinks_per_gpu": S,
-                   "l2": "inputs and outputs (>60 GB) far exceed L2; no flush needed",
-                   "tuning": tuning or "default",
-                   "autotune": ("given (--tuning)" if args.tuning else
-                                f"otg_rc_autotune on {min(TUNE_NETS, args.nets)} nets of the same "
-                                f"distribution (another seed), {tune_s:.1f} s, before warm-up")
-                   if tuning else "off",
-                   "parallelism": f"replicas x{world} (nets shard with no collective)"},
+        "config": headline_config(N, V, args.min_nodes, args.max_nodes, world),
+        "sinks_per_gpu": S,
+        "tuning": tuning or "default",
+        "autotune": ("given (--tuning)" if args.tuning else
+                     f"otg_rc_autotune on {min(TUNE_NETS, args.nets)} nets of the same "
+                     f"distribution (another seed), {tune_s:.1f} s, before warm-up")
+        if tuning else "off",
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": RC_DRAM_BYTES_PER_NODE * V,
                      "traffic_source": "ncu dram bytes per node of the pass (100k-net capture) "
@@ -357,10 +396,14 @@ def run_ours(args, world, rank, local):
     }
     if e2e:
         line["e2e"] = e2e
+    if parity is not None:
+        line["parity"] = parity
     if lv:
         line["levelize"] = lv
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = _section(cpu_baseline, g, ns_np)
+        # the free memory of the timed batch is not needed by the reference run
+        line["reference_gpu_rc"] = _section(reference_gpu_rc, ns_np, SEED + rank)
     # the per-GPU incremental and serving loops (one GPU only)
     if world == 1 and not (args.no_incremental and args.no_serving):
         del batch, g
@@ -373,11 +416,119 @@ def run_ours(args, world, rank, local):
     base = line.get("cpu_baseline")
     if base is not None and lv:
         base["levelize"] = _section(levelize_baseline, lv)
+        if parity is not None and isinstance(base["levelize"], dict):
+            for k in ("levels_match_reference", "levels_match_port"):
+                if k in base["levelize"]:
+                    parity[k] = base["levelize"][k]
     if rank == 0 and not args.no_spef:
         line["spef_ingest"] = _section(run_spef, base)
     if world == 1 and not args.no_full_update:
         line["full_update"] = _section(run_full_update, baseline=base if rank == 0 else None)
     return line
+
+
+PARITY_BINS = (2, 33, 129, 257, 513, 1025, 2049, 4097)  # warp path, then block classes
+PARITY_NETS_PER_BIN = 300
+
+
+def _net_max(ns, x):
+    sizes = np.diff(ns)
+    m = np.maximum.reduceat(np.abs(x), ns[:-1], axis=0)
+    return np.repeat(m, sizes, axis=0)
+
+
+def check_headline_outputs(batch, ns_np, seed):
+    """The timed run's outputs on a seeded sample of its nets: PARITY_NETS_PER_BIN
+    nets from each size bin (every size class of the pass), inputs rebuilt
+    on the host by the oracle's generator (bit-identical to the device
+    generator), outputs gathered from the device batch.  BFS slots, pid and
+    directed edges against the oracle's BFS rule (bit-exact); load, delay,
+    ldelay and impulse against the reference's own CPU Rct (oracle/_ref,
+    else the oracle's bit-exact restatement of it) within |d| <= 1e-5|ref| +
+    1e-6 max_net|ref|; sink slews within that tolerance carried through
+    sqrt; and the largest error against an FP64 evaluation, for ours and for
+    the reference, per quantity (max |x - exact| / max_net|exact|)."""
+    import torch
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    ns64 = ns_np.astype(np.int64)
+    sizes = np.diff(ns64)
+    rng = np.random.default_rng(seed + 99)
+    pick = []
+    for lo, hi in zip(PARITY_BINS[:-1], PARITY_BINS[1:]):
+        idx = np.nonzero((sizes >= lo) & (sizes < hi))[0]
+        if len(idx):
+            pick.append(rng.choice(idx, min(PARITY_NETS_PER_BIN, len(idx)), replace=False))
+    nets = np.sort(np.concatenate(pick + [np.argsort(sizes)[-8:]]))
+    nets = np.unique(nets)
+    # host inputs of the sampled nets, one net at a time from the generator
+    parts = [O.synth_forest(seed, ns64[i:i + 2], first_net=int(i), threads=1) for i in nets]
+    n = sizes[nets]
+    fs_ns = np.zeros(len(nets) + 1, np.int64)
+    fs_ns[1:] = np.cumsum(n)
+    f = O.Forest(fs_ns, np.concatenate([p[0].edges for p in parts]),
+                 np.concatenate([p[0].roots for p in parts]),
+                 np.concatenate([p[0].res for p in parts]),
+                 np.concatenate([p[0].cap for p in parts]))
+    slew = np.concatenate([p[1] for p in parts])
+    # device outputs of those nets
+    dev = batch.node2bfs.device
+    node_idx = np.concatenate([np.arange(ns64[i], ns64[i + 1]) for i in nets])
+    edge_idx = np.concatenate([np.arange(ns64[i] - i, ns64[i + 1] - i - 1) for i in nets])
+    ti = torch.from_numpy(node_idx).to(dev)
+    te = torch.from_numpy(edge_idx).to(dev)
+    got = {k: getattr(batch, k).index_select(0, ti).cpu().numpy()
+           for k in ("node2bfs", "pid", "load", "delay", "ldelay", "impulse")}
+    got["edges"] = batch.edges.index_select(0, te).cpu().numpy()
+    ss_dev = batch.sinks_start.cpu().numpy().astype(np.int64)
+    sink_idx = np.concatenate([np.arange(ss_dev[i], ss_dev[i + 1]) for i in nets])
+    ts = torch.from_numpy(sink_idx).to(dev)
+    got_sn = batch.sink_nodes.index_select(0, ts).cpu().numpy()
+    got_ss = batch.sink_slew.index_select(0, ts).cpu().numpy()
+    sn_count = ss_dev[nets + 1] - ss_dev[nets]
+    f_ss = np.zeros(len(nets) + 1, np.int64)
+    f_ss[1:] = np.cumsum(sn_count)
+    out = {"nets_checked": int(len(nets)), "nodes_checked": int(f.total_nodes),
+           "sinks_checked": int(len(sink_idx)),
+           "sample": f"{PARITY_NETS_PER_BIN} seeded nets per size bin {list(PARITY_BINS)} "
+                     "plus the 8 largest, from the timed batch after the timed steps"}
+    st, e, n2b, pid, _ = O.bfs(f)
+    out["bfs_pid_edges_bit_exact"] = bool(
+        st == 0 and np.array_equal(got["node2bfs"], n2b) and np.array_equal(got["pid"], pid)
+        and np.array_equal(got["edges"], e))
+    base = np.repeat(fs_ns[:-1], n)
+    local = {q: got[q][base + got["node2bfs"]] for q in ("load", "delay", "ldelay", "impulse")}
+    threads = os.cpu_count() or 1
+    if O.ref_available():
+        st, ref = O.ref_rct_update(f, threads, readback=True)
+        out["reference"] = "the reference's Rct::update_rc_timing (oracle/_ref)"
+    else:
+        st, ref = O.elmore_cpu_f32(f)
+        out["reference"] = "the oracle's restatement of Rct::update_rc_timing"
+    st64, ex = O.elmore_f64(f)
+    errs, rel_ours, rel_ref = {}, {}, {}
+    for q, r, x in zip(("load", "delay", "ldelay", "impulse"), ref, ex):
+        g = local[q].astype(np.float64)
+        tol = np.maximum(1e-5 * np.abs(r) + 1e-6 * _net_max(fs_ns, r), np.finfo(np.float32).tiny)
+        errs[q] = float(np.max(np.abs(g - r) / tol))
+        nm = np.maximum(_net_max(fs_ns, x), 1e-30)
+        rel_ours[q] = float(np.max(np.abs(g - x) / nm))
+        rel_ref[q] = float(np.max(np.abs(r.astype(np.float64) - x) / nm))
+    out["max_err_over_tol"] = errs
+    out["tolerance"] = "|ours - ref| <= 1e-5 |ref| + 1e-6 max_net|ref| per node, corner, quantity"
+    out["max_rel_vs_fp64"] = rel_ours
+    out["reference_max_rel_vs_fp64"] = rel_ref
+    # sink slews from the reference impulse
+    want = O.sink_slew(f, f_ss.astype(np.int32), got_sn, slew, ref[3])
+    nb = np.repeat(fs_ns[:-1], sn_count)
+    imp = ref[3][nb + got_sn]
+    imp_max = _net_max(fs_ns, ref[3])[nb + got_sn]
+    tol = (1e-5 * np.abs(imp) + 1e-6 * imp_max) / (2 * np.abs(want)) + 1e-6 * np.abs(want)
+    out["sink_slew_max_err_over_tol"] = float(np.max(np.abs(got_ss - want) / tol)) \
+        if len(want) else 0.0
+    out["pass"] = bool(out["bfs_pid_edges_bit_exact"] and st == 0 and st64 == 0 and
+                       max(errs.values()) <= 1.0 and out["sink_slew_max_err_over_tol"] <= 1.0)
+    return out
 
 
 def _section(fn, *args, **kw):
@@ -392,9 +543,12 @@ def _section(fn, *args, **kw):
         return {"error": f"{type(e).__name__}: {e}"}
 
 
-def run_e2e(args, world, g, ns_np, N, V, S, dev):
+def run_e2e(args, world, g, ns_np, N, V, S, dev, batch):
     """Same pass through otg_rc_timing_host: pinned host inputs -> device ->
-    compute -> host outputs, all inside the timed region."""
+    compute -> host outputs, all inside the timed region, `steps` times.
+    Afterwards the host outputs of the first and last 20k nets are compared
+    with the device-resident pass's (`batch`, the same inputs): identical
+    bits expected."""
     import torch
     import opentimer_b200 as otg
     def pin(t):
@@ -417,7 +571,7 @@ def run_e2e(args, world, g, ns_np, N, V, S, dev):
     L = otg.lib()
     for _ in range(1):
         otg.check("otg_rc_timing_host", L.otg_rc_timing_host(ctypes.byref(f)))
-    steps = max(1, min(args.steps, 3))
+    steps = max(1, args.steps)
     barrier(world)
     t0 = time.perf_counter()
     for _ in range(steps):
@@ -427,10 +581,22 @@ def run_e2e(args, world, g, ns_np, N, V, S, dev):
     E = V - N
     h2d = 4 * (N + 1) + 8 * E + 4 * N + 4 * E + 16 * V + 4 * (N + 1) + 4 * S + 16 * N
     d2h = 8 * E + 4 * V + 4 * V + 64 * V + 16 * S
-    # a sanity check of the copies: compare a slice with the device result
+    # the copies carried the pass's results: the first and last 20k nets
+    # against the device-resident pass on the same inputs, bit for bit
+    ok = True
+    for a, b in ((0, min(N, 20_000)), (max(0, N - 20_000), N)):
+        v0, v1 = int(ns_np[a]), int(ns_np[b])
+        for k in ["node2bfs", "pid", "load", "delay", "ldelay", "impulse"]:
+            hd = outs[k][v0:v1].numpy()
+            dd = getattr(batch, k)[v0:v1].cpu().numpy()
+            ok = ok and np.array_equal(hd.view(np.int32), dd.view(np.int32))
+        s0, s1 = int(h_ss[a]), int(h_ss[b])
+        ok = ok and np.array_equal(sink_slew[s0:s1].numpy().view(np.int32),
+                                   batch.sink_slew[s0:s1].cpu().numpy().view(np.int32))
     return {"value": world * V / dt, "unit": "nodes/s", "h2d_bytes_per_step": h2d,
             "d2h_bytes_per_step": d2h, "ms_per_step": dt * 1e3, "steps": steps,
             "host_buffers": "pinned (torch.pin_memory)",
+            "outputs_match_device_pass": bool(ok),
             "path": "otg_rc_timing_host (chunked H2D / compute / D2H on two streams)"}
 
 
@@ -892,6 +1058,73 @@ def _incremental_spef(d, keep, f0, caps, batch, graph, names, baseline=None):
     return out
 
 
+def reference_gpu_rc(ns_np, seed, budget_s=8.0):
+    """The reference's own sm_100a RC kernels (rct_bfs_and_compute_cuda,
+    ot/cuda/rct.cu:361-397, oracle/_ref) on the first nets of the headline
+    workload: the whole call as the Timer makes it (host arrays, its own
+    allocations and copies) and its kernels alone (CUDA events around each
+    of its launches), next to our fused pass on the very same nets.  The
+    sample is sized from a timed 300-net prefix to about `budget_s` of the
+    reference's time; its chains stay in (its BFS costs depth x edges per
+    net, which is the point of the comparison).  Its BFS slots and pid are
+    compared with ours."""
+    import torch
+    import opentimer_b200 as otg
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    if not O.ref_available():
+        return {"error": "oracle/_ref not built"}
+    ns64 = ns_np.astype(np.int64)
+
+    def sample(k):
+        f, slew, _ = O.synth_forest(seed, ns64[:k + 1], threads=os.cpu_count())
+        return f
+    O.ref_rct_gpu(sample(50))  # context, module load
+    t = {}
+    f = sample(300)
+    O.ref_rct_gpu(f, timing=t)
+    k = int(min(len(ns64) - 1, max(300, 300 * budget_s / max(t["call_s"], 1e-3))))
+    k = min(k, 200_000)
+    f = sample(k)
+    t = {}
+    e_ref, n2b_ref, pid_ref, _ = O.ref_rct_gpu(f, timing=t)
+    V = f.total_nodes
+    # ours on the same nets, device-resident inputs
+    d = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()  # noqa: E731
+    b = otg.RcBatch(d(f.nodes_start), d(f.edges.copy()), d(f.roots), d(f.res), d(f.cap),
+                    max_net_nodes=int(np.diff(ns64[:k + 1]).max()))
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    ts = []
+    for r in range(6):
+        torch.cuda.synchronize()
+        ev[0].record()
+        b.run()
+        ev[1].record()
+        torch.cuda.synchronize()
+        if r:
+            ts.append(ev[0].elapsed_time(ev[1]))
+    b.check()
+    ours_ms = float(np.median(ts))
+    nonroot = np.ones(V, bool)
+    nonroot[f.nodes_start[:-1]] = False  # the reference leaves a net's root pid unwritten
+    same = bool(np.array_equal(b.node2bfs.cpu().numpy(), n2b_ref) and
+                np.array_equal(b.pid.cpu().numpy()[nonroot], pid_ref[nonroot]))
+    del b
+    torch.cuda.empty_cache()
+    return {"sample": f"first {k} of the {len(ns64) - 1} headline nets ({V} nodes)",
+            "reference_call_nodes_per_s": V / t["call_s"],
+            "reference_call_ms": 1e3 * t["call_s"],
+            "reference_kernel_ms": t["kernel_ms"], "reference_kernel_launches": t["launches"],
+            "reference_kernel_nodes_per_s": V / (t["kernel_ms"] / 1e3),
+            "ours_pass_ms": ours_ms, "ours_nodes_per_s": V / (ours_ms / 1e3),
+            "kernel_speedup": t["kernel_ms"] / ours_ms,
+            "bfs_slots_match_reference_gpu": same,
+            "what": "reference: rct_bfs_and_compute_cuda built -arch sm_100a (oracle/_ref); "
+                    "kernel time = CUDA events around its compute_net_bfs, prepare_res_cap "
+                    "and compute_net_timing launches; ours: otg_rc_timing on device inputs, "
+                    "median of 5"}
+
+
 def cpu_baseline(g, ns_np):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     threads = os.cpu_count() or 1
@@ -919,6 +1152,7 @@ def main():
                     help="RC-pass tuning to apply instead of autotuning (JSON or a JSON file)")
     ap.add_argument("--no-spef", action="store_true")
     ap.add_argument("--no-full-update", action="store_true")
+    ap.add_argument("--no-parity", action="store_true")
     # smaller cases (profiling); the defaults are the benchmark workload
     ap.add_argument("--nets", type=int, default=NUM_NETS)
     ap.add_argument("--min-nodes", type=int, default=2)

@@ -186,15 +186,17 @@ void otg_release_host_context(void);
  * allocator owns all device memory, a loop that cannot afford cudaMalloc's
  * device-wide synchronization).  This entry point has no counterpart in the
  * reference.  Its workspace is a 16 MiB array compiled into libotg, held on
- * every GPU that loads the library until the process exits; the caller
- * passes only inputs and outputs (device pointers, as for otg_rc_timing).
- * The first call on a device looks up that array's address, so make it
- * before any stream capture.  Calls share the array: calls that overlap on
- * the GPU race, so serialize them.  Blocks until `stream` finishes and
- * returns the device-side status.  Limit: at most 524,284 nets per call and
- * no net beyond the shared-memory classes (about 4,700 nodes on a B200);
- * larger batches return OTG_ERR_WORKSPACE without launching.  Allocates
- * nothing.
+ * every GPU that loads it until the process exits; the caller passes only
+ * inputs and outputs (device pointers, as for otg_rc_timing).  The first
+ * call on a device loads the array (the CUDA runtime loads device code
+ * lazily) and looks up its address: make it before a pool allocator takes
+ * the device's memory and before any stream capture; a call with an empty
+ * forest does only that set-up.  Calls share the array: calls that overlap
+ * on the GPU race, so serialize them.  Blocks until `stream` finishes and
+ * returns the device-side status of the call.  Limit: at most 524,284 nets
+ * per call and no net beyond the shared-memory classes of the device's
+ * tuning (4,265 nodes on a B200 with the default tuning); larger batches
+ * return OTG_ERR_WORKSPACE without launching.  Allocates nothing.
  */
 otg_status otg_rc_timing_noalloc(const otg_rc_forest* forest, int32_t max_net_nodes,
                                  otg_stream_t stream);

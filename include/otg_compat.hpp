@@ -48,7 +48,8 @@ struct RctEdgeArrayCUDA {
 // Replaces rct_bfs_and_compute_cuda (ot/cuda/rct.cuh:45, ot/cuda/rct.cu:361-397).
 // Host arrays in, host arrays out (edges rewritten to parent->child,
 // node2bfs, pid, load/delay/ldelay/impulse in BFS order).  Errors are logged
-// to stderr and leave the outputs untouched (the reference asserts).
+// to stderr (the reference asserts); the copies back are queued before the
+// status is read, so after an error the output arrays hold undefined values.
 void rct_bfs_and_compute_cuda(RctEdgeArrayCUDA data_cpu);
 
 // Replaces the never-called rct_compute_cuda (ot/cuda/rct.cuh:44,

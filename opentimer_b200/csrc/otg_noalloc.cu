@@ -8,23 +8,29 @@
 // otg_rc_timing (otg_rc.cu) needs a workspace from its caller;
 // otg_rc_timing_noalloc runs the same pass with a workspace that is compiled
 // into this library instead: the fixed array below, 16 MiB of device memory
-// that every GPU which loads libotg holds until the process exits.
+// that every GPU which loads it holds until the process exits.
 //
 // How it behaves:
-//   * The first call on each device looks up the array's device address
-//     (cudaGetSymbolAddress) -- the array's name in host code only stands in
-//     for it.  Make that first call before any stream capture.
+//   * The CUDA runtime loads this file's device code, and with it the
+//     16 MiB array, lazily: on the first call on each device, which looks
+//     up the array's device address (cudaGetSymbolAddress -- the array's
+//     name in host code only stands in for it).  A host whose pool takes
+//     all device memory at start-up should make that first call before the
+//     pool does; a call with an empty forest (num_nets == 0) does only this
+//     set-up.  Make the first call before any stream capture, too.
 //   * Every call reuses the same array.  The call clears the parts that must
 //     start at zero (status word and work counters) before it launches, and
 //     everything else is written before it is read.  Two calls that overlap
 //     on the GPU (different streams, or different host threads) race on the
 //     array: serialize them.
-//   * The call synchronizes `stream` and returns the device-side status.
+//   * The call synchronizes `stream` and returns the device-side status of
+//     this call (an empty call returns OTG_OK without reading the array).
 //   * It never calls cudaMalloc, cudaFree or any other allocating routine.
 //   * Limit: the workspace of the batch must fit 16 MiB, i.e. at most
-//     524,284 nets per call, and every net small enough for the
-//     shared-memory classes (about 4,700 nodes on a B200); anything larger
-//     returns OTG_ERR_WORKSPACE before launching.
+//     524,284 nets per call, and every net within the shared-memory classes
+//     of the device's tuning (4,265 nodes on a B200 with the default
+//     tuning; otg_rc_set_tuning moves the bound); anything larger returns
+//     OTG_ERR_WORKSPACE before launching.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -76,6 +82,9 @@ extern "C" otg_status otg_rc_timing_noalloc(const otg_rc_forest* forest, int32_t
   void* ws = nullptr;
   st = scratch_address(&ws);
   if (st != OTG_OK) return st;
+  // An empty batch launches nothing and clears nothing: the status word may
+  // still hold an earlier call's error, so do not read it.
+  if (forest->num_nets == 0) return OTG_OK;
   st = otg::rc_launch(forest, max_net_nodes, ws, kNoAllocScratchBytes, (cudaStream_t)stream);
   if (st != OTG_OK) return st;
   return otg_rc_status(ws, stream, nullptr);

@@ -20,9 +20,9 @@
 //     bushy trees: a stable radix sort builds the adjacency, pointer
 //     jumping ranks the Euler tour, one scan over the tour yields parent,
 //     depth, DFS preorder and subtree sizes, a stable radix sort by depth
-//     yields the reference's BFS slots, and Elmore runs as two compensated
-//     (float-float) segmented scans up the preorder (subtree sums: load,
-//     ldelay) and two down the Euler tour (path sums: delay, beta).
+//     yields the reference's BFS slots, and Elmore runs as two exact int64
+//     fixed-point scans up the preorder (subtree sums: load, ldelay) and two
+//     down the Euler tour (path sums: delay, beta).
 //
 // BFS order is bit-exact with the reference: (distance asc, local id desc).
 #include <cuda_runtime.h>
@@ -337,9 +337,9 @@ namespace {
 //          order (the reference's (dist asc, id desc) rule)
 //   A8     topology outputs (node2bfs, pid, directed edges) and the
 //          parent resistance by preorder
-//   B      Elmore, one corner pair at a time: load and ldelay as
-//          compensated range sums over the preorder, delay and beta as
-//          compensated prefix sums over the signed tour.
+//   B      Elmore, one corner pair at a time: load and ldelay as exact
+//          int64 fixed-point range sums over the preorder, delay and beta
+//          as exact int64 fixed-point prefix sums over the signed tour.
 // =====================================================================
 
 template <class Ix> struct IxT;

@@ -62,6 +62,8 @@ def oracle_lib():
         lib.oracle_sink_slew.restype = None
         lib.oracle_levelize.argtypes = [I, P, P, P, P, I, P, P, P, P]
         lib.oracle_levelize.restype = I
+        lib.oracle_synth_rc_forest.argtypes = [ctypes.c_uint64, I, I, P, P, P, F, F, F, P, I]
+        lib.oracle_synth_rc_forest.restype = I
         _oracle = lib
     return _oracle
 
@@ -86,6 +88,10 @@ def ref_lib():
         lib.otref_spef_load.restype = I
         lib.otref_spef_fetch.argtypes = [P, P, P, F, F]
         lib.otref_spef_fetch.restype = None
+        lib.otref_launch_timing_begin.argtypes = []
+        lib.otref_launch_timing_begin.restype = None
+        lib.otref_launch_timing_end.argtypes = [ctypes.POINTER(ctypes.c_double)]
+        lib.otref_launch_timing_end.restype = I
         _ref = lib
     return _ref
 
@@ -192,6 +198,30 @@ def levelize(n, fanin_start, fanin, out_deg, frontier0):
     return order[:cnt], ends[:L + 1], level[:n]
 
 
+def synth_forest(seed, nodes_start, first_net=0, threads=None):
+    """Nets first_net.. of the seeded batched-Elmore workload, generated on
+    the host (synth_host.c: bit-identical to the product library's
+    generator).  nodes_start holds the slice's node offsets (any base).
+    Returns (Forest, driver_slew [N][4], sink_count [N])."""
+    ns = np.ascontiguousarray(nodes_start, np.int64)
+    ns = (ns - ns[0]).astype(np.int32)
+    N = len(ns) - 1
+    V = int(ns[-1])
+    e = np.zeros((max(V - N, 1), 2), np.int32)
+    roots = np.zeros(max(N, 1), np.int32)
+    res = np.zeros(max(V - N, 1), np.float32)
+    cap = np.zeros((max(V, 1), 4), np.float32)
+    slew = np.zeros((max(N, 1), 4), np.float32)
+    cnt = np.zeros(max(N, 1), np.int32)
+    st = oracle_lib().oracle_synth_rc_forest(seed, int(first_net), N, ns, e.reshape(-1), roots,
+                                             res, cap.reshape(-1), slew.reshape(-1), cnt,
+                                             int(threads or os.cpu_count() or 1))
+    if st != 0:
+        raise MemoryError("oracle_synth_rc_forest")
+    f = Forest(ns, e[:V - N], roots[:N], res[:V - N], cap[:V])
+    return f, slew[:N], cnt[:N]
+
+
 def to_local(f, node2bfs, arr_bfs):
     """Permute a [V][4] BFS-ordered array to local-id order."""
     b = np.repeat(f.nodes_start[:-1], np.diff(f.nodes_start))
@@ -211,9 +241,13 @@ def ref_rct_update(f, num_threads=0, readback=True):
     return st, outs
 
 
-def ref_rct_gpu(f):
+def ref_rct_gpu(f, timing=None):
     """The reference's own GPU path (needs a GPU).  Returns directed edges,
-    node2bfs, pid and the four outputs in BFS order."""
+    node2bfs, pid and the four outputs in BFS order.  With a dict `timing`,
+    its kernels' device time is recorded into it (CUDA events around each
+    of its launches: "kernel_ms", "launches") next to the whole call's wall
+    time ("call_s", host arrays in and out, as the Timer calls it)."""
+    import time
     lib = ref_lib()
     V = f.total_nodes
     ns = f.nodes_start.copy()
@@ -224,9 +258,17 @@ def ref_rct_gpu(f):
     node2bfs = np.zeros(V, np.int32)
     pid = np.zeros(V, np.int32)
     outs = [np.zeros((V, 4), np.float32) for _ in range(4)]
+    if timing is not None:
+        lib.otref_launch_timing_begin()
+    t0 = time.perf_counter()
     lib.otref_rct_bfs_and_compute_cuda(f.num_nets, V, ns, e.reshape(-1), roots, res,
                                        cap.reshape(-1), node2bfs, pid,
                                        *[o.reshape(-1) for o in outs])
+    if timing is not None:
+        timing["call_s"] = time.perf_counter() - t0
+        ms = ctypes.c_double()
+        timing["launches"] = lib.otref_launch_timing_end(ctypes.byref(ms))
+        timing["kernel_ms"] = ms.value
     return e, node2bfs, pid, outs
 
 

@@ -121,3 +121,28 @@ def test_levelize_oracle_definition():
     for k in range(1, len(ends) - 1):
         seg = order[ends[k]:ends[k + 1]]
         assert np.all(np.diff(seg) > 0)
+
+
+def test_host_generator_matches_product_generator():
+    """The reference arm of bench.py builds its inputs with the oracle's host
+    generator (so the product library is not loaded there); it must give
+    the very nets the product library's generator gives, including a slice
+    that starts in the middle of the workload."""
+    import opentimer_b200 as otg
+    ns = otg.workloads.net_sizes(77, 400, 2, 600)
+    g = otg.synth_forest_host(77, ns)
+    f, slew, cnt = O.synth_forest(77, ns, threads=3)
+    assert np.array_equal(f.edges, g["edges"])
+    assert np.array_equal(f.roots, g["roots"])
+    assert np.array_equal(f.res.view(np.int32), g["res"].view(np.int32))
+    assert np.array_equal(f.cap.view(np.int32), g["cap"].view(np.int32))
+    assert np.array_equal(slew.view(np.int32), g["driver_slew"].view(np.int32))
+    assert np.array_equal(cnt, g["sink_count"])
+    # nets 150..299 as a slice of their own
+    k0, k1 = 150, 300
+    fs, slew_s, cnt_s = O.synth_forest(77, ns[k0:k1 + 1], first_net=k0, threads=2)
+    v0, v1 = int(ns[k0]), int(ns[k1])
+    assert np.array_equal(fs.edges, g["edges"][v0 - k0:v1 - k1])
+    assert np.array_equal(fs.roots, g["roots"][k0:k1])
+    assert np.array_equal(fs.cap.view(np.int32), g["cap"][v0:v1].view(np.int32))
+    assert np.array_equal(slew_s.view(np.int32), g["driver_slew"][k0:k1].view(np.int32))
