@@ -419,6 +419,35 @@ otg_status otg_propagate(const otg_prop_graph* graph, const otg_prop_rc* rc,
                          otg_stream_t stream);
 otg_status otg_prop_status(const void* workspace, otg_stream_t stream);
 
+/*
+ * ---- Incremental gate resizing (the device side of Timer::repower_gate,
+ * ot/timer/timer.cpp:57-118, with Pin::_remap_cellpin, ot/timer/pin.cpp:
+ * 382-399) ---------------------------------------------------------------
+ * A resize remaps a gate's pins to another cell: each input pin's node in
+ * its net's RC tree gets the new cell pin's capacitance (ground cap plus
+ * pin cap, written whole), and each cell arc of the gate gets the new
+ * cell's timing record for its split.  otg_apply_updates writes both kinds
+ * of update in one launch (device arrays): cap_row[u] is a flat node index
+ * (nodes_start[net] + local id) into nodes_cap [V][4], cap_val[u] its [4]
+ * values; arc_slot[k] = arc * 2 + split into arc_timing [A][2], arc_rec[k]
+ * the record.  Out-of-range indices are skipped and set *status (device,
+ * caller-zeroed) to OTG_ERR_INVALID.  The caller re-times the nets of the
+ * changed nodes (otg_rc_timing_subset) and propagates (otg_propagate), as
+ * update_timing does for the dirty nets and the affected cone
+ * (ot/timer/timer.cpp:888-923, 1245-1334).  Asynchronous.
+ */
+otg_status otg_apply_updates(int32_t num_cap, const int32_t* cap_row, const float* cap_val,
+                             float* nodes_cap, int32_t total_nodes, int32_t num_arc,
+                             const int32_t* arc_slot, const int32_t* arc_rec,
+                             int32_t* arc_timing, int32_t num_arcs, int32_t* status,
+                             otg_stream_t stream);
+/* Worst (minimum) finite slack per corner over slack [P][4] (device) into
+ * out4 [4] (device; NaN where no pin has one), the per-corner worst slack
+ * of Timer::report_wns over the propagated pins.  scratch4: 4 uint32 of
+ * device scratch.  Asynchronous. */
+otg_status otg_worst_slack(const float* slack, int32_t num_pins, uint32_t* scratch4,
+                           float* out4, otg_stream_t stream);
+
 /* Human-readable name of a status code. */
 const char* otg_status_string(otg_status s);
 

@@ -30,7 +30,8 @@ C_SYMBOLS = [
     "otg_rc_get_tuning", "otg_rc_set_tuning", "otg_rc_autotune",
     "otg_spef_read", "otg_spef_sizes", "otg_spef_fill", "otg_spef_pins", "otg_spef_net_name",
     "otg_spef_pin_name", "otg_spef_free", "otg_prop_workspace_size", "otg_propagate",
-    "otg_prop_status", "otg_rc_move_nets", "otg_spef_names",
+    "otg_prop_status", "otg_rc_move_nets", "otg_spef_names", "otg_apply_updates",
+    "otg_worst_slack",
 ]
 # The reference-compatible C++ entry points (include/otg_compat.hpp), by
 # their Itanium-mangled names.
@@ -137,6 +138,8 @@ def lib():
         L.otg_propagate.argtypes = [P, P, P, P, P, P, P, P, P, S, P]
         L.otg_prop_status.argtypes = [P, P]
         L.otg_rc_move_nets.argtypes = [P, P, P, I32, P, P]
+        L.otg_apply_updates.argtypes = [I32, P, P, P, I32, I32, P, P, P, I32, P, P]
+        L.otg_worst_slack.argtypes = [P, I32, P, P, P]
         L.otg_spef_names.argtypes = [P, P, PS]
         L.otg_spef_free.restype = None
         for name in ["otg_rc_workspace_size", "otg_rc_timing", "otg_rc_status", "otg_rc_timing_subset",
@@ -149,7 +152,8 @@ def lib():
                      "otg_rc_get_tuning", "otg_rc_set_tuning", "otg_rc_autotune",
                      "otg_spef_read", "otg_spef_sizes", "otg_spef_fill", "otg_spef_pins",
                      "otg_prop_workspace_size", "otg_propagate", "otg_prop_status",
-                     "otg_rc_move_nets", "otg_spef_names"]:
+                     "otg_rc_move_nets", "otg_spef_names", "otg_apply_updates",
+                     "otg_worst_slack"]:
             getattr(L, name).restype = ctypes.c_int
         _lib = L
     return _lib

@@ -521,9 +521,10 @@ __global__ void __launch_bounds__(256) prop_kernel(G G_, const int* order, const
 
 size_t align256p(size_t x) { return (x + 255) & ~(size_t)255; }
 
-// Tables up to this many floats are staged in shared memory (32 KB per
-// CTA keeps five 256-thread CTAs per SM).
-constexpr int kLutSmemFloats = 8192;
+// Tables up to this many floats are staged in shared memory (40 KB per
+// CTA keeps five 256-thread CTAs per SM; a library with three drive
+// strengths of its combinational cells takes about 33 KB).
+constexpr int kLutSmemFloats = 10240;
 
 struct PropDev {
   int sms = 0;

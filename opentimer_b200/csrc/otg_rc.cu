@@ -30,6 +30,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 
@@ -1009,11 +1010,18 @@ __device__ void rc_net_block(const RcArgs& a, int net, char* ws, int n, int* sh,
   }
 }
 
-template <int T, int K, class Ix, bool SMEM>
+#include "otg_rc_tile.cuh"
+
+// Shared-memory bytes of a block-class net of n nodes with T threads.
+__host__ __device__ inline uint32_t rc_smem_bytes(int n, int T, int K, bool tile) {
+  return tile ? rc_tile_layout(n, T).total : rc_layout(n, T, K, 2).total;
+}
+
+template <int T, int K, class Ix, bool SMEM, bool TILE = false>
 __global__ void __launch_bounds__(T) rc_block_kernel(RcJob job, const int* list, const int* count,
                                                      int* work, char* gws, size_t ws_stride) {
   extern __shared__ __align__(16) char dsm[];
-  __shared__ int sh[64];
+  __shared__ int sh[96];
   __shared__ long long shl[4 * (T / 32) + 4];
   __shared__ int s_item[2];
   __shared__ RcArgs s_args;  // the current net's forest
@@ -1035,7 +1043,8 @@ __global__ void __launch_bounds__(T) rc_block_kernel(RcJob job, const int* list,
     __syncthreads();
     if (item >= cnt) break;
     const int n = s_args.nodes_start[net + 1] - s_args.nodes_start[net];
-    rc_net_block<T, K, Ix>(s_args, net, ws, n, sh, shl);
+    if constexpr (TILE) rc_net_tile<T>(s_args, net, ws, n, sh, shl);
+    else rc_net_block<T, K, Ix>(s_args, net, ws, n, sh, shl);
     __syncthreads();
   }
 }
@@ -1122,13 +1131,22 @@ int shape_index(int T, int K) {
 
 }  // namespace
 
+// The block path in use: the edge-wise tile kernel (otg_rc_tile.cuh), or
+// with OTG_RC_LEGACY set in the environment the earlier adjacency-list
+// kernel (kept for comparison while the tile kernel is measured).
+bool rc_use_tile() {
+  static const bool tile = std::getenv("OTG_RC_LEGACY") == nullptr;
+  return tile;
+}
+
 // Largest n whose 16-bit block layout fits the shared-memory budget.
 int rc_smem_nmax(int T, int K, int smem_budget) {
+  const bool tile = rc_use_tile();
   int lo = 33, hi = 32767;
-  if (rc_layout(lo, T, K, 2).total > (uint32_t)smem_budget) return 32;
+  if (rc_smem_bytes(lo, T, K, tile) > (uint32_t)smem_budget) return 32;
   while (lo < hi) {
     const int mid = (lo + hi + 1) / 2;
-    if (rc_layout(mid, T, K, 2).total <= (uint32_t)smem_budget) lo = mid; else hi = mid - 1;
+    if (rc_smem_bytes(mid, T, K, tile) <= (uint32_t)smem_budget) lo = mid; else hi = mid - 1;
   }
   return lo;
 }
@@ -1165,7 +1183,7 @@ bool tune_ok(const RcTune& t, int smem_budget) {
   for (int c = 0; c < t.num; ++c) {
     if (t.shape[c] < 0 || t.shape[c] >= kNumShapes || t.nmax[c] <= prev) return false;
     const Shape sh = kShapeSet[t.shape[c]];
-    if (rc_layout(t.nmax[c], sh.T, sh.K, 2).total > (uint32_t)smem_budget) return false;
+    if (rc_smem_bytes(t.nmax[c], sh.T, sh.K, rc_use_tile()) > (uint32_t)smem_budget) return false;
     prev = t.nmax[c];
   }
   return true;
@@ -1244,8 +1262,9 @@ namespace {
 template <int T, int K>
 cudaError_t launch_smem_class(const RcJob& job, const int* list, int* count, int* work, int nmax,
                               int sms, cudaStream_t stream) {
-  auto kern = rc_block_kernel<T, K, uint16_t, true>;
-  const size_t smem = rc_layout(nmax, T, K, 2).total;
+  const bool tile = rc_use_tile();
+  auto kern = tile ? rc_block_kernel<T, K, uint16_t, true, true> : rc_block_kernel<T, K, uint16_t, true>;
+  const size_t smem = rc_smem_bytes(nmax, T, K, tile);
   // The attribute is always set to the same (largest) value, so threads
   // launching with different nmax never lower it under one another.
   cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,

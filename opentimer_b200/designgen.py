@@ -172,7 +172,58 @@ def liberty(seed, scale, name, cells=None):
     text += '  pin(Q) {\n    direction : output;\n    function : "IQ";\n'
     text += _arc(rng, "CK", "non_unate", scale, kind="rising_edge",
                  groups=ff["timings"]["Q"]) + "  }\n}\n"
+    text += _drive_variants(seed, scale, caps, cells)
     text += "}\n"
+    return text
+
+
+# Drive strengths of the combinational cells: input capacitance grows with
+# the drive, the load-dependent part of the delay and transition tables
+# shrinks with it, and the intrinsic part grows a little.  The variants are
+# drawn from their own stream (the X1 cells above are unchanged by them).
+DRIVES = (2, 4)
+
+
+def _drive_arc(rng, related, sense, scale, drive, groups):
+    a, b, c = rng.uniform(0.01, 0.03), rng.uniform(0.1, 0.3), rng.uniform(0.002, 0.006)
+    ta, tb, tc = rng.uniform(0.005, 0.02), rng.uniform(0.05, 0.2), rng.uniform(0.004, 0.01)
+    k = 1.0 + 0.15 * np.log2(drive)  # intrinsic delay of the bigger stack
+    g = {"related": related, "sense": sense, "type": None}
+    out = "    timing() {\n"
+    out += f'      related_pin : "{related}";\n'
+    out += f"      timing_sense : {sense};\n"
+    out += _lut("cell_rise", "tbl7x7", _table(rng, a * k, b, c / drive, scale), g)
+    out += _lut("cell_fall", "tbl7x7", _table(rng, a * 0.9 * k, b, c * 1.1 / drive, scale), g)
+    out += _lut("rise_transition", "tbl7x7", _table(rng, ta * k, tb, tc / drive, scale), g)
+    out += _lut("fall_transition", "tbl7x7", _table(rng, ta * 1.1 * k, tb, tc / drive, scale), g)
+    out += "    }\n"
+    groups.append(g)
+    return out
+
+
+def _drive_variants(seed, scale, caps, cells):
+    rng = np.random.default_rng(seed + 7919)
+    text = ""
+    for drive in DRIVES:
+        cg = drive ** 0.8  # input capacitance factor
+        name = f"INV_X{drive}"
+        c = cells[name] = {"caps": {"A": f32(caps[0] * cg)}, "timings": {"ZN": []}}
+        text += f"cell({name}) {{\n  area : {drive};\n" + _pin_in("A", c["caps"]["A"]) + "  }\n"
+        text += '  pin(ZN) {\n    direction : output;\n    function : "(!A)";\n'
+        text += _drive_arc(rng, "A", "negative_unate", scale, drive, c["timings"]["ZN"])
+        text += "  }\n}\n"
+        for k, (base, fn) in enumerate([("NAND2", "(!(A1 A2))"), ("NOR2", "(!(A1+A2))")]):
+            name = f"{base}_X{drive}"
+            c = cells[name] = {"caps": {"A1": f32(caps[1 + 2 * k] * cg),
+                                        "A2": f32(caps[2 + 2 * k] * cg)},
+                               "timings": {"ZN": []}}
+            text += f"cell({name}) {{\n  area : {2 * drive};\n"
+            text += _pin_in("A1", c["caps"]["A1"]) + "  }\n" + _pin_in("A2", c["caps"]["A2"])
+            text += "  }\n"
+            text += f'  pin(ZN) {{\n    direction : output;\n    function : "{fn}";\n'
+            text += _drive_arc(rng, "A1", "negative_unate", scale, drive, c["timings"]["ZN"])
+            text += _drive_arc(rng, "A2", "negative_unate", scale, drive, c["timings"]["ZN"])
+            text += "  }\n}\n"
     return text
 
 
@@ -435,9 +486,10 @@ def timing_graph(design):
             rec[key] = len(timing) - 1
         return rec[key]
 
+    gate_arcs = [[] for _ in design["gates"]]  # per gate: (arc, split, cell pin, group)
     for el, lib in ((0, "early"), (1, "late")):
         cells = design["libs"][lib]
-        for inst, cell, conn in design["gates"]:
+        for gi, (inst, cell, conn) in enumerate(design["gates"]):
             for cp, groups in cells[cell]["timings"].items():
                 for k, g in enumerate(groups):
                     t = g["type"] or ""
@@ -445,6 +497,7 @@ def timing_graph(design):
                         continue
                     tm = [-1, -1]
                     tm[el] = record(lib, cell, cp, k, g)
+                    gate_arcs[gi].append((len(arc_from), el, cp, k))
                     arc_from.append(index[f"{inst}:{g['related']}"])
                     arc_to.append(index[f"{inst}:{cp}"])
                     arc_kind.append(1)
@@ -452,6 +505,17 @@ def timing_graph(design):
                     arc_net_name.append(None)
                     if t in _MIN_CONSTRAINT or t in _MAX_CONSTRAINT:
                         tests.append(len(arc_from) - 1)
+    # the timing records of every cell of the libraries, used or not, so that
+    # a resize (Timer::repower_gate) only re-points a gate's arcs
+    for el, lib in ((0, "early"), (1, "late")):
+        cells = design["libs"][lib]
+        for cell in sorted(cells):
+            for cp, groups in cells[cell]["timings"].items():
+                for k, g in enumerate(groups):
+                    t = g["type"] or ""
+                    if (el == 0 and t in _MAX_CONSTRAINT) or (el == 1 and t in _MIN_CONSTRAINT):
+                        continue
+                    record(lib, cell, cp, k, g)
     P = len(pins)
     nan4 = lambda: np.full((P, 4), np.nan, np.float32)  # noqa: E731
     pi_at, pi_slew, po_rat = nan4(), nan4(), nan4()
@@ -468,7 +532,10 @@ def timing_graph(design):
               "po_rat": po_rat, "timing": np.array(timing, np.int32),
               "lut_meta": np.array(lut_meta, np.int32),
               "lut_data": np.concatenate(lut_data).astype(np.float32),
-              "period": design["period"], "arc_net_name": arc_net_name}
+              "period": design["period"], "arc_net_name": arc_net_name,
+              "gate_arcs": gate_arcs,
+              "records": {(cell, el, cp, k): r for (lib, cell, cp, k), r in rec.items()
+                          for el in ((0,) if lib == "early" else (1,))}}
     return arrays, pins, [pin_net.get(i) for i in range(P)]
 
 

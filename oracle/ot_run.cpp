@@ -1,7 +1,8 @@
 // ot_run.cpp -- runs the reference OpenTimer Timer on a design directory and
 // dumps its results.  TEST INFRASTRUCTURE ONLY (the full-update parity check).
 //
-//   ot_run <dir> cpu|cuda <out.txt> [graph.txt]
+//   ot_run <dir> cpu|cuda <out.txt> [graph.txt] [change=<spef>]...
+//          [repower=<ops> [dump_every=<k>]]
 //
 // graph.txt (optional) is the Timer's timing graph, for the GPU propagation
 // check: pins, arcs (net arcs with their net, cell arcs with one timing
@@ -9,6 +10,12 @@
 // LUT ids), LUTs (variable order, indices, values), timing tests, the clock
 // period and the primary-input/-output assertions, all by pin index.
 // <dir> holds early.lib, late.lib, design.v, design.spef, design.timing.
+// repower=<ops>: after the first update, a sequence of gate resizes, one
+// "<gate> <cell>" per line, steps separated by lines holding "=": each step
+// is Timer::repower_gate for its lines, then update_timing (the dirty nets
+// and the affected cone only, as the Timer does).  The seconds of every
+// step go to stdout ("repower_step_s <k> <s>"); with dump_every=<k> the
+// pins (P lines) after every k-th step go to <out>.step<k>.
 // The same Timer sources are linked twice (oracle/Makefile): with the
 // reference's own CUDA module (ot_run_ref) and with libotg in its place
 // (ot_run_otg), so "cuda" runs either the reference kernels or ours behind
@@ -27,6 +34,7 @@
 // lines (ot/timer/net.cpp:388-410).
 #include <chrono>
 #include <cmath>
+#include <cstdlib>
 #include <cstdio>
 #include <string>
 #include <unordered_map>
@@ -159,9 +167,13 @@ int main(int argc, char** argv) {
   // update (read_spef + update_timing, as the TAU15 ops files do)
   const char* graph_path = nullptr;
   std::vector<std::string> changes;
+  std::string repower;
+  int dump_every = 0;
   for (int a = 4; a < argc; ++a) {
     const std::string s = argv[a];
     if (s.rfind("change=", 0) == 0) changes.push_back(s.substr(7));
+    else if (s.rfind("repower=", 0) == 0) repower = s.substr(8);
+    else if (s.rfind("dump_every=", 0) == 0) dump_every = std::atoi(s.c_str() + 11);
     else graph_path = argv[a];
   }
   ot::Timer timer;
@@ -185,10 +197,70 @@ int main(int argc, char** argv) {
     std::printf("incremental_update_timing_s %.6f\n", s2);
   }
 
-  FILE* f = std::fopen(argv[3], "w");
-  if (!f) return 3;
   const ot::Split splits[2] = {ot::MIN, ot::MAX};
   const ot::Tran trans[2] = {ot::RISE, ot::FALL};
+  auto dump_pins = [&](FILE* f) {
+    for (auto& [name, pin] : timer._pins) {
+      (void)pin;
+      std::fprintf(f, "P %s", name.c_str());
+      for (auto el : splits)
+        for (auto rf : trans) put(f, timer.report_at(name, el, rf));
+      for (auto el : splits)
+        for (auto rf : trans) put(f, timer.report_slew(name, el, rf));
+      for (auto el : splits)
+        for (auto rf : trans) put(f, timer.report_rat(name, el, rf));
+      for (auto el : splits)
+        for (auto rf : trans) put(f, timer.report_slack(name, el, rf));
+      std::fprintf(f, "\n");
+    }
+  };
+  if (!repower.empty()) {
+    FILE* ops = std::fopen(repower.c_str(), "r");
+    if (!ops) return 4;
+    char gate[256], cell[256];
+    int step = 0, pending = 0;
+    double total = 0.0;
+    auto finish_step = [&]() {
+      const auto t1 = std::chrono::steady_clock::now();
+      timer.update_timing();
+      const double s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t1).count();
+      total += s;
+      ++step;
+      std::printf("repower_step_s %d %.6f %d\n", step, s, pending);
+      if (dump_every > 0 && step % dump_every == 0) {
+        const std::string path = std::string(argv[3]) + ".step" + std::to_string(step);
+        if (FILE* g = std::fopen(path.c_str(), "w")) {
+          dump_pins(g);
+          std::fclose(g);
+        }
+      }
+      pending = 0;
+    };
+    char line[600];
+    const auto t0r = std::chrono::steady_clock::now();
+    double repower_calls = 0.0;
+    while (std::fgets(line, sizeof(line), ops)) {
+      if (line[0] == '=') {
+        finish_step();
+        continue;
+      }
+      if (std::sscanf(line, "%255s %255s", gate, cell) == 2) {
+        const auto t1 = std::chrono::steady_clock::now();
+        timer.repower_gate(gate, cell);
+        repower_calls += std::chrono::duration<double>(std::chrono::steady_clock::now() - t1).count();
+        ++pending;
+      }
+    }
+    if (pending) finish_step();
+    std::fclose(ops);
+    const double wall =
+        std::chrono::duration<double>(std::chrono::steady_clock::now() - t0r).count();
+    std::printf("repower_total_s %.6f %d %.6f %.6f\n", total + repower_calls, step, wall,
+                repower_calls);
+  }
+
+  FILE* f = std::fopen(argv[3], "w");
+  if (!f) return 3;
   for (auto& [name, pin] : timer._pins) {
     std::fprintf(f, "P %s", name.c_str());
     for (auto el : splits)

@@ -46,3 +46,32 @@ def bfs_local(nodes_start, node2bfs, arr_bfs):
 
 def levels_as_sets(order, ends):
     return [sorted(order[ends[k]:ends[k + 1]].tolist()) for k in range(len(ends) - 1)]
+
+
+def pin_err(got, ref, rtol=1e-5, atol=1e-5):
+    """Worst |got - ref| / (rtol s + atol) over pins and quantities, for
+    {pin: [4,4]} (at, slew, rat, slack by corner): s = |ref| for at and slew
+    and max(|ref|, |ref at|) for rat and slack (their rounding follows the
+    arrival time).  inf where one side has a value the other lacks."""
+    worst = 0.0
+    for name, r in ref.items():
+        g = got[name]
+        m = ~np.isnan(r)
+        if not np.array_equal(m, ~np.isnan(g)):
+            return float("inf")
+        scale = np.abs(r)
+        scale[2:] = np.maximum(scale[2:], np.nan_to_num(np.abs(r[0])))
+        if m.any():
+            worst = max(worst, float(np.max(np.abs(g[m] - r[m]) / (rtol * scale[m] + atol))))
+    return worst
+
+
+def read_ref_pins(path):
+    """P lines of oracle/ot_run.cpp's output: {pin: [4,4]}."""
+    pins = {}
+    with open(path) as f:
+        for line in f:
+            if line.startswith("P "):
+                t = line.split()
+                pins[t[1]] = np.array([float(x) for x in t[2:]], np.float64).reshape(4, 4)
+    return pins
