@@ -43,7 +43,7 @@ FU_GATES = 50_000
 FU_REPS = 5
 FU_CHANGE = 0.01  # fraction of the nets a change SPEF re-draws
 # incremental sizing loop
-INC_GATES, INC_ITERS, INC_FRAC, INC_PLAIN_ITERS, INC_CHECK = 200_000, 1000, 0.005, 20, True
+INC_GATES, INC_ITERS, INC_FRAC, INC_PLAIN_ITERS, INC_REF_ITERS = 200_000, 1000, 0.005, 100, 3
 # serving
 SRV_DESIGNS, SRV_PINS_LO, SRV_PINS_HI = 16, 10_000, 2_000_000
 SRV_RATES, SRV_SECONDS, SRV_SLOTS, SRV_SAT_REQ = (2_000, 10_000, 50_000), 0.5, 4, 20_000
@@ -409,7 +409,8 @@ def run_ours(args, world, rank, local):
         del batch, g
         torch.cuda.empty_cache()
     if world == 1 and not args.no_incremental:
-        line["incremental"] = _section(run_incremental)
+        line["incremental"] = _section(run_incremental,
+                                       baseline=line.get("cpu_baseline") if rank == 0 else None)
     if world == 1 and not args.no_serving:
         line["serving"] = _section(run_serving)
     # reference runs of the other sections belong to the CPU-baseline leg
@@ -688,64 +689,125 @@ def _state_matches(srv, did, design):
                for k in ["node2bfs", "load", "delay", "ldelay", "impulse", "sink_slew"])
 
 
-def run_incremental():
-    """Batched incremental sizing loop: a 200k-gate design (RC trees 2..512
-    nodes), 1000 iterations each resizing a random 0.5% of the gates.  The
-    batched path applies an iteration as one request (one graph replay
-    re-times all its dirty nets); the plain path applies every gate resize
-    by itself (its own launches and a synchronization)."""
-    from opentimer_b200 import workloads
-    from opentimer_b200.serve import TimingServer, synth_design
-    ns = workloads.net_sizes(SEED + 3, INC_GATES, 2, 512)
-    design = synth_design(SEED + 3, ns)
-    gm = workloads.gate_map(SEED + 4, design)
-    k = int(round(INC_FRAC * INC_GATES))
-    zeros = np.zeros(INC_ITERS, np.int64)
-    tr = workloads.request_trace(SEED + 5, [gm], INC_ITERS, None, lo=k, hi=k,
-                                 design_of=zeros, arrival=zeros)
-    plain_tr = workloads.per_gate_trace(tr, [gm], num_req=INC_PLAIN_ITERS)
+def run_incremental(baseline=None):
+    """Batched incremental sizing loop: a 200k-gate design of the small-design
+    kind (designgen: 4 cell functions in drive strengths X1/X2/X4, 7x7 NLDM
+    tables, 5% flops; RC trees of 2..512 nodes, log-uniform), 1000
+    iterations, each resizing a random 0.5% of the gates to another drive
+    strength (Timer::repower_gate) and re-timing: otg_apply_updates (new pin
+    caps, new cell-arc records), otg_rc_timing_subset over the dirty nets,
+    otg_propagate over the timing graph, otg_worst_slack.
+      batched: all iterations' launch sets queued back to back from device
+               arrays prepared before the timed region, no host round trip
+               between iterations;
+      plain:   the same launch set per iteration, with a synchronization and
+               a read of the worst slack after each.
+    Both are checked against each other iteration by iteration (worst
+    slacks bit-identical).  With `baseline` (the CPU-baseline leg's dict),
+    the reference Timer (oracle/_ref/ot_run_ref, CPU path, all host
+    threads) runs the first INC_REF_ITERS iterations, repower_gate per gate
+    and update_timing per iteration, timed; every pin after them is checked
+    against ours."""
+    import subprocess
+    import tempfile
     import torch
-    tuning, tune_s = autotune_on(SEED + 12, int(2.5 * k), 2, 512, torch.device("cuda", 0))
-    with TimingServer(slots=2, max_requests=4, max_updates=4 * k) as srv:
-        did, fp = srv.add_design(design)
-        warm_p = workloads.per_gate_trace(tr, [gm], num_req=2)
-        warm_b = workloads.request_trace(SEED + 6, [gm], 3, None, lo=k, hi=k,
-                                         design_of=zeros[:3], arrival=zeros[:3])
-        srv.replay(warm_p, plain=True)
-        srv.replay(warm_b)
-        lat_b, span_b = srv.replay(tr)
-        lat_p, span_p = srv.replay(plain_tr, plain=True)
-        # what the server holds now: the warm-ups, the batched iterations and
-        # the plain iterations, in that order
-        ok = True
-        if INC_CHECK:
-            check_design = {kk: v.copy() for kk, v in design.items()}
-            workloads.apply_trace(check_design, warm_p)
-            workloads.apply_trace(check_design, warm_b)
-            workloads.apply_trace(check_design, tr)
-            workloads.apply_trace(check_design, plain_tr)
-            ok = _state_matches(srv, did, check_design)
-    resizes_b = INC_ITERS * k
-    resizes_p = INC_PLAIN_ITERS * k
-    ups_b = resizes_b / span_b
-    ups_p = resizes_p / span_p
-    return {
-        "workload": f"{INC_GATES} gates/nets (RC 2..512 nodes, {int(ns[-1])} nodes), "
-                    f"{INC_ITERS} iterations x {k} gate resizes (0.5%)",
-        "batched": {"gate_resizes_per_s": ups_b, "ms_per_iteration": 1e3 * span_b / INC_ITERS,
-                    "path": "one request per iteration: graph replay (apply, fused RC pass "
-                            "over the dirty nets, results)"},
-        "plain": {"gate_resizes_per_s": ups_p, "ms_per_iteration": 1e3 * span_p / INC_PLAIN_ITERS,
-                  "iterations_timed": INC_PLAIN_ITERS,
-                  "path": "one otg_server_update_sync per gate resize (direct launches + sync)"},
-        "speedup": ups_b / ups_p,
-        "dirty_nets_per_iteration": float(2.5 * k),
-        "state_bit_exact_vs_full_pass": bool(ok),
-        "tuning": tuning,
-        "autotune": f"otg_rc_autotune on {int(2.5 * k)} nets of 2..512 nodes (a batch's "
-                    f"size), {tune_s:.1f} s, before the server captured its graphs",
-        "design_footprint_bytes": int(fp),
-    }
+    from opentimer_b200 import designgen
+    from opentimer_b200.sizing import SizingDesign, resize_trace, write_ops
+    out = {}
+    with tempfile.TemporaryDirectory() as d:
+        keep = {}
+        t0 = time.perf_counter()
+        info = designgen.write_design(d, seed=SEED + 3, gates=INC_GATES, keep=keep,
+                                      rc_nodes=(2, 512), rc_log=True)
+        t_gen = time.perf_counter() - t0
+        k = int(round(INC_FRAC * INC_GATES))
+        steps = resize_trace(keep, SEED + 5, INC_ITERS, k)
+        t0 = time.perf_counter()
+        sd = SizingDesign(d, keep)
+        sd.check()
+        t_load = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        prep = sd.prepare(steps)
+        t_prep = time.perf_counter() - t0
+        dirty = np.diff(prep["o_net"])
+        V = sd.batch.total_nodes
+        # warm-up: an empty batch through the whole launch set
+        for _ in range(3):
+            sd.resize([])
+        sd.check()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        torch.cuda.synchronize()
+        ev[0].record()
+        sd.run_prepared(prep)
+        ev[1].record()
+        torch.cuda.synchronize()
+        ms_b = ev[0].elapsed_time(ev[1]) / INC_ITERS
+        sd.check()
+        wns_b = prep["wns"].cpu().numpy()
+        del sd, prep
+        torch.cuda.empty_cache()
+        # plain path on a fresh copy of the design, the first iterations
+        n_p = min(INC_PLAIN_ITERS, INC_ITERS)
+        sp = SizingDesign(d, keep)
+        prep_p = sp.prepare(steps[:n_p])
+        for _ in range(3):
+            sp.resize([])
+        sp.check()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        wns_p = sp.run_prepared(prep_p, sync_each=True)
+        ms_p = 1e3 * (time.perf_counter() - t0) / n_p
+        same = bool(np.array_equal(np.array(wns_p), wns_b[:n_p]))
+        out = {"workload": f"{info['gates']} gates, {info['nets']} nets, {V} RC nodes "
+                           f"(trees 2..512, log-uniform), {sp.P} pins, {sp.graph.A} arcs, "
+                           f"{sp.graph.num_levels} levels; {INC_ITERS} iterations x {k} gate "
+                           f"resizes (0.5%)",
+               "batched": {"ms_per_iteration": ms_b, "gate_resizes_per_s": k / (ms_b / 1e3),
+                           "path": "iterations queued back to back: otg_apply_updates, "
+                                   "otg_rc_timing_subset (dirty nets), otg_propagate, "
+                                   "otg_worst_slack; device-resident design"},
+               "plain": {"ms_per_iteration": ms_p, "gate_resizes_per_s": k / (ms_p / 1e3),
+                         "iterations_timed": n_p,
+                         "path": "the same launch set per iteration, then a synchronization "
+                                 "and a read of its worst slack"},
+               "speedup_vs_plain": ms_p / ms_b,
+               "dirty_nets_per_iteration": float(dirty.mean()),
+               "worst_slack_batched_equals_plain": same,
+               "worst_slack_first_last": [wns_b[0].tolist(), wns_b[-1].tolist()],
+               "design_write_s": t_gen, "design_load_s": t_load, "prepare_s": t_prep}
+        exe = os.path.join(ROOT, "oracle", "_ref", "ot_run_ref")
+        if baseline is not None and os.path.exists(exe):
+            # ours after INC_REF_ITERS iterations: the plain copy, rebuilt
+            del sp, prep_p
+            torch.cuda.empty_cache()
+            sr = SizingDesign(d, keep)
+            for st in steps[:INC_REF_ITERS]:
+                sr.resize(st)
+            ours = sr.pins()
+            ops = os.path.join(d, "ops.txt")
+            write_ops(ops, steps[:INC_REF_ITERS])
+            ref_out = os.path.join(d, "ref.txt")
+            p = subprocess.run([exe, d, "cpu", ref_out, f"repower={ops}",
+                                f"dump_every={INC_REF_ITERS}"], capture_output=True, text=True,
+                               timeout=900)
+            secs = [float(x.split()[2]) for x in p.stdout.splitlines()
+                    if x.startswith("repower_step_s")]
+            if p.returncode == 0 and secs:
+                sys.path.insert(0, os.path.join(ROOT, "tests"))
+                from helpers import pin_err, read_ref_pins
+                ref = read_ref_pins(f"{ref_out}.step{INC_REF_ITERS}")
+                baseline["incremental"] = {
+                    "value": 1e3 * float(np.mean(secs)), "unit": "ms per iteration",
+                    "cores": os.cpu_count(), "kind": "reference",
+                    "sample": f"the first {INC_REF_ITERS} of the {INC_ITERS} iterations",
+                    "what": "the reference Timer (oracle/_ref): repower_gate per resized gate, "
+                            "then update_timing (dirty nets and the affected cone), CPU path",
+                    "ours_pins_err_over_tol": pin_err(ours, ref)}
+                out["reference_ms_per_iteration"] = 1e3 * float(np.mean(secs))
+                out["speedup_vs_reference"] = 1e3 * float(np.mean(secs)) / ms_b
+                out["pins_err_over_tol_vs_reference"] = baseline["incremental"][
+                    "ours_pins_err_over_tol"]
+    return out
 
 
 def run_serving():
@@ -1137,6 +1199,7 @@ def cpu_baseline(g, ns_np):
 
 
 def main():
+    global INC_GATES, INC_ITERS
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
@@ -1153,11 +1216,15 @@ def main():
     ap.add_argument("--no-spef", action="store_true")
     ap.add_argument("--no-full-update", action="store_true")
     ap.add_argument("--no-parity", action="store_true")
+    ap.add_argument("--inc-gates", type=int, default=INC_GATES,
+                    help="gates of the incremental sizing loop's design (smaller: quick runs)")
+    ap.add_argument("--inc-iters", type=int, default=INC_ITERS)
     # smaller cases (profiling); the defaults are the benchmark workload
     ap.add_argument("--nets", type=int, default=NUM_NETS)
     ap.add_argument("--min-nodes", type=int, default=2)
     ap.add_argument("--max-nodes", type=int, default=4096)
     args = ap.parse_args()
+    INC_GATES, INC_ITERS = args.inc_gates, args.inc_iters
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
     world, rank, local = dist_setup(args)
     try:

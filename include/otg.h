@@ -346,6 +346,22 @@ const char* otg_spef_pin_name(const otg_spef* spef, int32_t net, int32_t k);
  * NUL-terminated, into buf (*bytes: its size in, the size used out).  With
  * buf NULL it only sets *bytes.  OTG_ERR_WORKSPACE if buf is too small. */
 otg_status otg_spef_names(const otg_spef* spef, char* buf, size_t* bytes);
+/* The other direction (no single reference counterpart; the inverse of
+ * spef::Spef::read for the subset above): writes nets as SPEF text with
+ * units ns / fF / ohm.  names_blob holds '\0'-terminated names, name k at
+ * name_off[k] (name_off has one more entry than there are names).  Net i:
+ * name net_name[i]; pins pins_start[i]..pins_start[i+1]-1 (name pin_name[p],
+ * pin_port[p] 1 for a port, the first pin is the driver); nodes
+ * nodes_start[i]..nodes_start[i+1]-1 in *CAP order, node_code >= 0 the
+ * net's pin of that index, < 0 the internal node "<net>:<-code>", ground
+ * cap node_cap; edges [V-N][2] (node indices within the net) and res in
+ * *RES order.  threads <= 0: all hardware threads. */
+otg_status otg_spef_write(const char* path, int32_t num_nets, const char* names_blob,
+                          const int64_t* name_off, const int32_t* net_name,
+                          const int32_t* pins_start, const int32_t* pin_name,
+                          const int8_t* pin_port, const int32_t* nodes_start,
+                          const int32_t* node_code, const float* node_cap, const int32_t* edges,
+                          const float* res, int32_t threads);
 void otg_spef_free(otg_spef* spef);
 
 /*
@@ -441,6 +457,30 @@ otg_status otg_apply_updates(int32_t num_cap, const int32_t* cap_row, const floa
                              const int32_t* arc_slot, const int32_t* arc_rec,
                              int32_t* arc_timing, int32_t num_arcs, int32_t* status,
                              otg_stream_t stream);
+/*
+ * otg_fanin_csr -- the levelization input of a timing update, built on the
+ * device (replaces Timer::_build_prop_tasks_cuda steps 1-2,
+ * ot/timer/timer.cpp:996-1061, which build it on the host with taskflow
+ * and a serial prefix sum).  An arc counts when arc_skip[a] is 0 (a loop
+ * breaker otherwise; arc_skip may be NULL) and both its pins are
+ * candidates (pin_cand[p] != 0; NULL: every pin).  Outputs (device):
+ * fanin_start[n+1] and fanin[]: per pin its counted fanin arcs in arc
+ * order, as source pins (or, with fanin_as_arcs, as arc indices);
+ * out_deg[n]: counted fanout arcs; frontier0: the candidates of
+ * cand_order[num_cands] without counted fanout, in that order (the first
+ * frontier); counts[0] = their number, counts[1] = the arcs counted.  These
+ * are exactly otg_levelize's inputs.  Asynchronous; otg_fanin_csr_status
+ * synchronizes and reports OTG_ERR_INVALID for an out-of-range pin. */
+otg_status otg_fanin_csr_workspace_size(int32_t num_pins, int32_t num_arcs, int32_t num_cands,
+                                        size_t* bytes);
+otg_status otg_fanin_csr(int32_t num_pins, int32_t num_arcs, const int32_t* from,
+                         const int32_t* to, const uint8_t* arc_skip, const uint8_t* pin_cand,
+                         int32_t num_cands, const int32_t* cand_order, int32_t fanin_as_arcs,
+                         int32_t* fanin_start, int32_t* fanin, int32_t* out_deg,
+                         int32_t* frontier0, int32_t* counts, void* workspace,
+                         size_t workspace_bytes, otg_stream_t stream);
+otg_status otg_fanin_csr_status(const void* workspace, otg_stream_t stream);
+
 /* Worst (minimum) finite slack per corner over slack [P][4] (device) into
  * out4 [4] (device; NaN where no pin has one), the per-corner worst slack
  * of Timer::report_wns over the propagated pins.  scratch4: 4 uint32 of

@@ -17,7 +17,7 @@ import numpy as np
 from . import workloads  # noqa: F401
 from ._lib import C_SYMBOLS, CXX_SYMBOLS, OtgError, RcForest, check, lib  # noqa: F401
 
-__all__ = ["RcBatch", "rc_timing", "rc_timing_host", "levelize", "levelize_host",
+__all__ = ["RcBatch", "rc_timing", "rc_timing_host", "levelize", "levelize_host", "fanin_csr",
            "synth_forest", "kernel_launches", "get_tuning", "set_tuning", "autotune",
            "OtgError", "lib"]
 
@@ -301,6 +301,39 @@ class LevelizeBatch:
         L, emitted = [int(x) for x in self.counts.tolist()]
         return (self.order[:emitted].cpu().numpy(), self.level_ends[:L + 1].cpu().numpy(),
                 self.level[:self.n].cpu().numpy())
+
+
+def fanin_csr(num_pins, arc_from, arc_to, arc_skip=None, pin_cand=None, cand_order=None,
+              as_arcs=False, stream=None):
+    """The levelization input built on the device (otg_fanin_csr): arcs
+    (CUDA int32 tensors from, to; optional uint8 arc_skip) over num_pins
+    pins, candidates pin_cand (uint8, optional) listed in cand_order (int32;
+    default: all pins in index order).  Returns CUDA tensors (fanin_start,
+    fanin, out_deg, frontier0) -- fanin as source pins, or arc indices with
+    as_arcs -- ready for levelize / LevelizeBatch."""
+    import torch
+    dev = arc_from.device
+    n, A = int(num_pins), int(arc_from.numel())
+    if cand_order is None:
+        cand_order = torch.arange(n, dtype=torch.int32, device=dev)
+    C = int(cand_order.numel())
+    ws = ctypes.c_size_t()
+    check("otg_fanin_csr_workspace_size",
+          lib().otg_fanin_csr_workspace_size(n, A, C, ctypes.byref(ws)))
+    work = torch.empty(max(ws.value, 256), dtype=torch.uint8, device=dev)
+    start = torch.empty(n + 1, dtype=torch.int32, device=dev)
+    fanin = torch.empty(max(A, 1), dtype=torch.int32, device=dev)
+    out_deg = torch.empty(max(n, 1), dtype=torch.int32, device=dev)
+    front = torch.empty(max(C, 1), dtype=torch.int32, device=dev)
+    counts = torch.zeros(2, dtype=torch.int32, device=dev)
+    s = _stream(stream)
+    check("otg_fanin_csr", lib().otg_fanin_csr(
+        n, A, _ptr(arc_from), _ptr(arc_to), _ptr(arc_skip), _ptr(pin_cand), C, _ptr(cand_order),
+        1 if as_arcs else 0, _ptr(start), _ptr(fanin), _ptr(out_deg), _ptr(front),
+        _ptr(counts), _ptr(work), work.numel(), s))
+    check("otg_fanin_csr_status", lib().otg_fanin_csr_status(_ptr(work), s))
+    first, E = [int(x) for x in counts.tolist()]
+    return start, fanin[:E], out_deg[:n], front[:first]
 
 
 def levelize(fanin_start, fanin, out_deg, frontier0):

@@ -302,39 +302,76 @@ def verilog(glist, ins, outs):
                                       for i, s in enumerate(outs)]
 
 
-def spef(rng, nets):
-    """nets: {name: (driver_pin, driver_is_port, [(sink_pin, sink_is_port)])}"""
-    out = ['*SPEF "IEEE 1481-1998"', '*DESIGN "top"', '*DATE "0"', '*VENDOR "otg"',
-           '*PROGRAM "opentimer_b200 designgen"', '*VERSION "0"', '*DESIGN_FLOW "NETLIST_TYPE_VERILOG"',
-           "*DIVIDER /", "*DELIMITER :", "*BUS_DELIMITER [ ]", "*T_UNIT 1 NS", "*C_UNIT 1 FF",
-           "*R_UNIT 1 OHM", "*L_UNIT 1 HENRY", ""]
-    for name in sorted(nets):
+def spef(path, rng, nets, rc_nodes=(2, 16), rc_log=False):
+    """Writes the SPEF of `nets` ({name: (driver_pin, driver_is_port,
+    [(sink_pin, sink_is_port)])}) to `path`: per net (sorted by name) an RC
+    tree of its pins plus internal nodes <net>:<k>, rc_nodes[0]..rc_nodes[1]
+    nodes (uniform, or log-uniform with rc_log) but never fewer than its
+    pins, a random recursive tree rooted at the driver, R ~ U(0.5, 20) ohm,
+    ground C ~ U(0.1, 3) fF, RES lines shuffled with random orientation.
+    The random draws are made here; the text is formatted by
+    otg_spef_write (the library's SPEF writer)."""
+    import ctypes
+    from . import lib
+    names = sorted(nets)
+    name_id, blob = {}, []
+
+    def nid(x):
+        k = name_id.get(x)
+        if k is None:
+            k = name_id[x] = len(blob)
+            blob.append(x)
+        return k
+    lo, hi = rc_nodes
+    net_name, pins_start, pin_name, pin_port = [], [0], [], []
+    nodes_start, codes, caps, edges, res = [0], [], [], [], []
+    for name in names:
         drv, drv_port, sinks = nets[name]
-        pins = [drv] + [s for s, _ in sinks]
-        n = max(len(pins), int(rng.integers(2, 17)))
-        internal = [f"{name}:{i + 1}" for i in range(n - len(pins))]
-        order = [drv] + list(rng.permutation(pins[1:] + internal))
-        caps = rng.uniform(0.1, 3.0, n)
-        edges = [(order[int(rng.integers(0, i))], order[i]) for i in range(1, n)]
-        res = rng.uniform(0.5, 20.0, n - 1)
-        perm = rng.permutation(n - 1)
-        out.append(f"*D_NET {name} {caps.sum():.4f}")
-        out.append("*CONN")
-        out.append(f"*P {drv} I" if drv_port else f"*I {drv} O")
-        for s, is_port in sinks:
-            out.append(f"*P {s} O" if is_port else f"*I {s} I")
-        out.append("*CAP")
-        for i, (node, c) in enumerate(zip(order, caps)):
-            out.append(f"{i + 1} {node} {c:.4f}")
-        out.append("*RES")
-        for i, j in enumerate(perm):
-            a, b = edges[j]
-            if rng.random() < 0.5:
-                a, b = b, a
-            out.append(f"{i + 1} {a} {b} {res[j]:.4f}")
-        out.append("*END")
-        out.append("")
-    return "\n".join(out) + "\n"
+        net_name.append(nid(name))
+        pin_name.append(nid(drv))
+        pin_port.append(1 if drv_port else 0)
+        for sp, is_port in sinks:
+            pin_name.append(nid(sp))
+            pin_port.append(1 if is_port else 0)
+        npins = 1 + len(sinks)
+        pins_start.append(len(pin_name))
+        size = (int(np.exp(rng.uniform(np.log(lo), np.log(hi + 1)))) if rc_log
+                else int(rng.integers(lo, hi + 1)))
+        n = max(npins, min(size, hi) if rc_log else size)
+        # node order: the driver first, then pins and internal nodes shuffled;
+        # code >= 0 is a pin of the net, -k its internal node <net>:<k>
+        rest = np.concatenate([np.arange(1, npins), -np.arange(1, n - npins + 1)])
+        code = np.concatenate([[0], rng.permutation(rest)]).astype(np.int32)
+        codes.append(code)
+        caps.append(rng.uniform(0.1, 3.0, n))
+        if n > 1:
+            par = rng.integers(0, np.arange(1, n))  # random recursive tree
+            r = rng.uniform(0.5, 20.0, n - 1)
+            perm = rng.permutation(n - 1)
+            flip = rng.random(n - 1) < 0.5
+            a, b = par[perm], np.arange(1, n)[perm]
+            edges.append(np.stack([np.where(flip, b, a), np.where(flip, a, b)], 1))
+            res.append(r[perm])
+        nodes_start.append(nodes_start[-1] + n)
+    enc = [x.encode() + b"\0" for x in blob]
+    off = np.zeros(len(enc) + 1, np.int64)
+    np.cumsum([len(x) for x in enc], out=off[1:])
+    buf = b"".join(enc)
+    arr = lambda x, dt: np.ascontiguousarray(np.asarray(x, dt))  # noqa: E731
+    net_name, pins_start = arr(net_name, np.int32), arr(pins_start, np.int32)
+    pin_name, pin_port = arr(pin_name, np.int32), arr(pin_port, np.int8)
+    nodes_start = arr(nodes_start, np.int32)
+    codes = arr(np.concatenate(codes) if codes else np.zeros(0), np.int32)
+    caps = arr(np.concatenate(caps) if caps else np.zeros(0), np.float32)
+    edges = arr(np.concatenate(edges) if edges else np.zeros((0, 2)), np.int32)
+    res = arr(np.concatenate(res) if res else np.zeros(0), np.float32)
+    P = lambda x: x.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
+    L = lib()
+    st = L.otg_spef_write(path.encode(), len(names), buf, P(off), P(net_name), P(pins_start),
+                          P(pin_name), P(pin_port), P(nodes_start), P(codes), P(caps), P(edges),
+                          P(res), 0)
+    if st != 0:
+        raise OSError(f"otg_spef_write({path}) failed: {st}")
 
 
 def change_spef(design, path, frac=0.01, seed=0):
@@ -347,14 +384,14 @@ def change_spef(design, path, frac=0.01, seed=0):
     k = max(1, int(round(frac * len(names))))
     chosen = sorted(rng.choice(len(names), size=k, replace=False).tolist())
     nets = {names[i]: design["nets"][names[i]] for i in chosen}
-    with open(path, "w") as f:
-        f.write(spef(rng, nets))
+    spef(path, rng, nets, **design.get("rc", {}))
     return [names[i] for i in chosen]
 
 
-def write_design(dirpath, seed=2024, gates=2000, keep=None):
+def write_design(dirpath, seed=2024, gates=2000, keep=None, rc_nodes=(2, 16), rc_log=False):
     """Writes the design files; returns a summary.  With `keep` (a dict), it
-    also receives the in-memory design for timing_graph/pin_caps."""
+    also receives the in-memory design for timing_graph/pin_caps.
+    rc_nodes / rc_log: the RC tree sizes of the nets (see spef)."""
     rng = np.random.default_rng(seed)
     os.makedirs(dirpath, exist_ok=True)
     libs = {"early": {}, "late": {}}
@@ -386,8 +423,7 @@ def write_design(dirpath, seed=2024, gates=2000, keep=None):
     # every driven net gets a tree, even one without sinks: the reference's
     # flat (CUDA) path expects SPEF data for every net (net.cpp:500-507)
     nets = {n: (drivers[n][0], drivers[n][1], sinks.get(n, [])) for n in drivers}
-    with open(os.path.join(dirpath, "design.spef"), "w") as f:
-        f.write(spef(rng, nets))
+    spef(os.path.join(dirpath, "design.spef"), rng, nets, rc_nodes, rc_log)
     period = 1.0
     assert_at, assert_slew, assert_rat, assert_load = {}, {}, {}, {}
     assert_at["clk"] = f32([0.0, 0.5, 0.0, 0.5])  # rise at 0, fall at half a period
@@ -415,7 +451,7 @@ def write_design(dirpath, seed=2024, gates=2000, keep=None):
         keep.update(libs=libs, gates=gates_all, ports_in=ins + ["clk"],
                     ports_out=[f"out{i}" for i in range(len(outs))], nets=nets,
                     at=assert_at, slew=assert_slew, rat=assert_rat, load=assert_load,
-                    period=period)
+                    period=period, rc={"rc_nodes": tuple(rc_nodes), "rc_log": rc_log})
     return {"gates": len(glist) + 2 * len(outs), "nets": len(nets)}
 
 
