@@ -14,7 +14,7 @@ from itertools import compress
 
 import numpy as np
 
-from . import LevelizeBatch, _ptr, _stream, check, lib
+from . import LevelizeBatch, _ptr, _stream, check, fanin_csr, lib
 
 NC = 4
 
@@ -60,20 +60,17 @@ class TimingGraph:
         P = int(a["num_pins"])
         A = len(a["arc_from"])
         self.P, self.A = P, A
-        fanin_start, fanin = _csr(a["arc_to"], P)
-        fanout_start, fanout = _csr(a["arc_from"], P)
-        test_arc = np.asarray(a["test_arc"], np.int32)
-        test_start, test_of_pin = _csr(np.asarray(a["arc_to"])[test_arc], P)
-        host = {
-            "arc_from": a["arc_from"], "arc_to": a["arc_to"], "arc_kind": a["arc_kind"],
-            "arc_timing": a["arc_timing"], "arc_net": a["arc_net"], "arc_node": a["arc_node"],
-            "fanin_start": fanin_start, "fanin": fanin, "fanout_start": fanout_start,
-            "fanout": fanout, "test_arc": test_arc, "test_start": test_start,
-            "test_of_pin": test_of_pin, "timing": a["timing"], "lut_meta": a["lut_meta"],
-        }
         t = lambda x, dt: torch.from_numpy(  # noqa: E731
             np.ascontiguousarray(x, dt).reshape(-1) if np.size(x) else np.zeros(1, dt)).to(device)
-        self.dev = {k: t(v, np.int32) for k, v in host.items()}
+        self.dev = {k: t(a[k], np.int32) for k in
+                    ("arc_from", "arc_to", "arc_kind", "arc_timing", "arc_net", "arc_node",
+                     "timing", "lut_meta")}
+        test_arc = np.asarray(a["test_arc"], np.int32)
+        self.dev["test_arc"] = t(test_arc, np.int32)
+        self.T = len(test_arc)
+        # the CSRs of the graph, built on the device (otg_fanin_csr): arcs into
+        # and out of every pin, tests at every constrained pin
+        self.build_csr()
         # what the host side of an incremental change reads
         self.arc_to = np.asarray(a["arc_to"], np.int32)
         self.net_arcs = net_arc_index(a["arc_kind"], a["arc_net"])
@@ -98,12 +95,9 @@ class TimingGraph:
             self.order, self.levelizer, self.num_levels = t(order, np.int32), None, None
             return
         # levels over the pin graph: a pin's level is its longest path to a pin
-        # without fanout (otg_levelize, the reference's frontier rule)
-        fin_src = np.asarray(a["arc_from"], np.int32)[fanin]
-        out_deg = np.diff(fanout_start).astype(np.int32)
-        frontier0 = np.nonzero(out_deg == 0)[0].astype(np.int32)
-        lb = LevelizeBatch(t(fanin_start, np.int32), t(fin_src, np.int32), t(out_deg, np.int32),
-                           t(frontier0, np.int32))
+        # without fanout (otg_levelize, the reference's frontier rule), on the
+        # levelization input built on the device
+        lb = LevelizeBatch(*self.levelize_input())
         lb.run()
         lb.check()
         self.levelizer = lb  # re-run after a topology change (otg_levelize)
@@ -115,17 +109,35 @@ class TimingGraph:
         if forward == "sources":
             # the same levelization over the reversed arcs: a pin after all of
             # its fanins, sources first
-            fo_dst = np.asarray(a["arc_to"], np.int32)[fanout]
-            in_deg = np.diff(fanin_start).astype(np.int32)
-            sources = np.nonzero(in_deg == 0)[0].astype(np.int32)
-            fl = LevelizeBatch(t(fanout_start, np.int32), t(fo_dst, np.int32), t(in_deg, np.int32),
-                               t(sources, np.int32))
+            fl = LevelizeBatch(*fanin_csr(P, self.dev["arc_to"][:A], self.dev["arc_from"][:A]))
             fl.run()
             fl.check()
             self.fwd_levelizer = fl  # re-run with levelizer after a topology change
             fwd, _, _ = fl.result()
             assert len(fwd) == P, "the timing graph has a cycle"
             self.fwd_order = t(fwd, np.int32)
+
+    def build_csr(self):
+        """Fanin and fanout arc lists of every pin and the tests constrained
+        at every pin, on the device (otg_fanin_csr, arc order within a pin)."""
+        import torch
+        P, A = self.P, self.A
+        frm, to = self.dev["arc_from"][:A], self.dev["arc_to"][:A]
+        self.dev["fanin_start"], fi, _, _ = fanin_csr(P, frm, to, as_arcs=True)
+        self.dev["fanout_start"], fo, _, _ = fanin_csr(P, to, frm, as_arcs=True)
+        ta = self.dev["test_arc"][:self.T]
+        keys = to[ta.long()] if self.T else torch.zeros(0, dtype=torch.int32, device=to.device)
+        self.dev["test_start"], tp, _, _ = fanin_csr(P, keys, keys, as_arcs=True)
+
+        def pad(x):
+            return x if x.numel() else torch.zeros(1, dtype=torch.int32, device=to.device)
+        self.dev["fanin"], self.dev["fanout"], self.dev["test_of_pin"] = pad(fi), pad(fo), pad(tp)
+
+    def levelize_input(self):
+        """otg_levelize's input for this graph, built on the device: per pin
+        its fanin source pins, fanout counts and the pins without fanout
+        (Timer::_build_prop_tasks_cuda steps 1-2)."""
+        return fanin_csr(self.P, self.dev["arc_from"][:self.A], self.dev["arc_to"][:self.A])
 
     def propagate(self, batch, stream=None):
         """Forward and backward propagation on the RC outputs of `batch`
