@@ -434,6 +434,17 @@ otg_status otg_propagate(const otg_prop_graph* graph, const otg_prop_rc* rc,
                          float* rat, float* slack, void* workspace, size_t workspace_bytes,
                          otg_stream_t stream);
 otg_status otg_prop_status(const void* workspace, otg_stream_t stream);
+/* The same over a graph that is the union of independent designs (no arc
+ * between two of them): pin_group [P] gives each pin its design, and only
+ * the pins whose group_active[design] is nonzero are propagated (and
+ * marked pending); every other pin keeps its values.  order / fwd_order
+ * cover all pins, as for otg_propagate (a levelization of the union).  An
+ * incremental update of some designs then re-times only those. */
+otg_status otg_propagate_groups(const otg_prop_graph* graph, const otg_prop_rc* rc,
+                                const int32_t* order, const int32_t* fwd_order,
+                                const int32_t* pin_group, const uint8_t* group_active,
+                                float* at, float* slew, float* rat, float* slack,
+                                void* workspace, size_t workspace_bytes, otg_stream_t stream);
 
 /*
  * ---- Incremental gate resizing (the device side of Timer::repower_gate,
@@ -487,6 +498,13 @@ otg_status otg_fanin_csr_status(const void* workspace, otg_stream_t stream);
  * device scratch.  Asynchronous. */
 otg_status otg_worst_slack(const float* slack, int32_t num_pins, uint32_t* scratch4,
                            float* out4, otg_stream_t stream);
+/* Per group (the pin_group / group_active of otg_propagate_groups): the
+ * worst finite slack per corner of the active groups' pins into
+ * out [num_groups][4] (NaN for inactive groups and groups without slack).
+ * scratch: 4 * num_groups uint32 of device scratch.  Asynchronous. */
+otg_status otg_worst_slack_groups(const float* slack, int32_t num_pins, const int32_t* pin_group,
+                                  const uint8_t* group_active, int32_t num_groups,
+                                  uint32_t* scratch, float* out, otg_stream_t stream);
 
 /* Human-readable name of a status code. */
 const char* otg_status_string(otg_status s);

@@ -32,7 +32,7 @@ C_SYMBOLS = [
     "otg_spef_pin_name", "otg_spef_free", "otg_prop_workspace_size", "otg_propagate",
     "otg_prop_status", "otg_rc_move_nets", "otg_spef_names", "otg_apply_updates",
     "otg_worst_slack", "otg_spef_write", "otg_fanin_csr_workspace_size", "otg_fanin_csr",
-    "otg_fanin_csr_status",
+    "otg_fanin_csr_status", "otg_propagate_groups", "otg_worst_slack_groups",
 ]
 # The reference-compatible C++ entry points (include/otg_compat.hpp), by
 # their Itanium-mangled names.
@@ -145,6 +145,8 @@ def lib():
         L.otg_fanin_csr_workspace_size.argtypes = [I32, I32, I32, PS]
         L.otg_fanin_csr.argtypes = [I32, I32, P, P, P, P, I32, P, I32, P, P, P, P, P, P, S, P]
         L.otg_fanin_csr_status.argtypes = [P, P]
+        L.otg_propagate_groups.argtypes = [P, P, P, P, P, P, P, P, P, P, P, S, P]
+        L.otg_worst_slack_groups.argtypes = [P, I32, P, P, I32, P, P, P]
         L.otg_spef_names.argtypes = [P, P, PS]
         L.otg_spef_free.restype = None
         for name in ["otg_rc_workspace_size", "otg_rc_timing", "otg_rc_status", "otg_rc_timing_subset",
@@ -159,7 +161,8 @@ def lib():
                      "otg_prop_workspace_size", "otg_propagate", "otg_prop_status",
                      "otg_rc_move_nets", "otg_spef_names", "otg_apply_updates",
                      "otg_worst_slack", "otg_spef_write", "otg_fanin_csr_workspace_size",
-                     "otg_fanin_csr", "otg_fanin_csr_status"]:
+                     "otg_fanin_csr", "otg_fanin_csr_status", "otg_propagate_groups",
+                     "otg_worst_slack_groups"]:
             getattr(L, name).restype = ctypes.c_int
         _lib = L
     return _lib

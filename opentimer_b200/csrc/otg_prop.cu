@@ -482,11 +482,19 @@ __device__ bool bprop_warp(const G& G_, int v, int lane, const float* at, float*
 }
 
 // Marks every arrival time and slew pending and clears the control block.
-__global__ void prop_init_kernel(float4* at, float4* slew, int num_pins, GridCtl* ctl) {
+// (pin_group: only the pins whose group is active, see otg_propagate_groups.)
+__device__ __forceinline__ bool pin_on(const int32_t* pin_group, const uint8_t* group_active,
+                                       int v) {
+  return !pin_group || group_active[__ldg(pin_group + v)];
+}
+
+__global__ void prop_init_kernel(float4* at, float4* slew, int num_pins, GridCtl* ctl,
+                                 const int32_t* pin_group, const uint8_t* group_active) {
   const int i0 = blockIdx.x * blockDim.x + threadIdx.x;
   if (i0 == 0) *ctl = GridCtl{0u, 0u, 0, 0};
   const float p = __uint_as_float(kPending);
   for (int i = i0; i < num_pins; i += gridDim.x * blockDim.x) {
+    if (!pin_on(pin_group, group_active, i)) continue;
     at[i] = make_float4(p, p, p, p);
     slew[i] = make_float4(p, p, p, p);
   }
@@ -498,7 +506,9 @@ __global__ void __launch_bounds__(256) prop_kernel(G G_, const int* order, const
                                                    int num_pins,
                                                    float* at, float* slew, float* rat,
                                                    float* slack, float* arc_delay,
-                                                   float* test_rat, GridCtl* ctl, int lut_smem) {
+                                                   float* test_rat, GridCtl* ctl, int lut_smem,
+                                                   const int32_t* pin_group,
+                                                   const uint8_t* group_active) {
   // the library's tables, staged on chip when the caller gave their size
   // and they fit (lut_smem floats)
   extern __shared__ float s_lut[];
@@ -511,12 +521,16 @@ __global__ void __launch_bounds__(256) prop_kernel(G G_, const int* order, const
   bool ok = true;
   for (int j = warp; ok && j < num_pins; j += W) {
     const int v = fwd_order ? __ldg(fwd_order + j) : __ldg(order + num_pins - 1 - j);
+    if (!pin_on(pin_group, group_active, v)) continue;
     ok = fprop_warp(G_, lutd, v, lane, at, slew, rat, arc_delay, test_rat, ctl);
   }
   // the barrier also lets every CTA leave together when a wait gave up
   if (!grid_barrier(ctl) || !ok) return;
-  for (int j = warp; ok && j < num_pins; j += W)
-    ok = bprop_warp(G_, __ldg(order + j), lane, at, rat, slack, arc_delay, test_rat, ctl);
+  for (int j = warp; ok && j < num_pins; j += W) {
+    const int v = __ldg(order + j);
+    if (!pin_on(pin_group, group_active, v)) continue;
+    ok = bprop_warp(G_, v, lane, at, rat, slack, arc_delay, test_rat, ctl);
+  }
 }
 
 size_t align256p(size_t x) { return (x + 255) & ~(size_t)255; }
@@ -545,10 +559,11 @@ otg_status otg_prop_workspace_size(int32_t num_pins, int32_t num_arcs, int32_t n
   return OTG_OK;
 }
 
-otg_status otg_propagate(const otg_prop_graph* g, const otg_prop_rc* rc, const int32_t* order,
-                         const int32_t* fwd_order, float* at, float* slew, float* rat,
-                         float* slack, void* workspace, size_t workspace_bytes,
-                         otg_stream_t stream) {
+static otg_status propagate_impl(const otg_prop_graph* g, const otg_prop_rc* rc,
+                                 const int32_t* order, const int32_t* fwd_order,
+                                 const int32_t* pin_group, const uint8_t* group_active, float* at,
+                                 float* slew, float* rat, float* slack, void* workspace,
+                                 size_t workspace_bytes, otg_stream_t stream) {
   if (!g || !rc || !order || !at || !slew || !rat || !slack || !workspace || g->num_pins < 0)
     return OTG_ERR_INVALID;
   // lut_meta rows and the per-pin [4] rows are read and written as 16-byte vectors
@@ -565,7 +580,7 @@ otg_status otg_propagate(const otg_prop_graph* g, const otg_prop_rc* rc, const i
   float* test_rat = (float*)(ws + 256 + otg::align256p(32 * (size_t)g->num_arcs));
   cudaStream_t st = (cudaStream_t)stream;
   otg::prop_init_kernel<<<std::max(1, std::min(1184, (P + 255) / 256)), 256, 0, st>>>(
-      (float4*)at, (float4*)slew, P, ctl);
+      (float4*)at, (float4*)slew, P, ctl, pin_group, group_active);
   otg::count_launch();
   if (cudaGetLastError() != cudaSuccess) return OTG_ERR_CUDA;
   if (P == 0) return OTG_OK;
@@ -588,8 +603,10 @@ otg_status otg_propagate(const otg_prop_graph* g, const otg_prop_rc* rc, const i
   const int grid = std::max(1, std::min(d.sms * std::max(occ, 1), (P + 7) / 8));
   otg::G G_{*g, *rc};
   int num_pins = P;
-  void* args[] = {&G_,       (void*)&order, (void*)&fwd_order, &num_pins, &at,  &slew,
-                  &rat,      &slack,        &arc_delay,        &test_rat, &ctl, &lut_smem};
+  void* args[] = {&G_,       (void*)&order, (void*)&fwd_order, &num_pins,
+                  &at,       &slew,         &rat,              &slack,
+                  &arc_delay, &test_rat,    &ctl,              &lut_smem,
+                  (void*)&pin_group, (void*)&group_active};
   const cudaError_t e = cudaLaunchCooperativeKernel(
       (const void*)otg::prop_kernel, dim3(grid), dim3(256), args, 4 * (size_t)lut_smem, st);
   otg::count_launch();
@@ -598,6 +615,24 @@ otg_status otg_propagate(const otg_prop_graph* g, const otg_prop_rc* rc, const i
     return OTG_ERR_CUDA;
   }
   return OTG_OK;
+}
+
+otg_status otg_propagate(const otg_prop_graph* g, const otg_prop_rc* rc, const int32_t* order,
+                         const int32_t* fwd_order, float* at, float* slew, float* rat,
+                         float* slack, void* workspace, size_t workspace_bytes,
+                         otg_stream_t stream) {
+  return propagate_impl(g, rc, order, fwd_order, nullptr, nullptr, at, slew, rat, slack,
+                        workspace, workspace_bytes, stream);
+}
+
+otg_status otg_propagate_groups(const otg_prop_graph* g, const otg_prop_rc* rc,
+                                const int32_t* order, const int32_t* fwd_order,
+                                const int32_t* pin_group, const uint8_t* group_active,
+                                float* at, float* slew, float* rat, float* slack,
+                                void* workspace, size_t workspace_bytes, otg_stream_t stream) {
+  if (!pin_group || !group_active) return OTG_ERR_INVALID;
+  return propagate_impl(g, rc, order, fwd_order, pin_group, group_active, at, slew, rat, slack,
+                        workspace, workspace_bytes, stream);
 }
 
 otg_status otg_prop_status(const void* workspace, otg_stream_t stream) {

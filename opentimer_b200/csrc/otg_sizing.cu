@@ -73,14 +73,57 @@ __global__ void worst_slack_kernel(const float4* __restrict__ slack, int P, unsi
   }
 }
 
-__global__ void worst_slack_init(unsigned* out) {
-  if (threadIdx.x < 4) out[threadIdx.x] = 0xFFFFFFFFu;
+__global__ void worst_slack_init(unsigned* out, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    out[i] = 0xFFFFFFFFu;
 }
 
-__global__ void worst_slack_finish(const unsigned* in, float* out) {
-  if (threadIdx.x < 4) {
-    const unsigned u = in[threadIdx.x];
-    out[threadIdx.x] = u == 0xFFFFFFFFu ? __uint_as_float(0x7FC00000u) : ord2f(u);
+__global__ void worst_slack_finish(const unsigned* in, float* out, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const unsigned u = in[i];
+    out[i] = u == 0xFFFFFFFFu ? __uint_as_float(0x7FC00000u) : ord2f(u);
+  }
+}
+
+// Per group: pins with an active group reduce into their group's row.
+// Pins of a group are mostly contiguous, so a warp reduces runs of equal
+// groups before it touches the result row.
+__global__ void worst_slack_groups_kernel(const float4* __restrict__ slack, int P,
+                                          const int32_t* __restrict__ pin_group,
+                                          const uint8_t* __restrict__ group_active,
+                                          unsigned* out) {
+  for (int p0 = (blockIdx.x * blockDim.x + threadIdx.x) & ~31; p0 < P;
+       p0 += gridDim.x * blockDim.x) {
+    const int p = p0 + (threadIdx.x & 31);
+    const int g = p < P ? pin_group[p] : -1;
+    const bool on = g >= 0 && group_active[g];
+    unsigned m[4] = {0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu};
+    if (on) {
+      const float4 s = slack[p];
+      const float v[4] = {s.x, s.y, s.z, s.w};
+#pragma unroll
+      for (int c = 0; c < 4; ++c)
+        if (isfinite(v[c])) m[c] = f2ord(v[c]);
+    }
+    const unsigned peers = __match_any_sync(0xFFFFFFFFu, on ? g : -1);
+    if (peers == 0xFFFFFFFFu) {  // the whole warp in one group (the common case)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) m[c] = __reduce_min_sync(0xFFFFFFFFu, m[c]);
+    } else {
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        unsigned x = m[c];
+        for (int k = 0; k < 32; ++k) {  // min over the lanes of the same group
+          const unsigned y = __shfl_sync(0xFFFFFFFFu, x, k);
+          if ((peers >> k) & 1u) x = min(x, y);
+        }
+        m[c] = x;
+      }
+    }
+    if (on && (__ffs(peers) - 1) == (threadIdx.x & 31))
+#pragma unroll
+      for (int c = 0; c < 4; ++c)
+        if (m[c] != 0xFFFFFFFFu) atomicMin(&out[4 * g + c], m[c]);
   }
 }
 
@@ -115,14 +158,37 @@ otg_status otg_worst_slack(const float* slack, int32_t num_pins, uint32_t* scrat
   if (!slack || num_pins < 0 || !scratch4 || !out4) return OTG_ERR_INVALID;
   if ((uintptr_t)slack & 15) return OTG_ERR_INVALID;
   cudaStream_t st = (cudaStream_t)stream;
-  otg::worst_slack_init<<<1, 32, 0, st>>>(scratch4);
+  otg::worst_slack_init<<<1, 32, 0, st>>>(scratch4, 4);
   otg::count_launch();
   if (num_pins > 0) {
     const int blocks = (num_pins + 255) / 256 < 296 ? (num_pins + 255) / 256 : 296;
     otg::worst_slack_kernel<<<blocks, 256, 0, st>>>((const float4*)slack, num_pins, scratch4);
     otg::count_launch();
   }
-  otg::worst_slack_finish<<<1, 32, 0, st>>>(scratch4, out4);
+  otg::worst_slack_finish<<<1, 32, 0, st>>>(scratch4, out4, 4);
+  otg::count_launch();
+  return cudaGetLastError() == cudaSuccess ? OTG_OK : OTG_ERR_CUDA;
+}
+
+otg_status otg_worst_slack_groups(const float* slack, int32_t num_pins, const int32_t* pin_group,
+                                  const uint8_t* group_active, int32_t num_groups,
+                                  uint32_t* scratch, float* out, otg_stream_t stream) {
+  if (!slack || num_pins < 0 || num_groups < 0 || !pin_group || !group_active || !scratch ||
+      !out)
+    return OTG_ERR_INVALID;
+  if ((uintptr_t)slack & 15) return OTG_ERR_INVALID;
+  cudaStream_t st = (cudaStream_t)stream;
+  const int n = 4 * num_groups;
+  const int gb = (n + 255) / 256 < 64 ? (n + 255) / 256 : 64;
+  otg::worst_slack_init<<<gb > 0 ? gb : 1, 256, 0, st>>>(scratch, n);
+  otg::count_launch();
+  if (num_pins > 0) {
+    const int blocks = (num_pins + 255) / 256 < 592 ? (num_pins + 255) / 256 : 592;
+    otg::worst_slack_groups_kernel<<<blocks, 256, 0, st>>>((const float4*)slack, num_pins,
+                                                           pin_group, group_active, scratch);
+    otg::count_launch();
+  }
+  otg::worst_slack_finish<<<gb > 0 ? gb : 1, 256, 0, st>>>(scratch, out, n);
   otg::count_launch();
   return cudaGetLastError() == cudaSuccess ? OTG_OK : OTG_ERR_CUDA;
 }

@@ -314,45 +314,54 @@ def spef(path, rng, nets, rc_nodes=(2, 16), rc_log=False):
     import ctypes
     from . import lib
     names = sorted(nets)
-    name_id, blob = {}, []
-
-    def nid(x):
-        k = name_id.get(x)
-        if k is None:
-            k = name_id[x] = len(blob)
-            blob.append(x)
-        return k
-    lo, hi = rc_nodes
-    net_name, pins_start, pin_name, pin_port = [], [0], [], []
-    nodes_start, codes, caps, edges, res = [0], [], [], [], []
-    for name in names:
-        drv, drv_port, sinks = nets[name]
-        net_name.append(nid(name))
-        pin_name.append(nid(drv))
+    N = len(names)
+    # names: the nets, then every net's pins (driver first); a pin belongs to
+    # one net, so every name is stored once
+    pins = [(nets[nm][0], nets[nm][1], nets[nm][2]) for nm in names]
+    npins = np.fromiter((1 + len(sk) for _, _, sk in pins), np.int64, N)
+    blob = list(names)
+    pin_port = []
+    for drv, drv_port, sinks in pins:
+        blob.append(drv)
         pin_port.append(1 if drv_port else 0)
         for sp, is_port in sinks:
-            pin_name.append(nid(sp))
+            blob.append(sp)
             pin_port.append(1 if is_port else 0)
-        npins = 1 + len(sinks)
-        pins_start.append(len(pin_name))
-        size = (int(np.exp(rng.uniform(np.log(lo), np.log(hi + 1)))) if rc_log
-                else int(rng.integers(lo, hi + 1)))
-        n = max(npins, min(size, hi) if rc_log else size)
-        # node order: the driver first, then pins and internal nodes shuffled;
-        # code >= 0 is a pin of the net, -k its internal node <net>:<k>
-        rest = np.concatenate([np.arange(1, npins), -np.arange(1, n - npins + 1)])
-        code = np.concatenate([[0], rng.permutation(rest)]).astype(np.int32)
-        codes.append(code)
-        caps.append(rng.uniform(0.1, 3.0, n))
-        if n > 1:
-            par = rng.integers(0, np.arange(1, n))  # random recursive tree
-            r = rng.uniform(0.5, 20.0, n - 1)
-            perm = rng.permutation(n - 1)
-            flip = rng.random(n - 1) < 0.5
-            a, b = par[perm], np.arange(1, n)[perm]
-            edges.append(np.stack([np.where(flip, b, a), np.where(flip, a, b)], 1))
-            res.append(r[perm])
-        nodes_start.append(nodes_start[-1] + n)
+    net_name = np.arange(N, dtype=np.int32)
+    pins_start = np.zeros(N + 1, np.int64)
+    np.cumsum(npins, out=pins_start[1:])
+    pin_name = (N + np.arange(int(pins_start[-1]))).astype(np.int32)
+    lo, hi = rc_nodes
+    if rc_log:
+        size = np.minimum(np.exp(rng.uniform(np.log(lo), np.log(hi + 1), N)).astype(np.int64), hi)
+    else:
+        size = rng.integers(lo, hi + 1, N)
+    n = np.maximum(npins, size)
+    nodes_start = np.zeros(N + 1, np.int64)
+    np.cumsum(n, out=nodes_start[1:])
+    V = int(nodes_start[-1])
+    net_of = np.repeat(np.arange(N), n)
+    local = np.arange(V) - nodes_start[:-1][net_of]
+    # node order: the driver first, then the other pins and the internal nodes
+    # <net>:<k> shuffled; code >= 0 is a pin of the net, -k internal node k
+    npn = npins[net_of]
+    code0 = np.where(local < npn, local, -(local - npn + 1))
+    key = np.where(local == 0, -1.0, rng.random(V))
+    order = np.lexsort((key, net_of))
+    codes = code0[order]
+    caps = rng.uniform(0.1, 3.0, V)
+    # random recursive tree over the positions: parent of position i in [0, i)
+    E = V - N
+    child = np.nonzero(local > 0)[0]
+    enet = net_of[child]
+    li = local[child]
+    par = (rng.random(E) * li).astype(np.int64)
+    r = rng.uniform(0.5, 20.0, E)
+    perm = np.lexsort((rng.random(E), enet))  # RES lines shuffled within each net
+    flip = rng.random(E) < 0.5
+    a, b = par[perm], li[perm]
+    edges = np.stack([np.where(flip, b, a), np.where(flip, a, b)], 1)
+    res = r[perm]
     enc = [x.encode() + b"\0" for x in blob]
     off = np.zeros(len(enc) + 1, np.int64)
     np.cumsum([len(x) for x in enc], out=off[1:])
@@ -361,13 +370,11 @@ def spef(path, rng, nets, rc_nodes=(2, 16), rc_log=False):
     net_name, pins_start = arr(net_name, np.int32), arr(pins_start, np.int32)
     pin_name, pin_port = arr(pin_name, np.int32), arr(pin_port, np.int8)
     nodes_start = arr(nodes_start, np.int32)
-    codes = arr(np.concatenate(codes) if codes else np.zeros(0), np.int32)
-    caps = arr(np.concatenate(caps) if caps else np.zeros(0), np.float32)
-    edges = arr(np.concatenate(edges) if edges else np.zeros((0, 2)), np.int32)
-    res = arr(np.concatenate(res) if res else np.zeros(0), np.float32)
+    codes, caps = arr(codes, np.int32), arr(caps, np.float32)
+    edges, res = arr(edges.reshape(-1, 2), np.int32), arr(res, np.float32)
     P = lambda x: x.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
     L = lib()
-    st = L.otg_spef_write(path.encode(), len(names), buf, P(off), P(net_name), P(pins_start),
+    st = L.otg_spef_write(path.encode(), N, buf, P(off), P(net_name), P(pins_start),
                           P(pin_name), P(pin_port), P(nodes_start), P(codes), P(caps), P(edges),
                           P(res), 0)
     if st != 0:
@@ -388,17 +395,21 @@ def change_spef(design, path, frac=0.01, seed=0):
     return [names[i] for i in chosen]
 
 
-def write_design(dirpath, seed=2024, gates=2000, keep=None, rc_nodes=(2, 16), rc_log=False):
+def write_design(dirpath, seed=2024, gates=2000, keep=None, rc_nodes=(2, 16), rc_log=False,
+                 lib_seed=None):
     """Writes the design files; returns a summary.  With `keep` (a dict), it
     also receives the in-memory design for timing_graph/pin_caps.
-    rc_nodes / rc_log: the RC tree sizes of the nets (see spef)."""
+    rc_nodes / rc_log: the RC tree sizes of the nets (see spef).  lib_seed:
+    the seed of the cell library (default: seed), so that several designs
+    can share one library."""
     rng = np.random.default_rng(seed)
     os.makedirs(dirpath, exist_ok=True)
     libs = {"early": {}, "late": {}}
+    ls = (seed if lib_seed is None else lib_seed) + 1
     with open(os.path.join(dirpath, "late.lib"), "w") as f:
-        f.write(liberty(seed + 1, 1.0, "late", libs["late"]))
+        f.write(liberty(ls, 1.0, "late", libs["late"]))
     with open(os.path.join(dirpath, "early.lib"), "w") as f:
-        f.write(liberty(seed + 1, 0.9, "early", libs["early"]))
+        f.write(liberty(ls, 0.9, "early", libs["early"]))
     glist, ins, outs = netlist(rng, gates)
     vtext, po_chain = verilog(glist, ins, outs)
     with open(os.path.join(dirpath, "design.v"), "w") as f:
