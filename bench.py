@@ -46,7 +46,8 @@ FU_CHANGE = 0.01  # fraction of the nets a change SPEF re-draws
 INC_GATES, INC_ITERS, INC_FRAC, INC_PLAIN_ITERS, INC_REF_ITERS = 200_000, 1000, 0.005, 100, 3
 # serving
 SRV_DESIGNS, SRV_PINS_LO, SRV_PINS_HI = 16, 10_000, 2_000_000
-SRV_RATES, SRV_SECONDS, SRV_SLOTS, SRV_SAT_REQ = (2_000, 10_000, 50_000), 0.5, 4, 20_000
+SRV_RATES, SRV_MAX_REQ, SRV_SAT_REQ, SRV_REF_REQ = (2_000, 10_000, 50_000), 2_000, 3_000, 12
+SRV_PINS_PER_GATE = 2.75  # designgen: pins per gate of a design
 
 
 def algorithmic_bytes(num_nets, total_nodes, num_sinks):
@@ -412,7 +413,8 @@ def run_ours(args, world, rank, local):
         line["incremental"] = _section(run_incremental,
                                        baseline=line.get("cpu_baseline") if rank == 0 else None)
     if world == 1 and not args.no_serving:
-        line["serving"] = _section(run_serving)
+        line["serving"] = _section(run_serving,
+                                   baseline=line.get("cpu_baseline") if rank == 0 else None)
     # reference runs of the other sections belong to the CPU-baseline leg
     base = line.get("cpu_baseline")
     if base is not None and lv:
@@ -677,18 +679,6 @@ def _pct(lat, q):
     return float(np.percentile(lat, q)) * 1e3 if len(lat) else None
 
 
-def _state_matches(srv, did, design):
-    """The server's state of a design equals a full pass over its updated
-    inputs (bit for bit)."""
-    import opentimer_b200 as otg
-    c = {k: v.copy() for k, v in design.items()}
-    ref = otg.rc_timing_host(c["nodes_start"], c["edges"], c["roots"], c["res"], c["cap"],
-                             c["sinks_start"], c["sink_nodes"], c["driver_slew"])
-    got = srv.read(did)
-    return all(np.array_equal(got[k], ref[k])
-               for k in ["node2bfs", "load", "delay", "ldelay", "impulse", "sink_slew"])
-
-
 def run_incremental(baseline=None):
     """Batched incremental sizing loop: a 200k-gate design of the small-design
     kind (designgen: 4 cell functions in drive strengths X1/X2/X4, 7x7 NLDM
@@ -810,61 +800,127 @@ def run_incremental(baseline=None):
     return out
 
 
-def run_serving():
-    """Served incremental timing: 16 device-resident designs of 10k..2M pins
-    (small-design generator: RC trees 2..16 nodes), Poisson request streams,
-    each request resizing 1..64 random gates of one design.  Batched server
-    vs the plain per-request path on the same trace."""
-    from opentimer_b200 import workloads
-    from opentimer_b200.serve import TimingServer, synth_design
+def _served_design(args):
+    """One served design, built in a worker process: its files in `d` and
+    its host side (gateserve.build_design); the gates and libraries the
+    request generator needs come back with it."""
+    d, seed, gates = args
+    sys.path.insert(0, ROOT)
+    from opentimer_b200 import designgen
+    from opentimer_b200.gateserve import build_design
+    keep = {}
+    designgen.write_design(d, seed=seed, gates=gates, keep=keep, lib_seed=SEED + 400)
+    out = build_design(d, keep)
+    light = {"gates": [(g, c, None) for g, c, _ in keep["gates"]], "libs": keep["libs"]}
+    return out, light
+
+
+def run_serving(baseline=None):
+    """Served incremental timing: SRV_DESIGNS device-resident designs of the
+    small-design kind (one shared cell library), pins log-uniform in
+    SRV_PINS_LO..SRV_PINS_HI, held as one union on the device
+    (gateserve.DesignSet).  Requests resize 1..64 random gates of one design
+    (another drive strength each) and ask for its worst slack; Poisson
+    streams at SRV_RATES req/s (up to SRV_MAX_REQ requests each) and a
+    saturation run (SRV_SAT_REQ requests queued at once).  Batched:
+    continuous batching, at most one request per design per batch, one
+    launch set per batch (apply, RC over the dirty nets, propagation of the
+    batch's designs only, worst slack per design).  Plain: one request at a
+    time through the same launch set.  Every request's worst slack is
+    checked equal on both paths.  With `baseline`, SRV_DESIGNS reference
+    Timers (oracle/_ref/ot_run_ref, CPU path, one process per design, all
+    at once) serve the first SRV_REF_REQ requests of every design of the
+    saturation trace (repower_gate per gate, update_timing), timed."""
+    import multiprocessing as mp
+    import subprocess
+    import tempfile
+    import torch
+    from concurrent.futures import ThreadPoolExecutor
+    from opentimer_b200.gateserve import DesignSet, GateServer, request_trace
+    from opentimer_b200.sizing import write_ops
     rng = np.random.default_rng(SEED + 7)
     pins = np.exp(rng.uniform(np.log(SRV_PINS_LO), np.log(SRV_PINS_HI), SRV_DESIGNS))
-    gates = np.maximum((pins / 2.5).astype(np.int64), 1000)
-    designs, gmaps = [], []
-    for i, G in enumerate(gates):
-        d = synth_design(SEED + 100 + i, workloads.uniform_sizes(SEED + 100 + i, int(G), 2, 16))
-        designs.append(d)
-        gmaps.append(workloads.gate_map(SEED + 200 + i, d))
-    out = {"workload": f"{SRV_DESIGNS} designs, {int(pins.sum())} pins, {int(gates.sum())} "
-                       "nets (RC 2..16 nodes); requests resize 1..64 gates",
-           "rates": []}
-    with TimingServer(slots=SRV_SLOTS, max_requests=64, max_updates=1 << 14) as srv:
-        ids, fps = zip(*[srv.add_design(d) for d in designs])
-        id_of = np.array(ids, np.int32)
-        out["designs_footprint_bytes"] = int(sum(fps))
-        warm = workloads.request_trace(SEED + 8, gmaps, 500, 1e5)
-        warm["design"] = id_of[warm["design"]]
+    gates = np.maximum((pins / SRV_PINS_PER_GATE).astype(np.int64), 1000)
+    with tempfile.TemporaryDirectory() as root:
+        dirs = [os.path.join(root, f"d{i}") for i in range(SRV_DESIGNS)]
+        t0 = time.perf_counter()
+        order = np.argsort(-gates)  # the largest designs first
+        with mp.get_context("spawn").Pool(min(SRV_DESIGNS, os.cpu_count() or 1)) as pool:
+            built = pool.map(_served_design, [(dirs[i], SEED + 100 + int(i), int(gates[i]))
+                                              for i in order.tolist()], chunksize=1)
+        designs, keeps = [None] * SRV_DESIGNS, [None] * SRV_DESIGNS
+        for k, i in enumerate(order.tolist()):
+            designs[i], keeps[i] = built[k]
+        t_build = time.perf_counter() - t0
+        ds = DesignSet(designs)
+        out = {"workload": f"{SRV_DESIGNS} designs, {ds.P} pins, {ds.graph.A} arcs, "
+                           f"{ds.batch.num_nets} nets, {ds.batch.total_nodes} RC nodes; "
+                           "requests resize 1..64 gates and ask for the worst slack",
+               "levels": ds.graph.num_levels, "designs_build_s": t_build, "rates": []}
+        srv = GateServer(ds)
+        # warm-up: a few requests through both paths
+        warm = request_trace(keeps, SEED + 8, 40, None, at_zero=True)
         srv.replay(warm)
         srv.replay(warm, plain=True)
         for rate in SRV_RATES:
-            n = int(rate * SRV_SECONDS)
-            tr = workloads.request_trace(SEED + int(rate), gmaps, n, rate)
-            tr["design"] = id_of[tr["design"]]
-            gates_total = int(tr["gate_start"][-1])
-            b0, r0 = srv.stats()
-            lat_b, span_b = srv.replay(tr)
-            b1, r1 = srv.stats()
-            lat_p, span_p = srv.replay(tr, plain=True)
+            n = min(SRV_MAX_REQ, int(rate * 0.5))
+            tr = request_trace(keeps, SEED + int(rate), n, rate)
+            lat_b, span_b, _ = srv.replay(tr)
+            lat_p, span_p, _ = srv.replay(tr, plain=True)
             out["rates"].append({
                 "offered_req_per_s": rate, "requests": n,
                 "batched": {"p50_ms": _pct(lat_b, 50), "p99_ms": _pct(lat_b, 99),
-                            "req_per_s": n / span_b, "gate_resizes_per_s": gates_total / span_b,
-                            "requests_per_batch": (r1 - r0) / max(b1 - b0, 1)},
+                            "req_per_s": n / span_b},
                 "plain": {"p50_ms": _pct(lat_p, 50), "p99_ms": _pct(lat_p, 99),
-                          "req_per_s": n / span_p, "gate_resizes_per_s": gates_total / span_p}})
-        # saturation: every request queued at t=0
+                          "req_per_s": n / span_p}})
+        # saturation, and the results of the two paths on the same states:
+        # two fresh copies of the designs take the same trace
         n = SRV_SAT_REQ
-        tr = workloads.request_trace(SEED + 9, gmaps, n, None, arrival=np.zeros(n, np.int64))
-        tr["design"] = id_of[tr["design"]]
-        gates_total = int(tr["gate_start"][-1])
-        b0, r0 = srv.stats()
-        _, span_b = srv.replay(tr)
-        b1, r1 = srv.stats()
-        _, span_p = srv.replay(tr, plain=True)
-        out["saturation"] = {"requests": n, "batched_gate_resizes_per_s": gates_total / span_b,
-                             "requests_per_batch": (r1 - r0) / max(b1 - b0, 1),
-                             "plain_gate_resizes_per_s": gates_total / span_p,
-                             "speedup": span_p / span_b}
+        tr = request_trace(keeps, SEED + 9, n, None, at_zero=True)
+        del srv, ds
+        torch.cuda.empty_cache()
+        ds = DesignSet(designs)  # fresh: every gate back at its initial cell
+        srv = GateServer(ds)
+        _, span_b, res_b = srv.replay(tr)
+        del srv, ds
+        torch.cuda.empty_cache()
+        ds = DesignSet(designs)
+        srv = GateServer(ds)
+        _, span_p, res_p = srv.replay(tr, plain=True)
+        out["saturation"] = {"requests": n, "batched_req_per_s": n / span_b,
+                             "plain_req_per_s": n / span_p, "speedup": span_p / span_b,
+                             "results_equal_alone_and_mixed": bool(
+                                 np.array_equal(res_b.view(np.int32), res_p.view(np.int32)))}
+        exe = os.path.join(ROOT, "oracle", "_ref", "ot_run_ref")
+        if baseline is not None and os.path.exists(exe):
+            def ref_one(i):
+                mine = [k for k in range(n) if tr["design"][k] == i][:SRV_REF_REQ]
+                if not mine:
+                    return None
+                ops = os.path.join(dirs[i], "ops.txt")
+                write_ops(ops, [tr["resizes"][k] for k in mine])
+                p = subprocess.run([exe, dirs[i], "cpu", os.path.join(dirs[i], "ref.txt"),
+                                    f"repower={ops}"], capture_output=True, text=True,
+                                   timeout=1200)
+                if p.returncode != 0:
+                    return None
+                return [float(x.split()[2]) for x in p.stdout.splitlines()
+                        if x.startswith("repower_step_s")]
+            with ThreadPoolExecutor(SRV_DESIGNS) as ex:
+                steps = [x for x in ex.map(ref_one, range(SRV_DESIGNS)) if x]
+            if steps:
+                allst = np.concatenate(steps)
+                busiest = max(sum(x) for x in steps)
+                baseline["serving"] = {
+                    "value": len(allst) / busiest, "unit": "requests/s",
+                    "cores": os.cpu_count(), "kind": "reference",
+                    "sample": f"the first {SRV_REF_REQ} requests of every design of the "
+                              "saturation trace, the designs' Timers running at once",
+                    "service_p50_ms": _pct(allst, 50), "service_p99_ms": _pct(allst, 99),
+                    "what": "one reference Timer per design (oracle/_ref, CPU path): "
+                            "repower_gate per resized gate, then update_timing"}
+                out["reference_req_per_s"] = len(allst) / busiest
+                out["speedup_vs_reference"] = (n / span_b) / (len(allst) / busiest)
     return out
 
 

@@ -52,6 +52,7 @@ class ResizeTable:
         self.gates = [g for g, _, _ in keep["gates"]]
         self.gate_index = {g: i for i, g in enumerate(self.gates)}
         self.cell_of = [c for _, c, _ in keep["gates"]]
+        self.cell0 = list(self.cell_of)
         ns = np.asarray(spef["nodes_start"], np.int64)
         net_idx = {n: i for i, n in enumerate(spef["net_names"])}
         self.gate_inputs = []  # per gate: (cell pin, flat RC row, net) of its inputs
@@ -65,6 +66,10 @@ class ResizeTable:
                 if node is not None:
                     ins.append((cp, int(ns[i] + node), i))
             self.gate_inputs.append(ins)
+
+    def reset(self):
+        """Every gate back at the cell the design was built with."""
+        self.cell_of = list(self.cell0)
 
     def updates(self, resizes):
         """Host arrays of one batch of resizes [(gate name or index, cell),
