@@ -1259,7 +1259,7 @@ def cpu_baseline(g, ns_np):
 
 
 def main():
-    global INC_GATES, INC_ITERS
+    global INC_GATES, INC_ITERS, SRV_DESIGNS, SRV_PINS_HI
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
@@ -1279,12 +1279,16 @@ def main():
     ap.add_argument("--inc-gates", type=int, default=INC_GATES,
                     help="gates of the incremental sizing loop's design (smaller: quick runs)")
     ap.add_argument("--inc-iters", type=int, default=INC_ITERS)
+    ap.add_argument("--srv-designs", type=int, default=SRV_DESIGNS,
+                    help="served designs (smaller: quick runs)")
+    ap.add_argument("--srv-pins-hi", type=int, default=SRV_PINS_HI)
     # smaller cases (profiling); the defaults are the benchmark workload
     ap.add_argument("--nets", type=int, default=NUM_NETS)
     ap.add_argument("--min-nodes", type=int, default=2)
     ap.add_argument("--max-nodes", type=int, default=4096)
     args = ap.parse_args()
     INC_GATES, INC_ITERS = args.inc_gates, args.inc_iters
+    SRV_DESIGNS, SRV_PINS_HI = args.srv_designs, args.srv_pins_hi
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
     world, rank, local = dist_setup(args)
     try:

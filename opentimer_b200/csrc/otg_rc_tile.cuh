@@ -263,6 +263,7 @@ __device__ void rc_net_tile(const RcArgs& a, int net, char* ws, int n, int* sh, 
     return f != 0;
   };
 
+  PHASE_BEGIN();
   // ---- T1: edges, degrees, cap maxima
   if (tid == 0) {
     *s_flag = ((unsigned)root >= (unsigned)n) ? OTG_ERR_INVALID : 0;
@@ -300,6 +301,7 @@ __device__ void rc_net_tile(const RcArgs& a, int net, char* ws, int n, int* sh, 
   }
   if (fail()) return;
 
+  PHASE(0);
   // ---- T2: arc ranges; the counters become placement cursors
   {
     const int KW = tile_items(NW, T);
@@ -326,6 +328,7 @@ __device__ void rc_net_tile(const RcArgs& a, int net, char* ws, int n, int* sh, 
   }
   if (fail()) return;
 
+  PHASE(1);
   // ---- T3: place arcs, Euler-tour successors
   const int head = (int)off[root];
   for (int e = tid; e < m; e += T) {
@@ -368,6 +371,7 @@ __device__ void rc_net_tile(const RcArgs& a, int net, char* ws, int n, int* sh, 
     if (tid == 0) *s_ns = 0;
     ++sel;  // uniform: every thread read the same count
   }
+  PHASE(2);
   for (int s = tid; s < ns; s += T) {
     int cur = (int)spos[s];
     unsigned o = 0, next = 0xFFFFFFFFu;
@@ -385,6 +389,7 @@ __device__ void rc_net_tile(const RcArgs& a, int net, char* ws, int n, int* sh, 
     sl[s] = sl_pack(next, o);
   }
   __syncthreads();
+  PHASE(3);
   {
     int rounds = 1;
     while ((1 << rounds) < ns) ++rounds;
@@ -399,6 +404,7 @@ __device__ void rc_net_tile(const RcArgs& a, int net, char* ws, int n, int* sh, 
       __syncthreads();
     }
   }
+  PHASE(4);
   // the head's chain must be the whole tour (else: a cycle or a second
   // component, i.e. not a tree)
   if (tid == 0) {
@@ -415,6 +421,7 @@ __device__ void rc_net_tile(const RcArgs& a, int net, char* ws, int n, int* sh, 
   for (int w = tid; w < NDW; w += T) db[w] = 0u;
   __syncthreads();
 
+  PHASE(5);
   // ---- T5: per edge: down arc, parent/child, entry/exit; directed edge out
   for (int e = tid; e < m; e += T) {
     const unsigned pp = PX[e], xy = E[e];
@@ -429,6 +436,7 @@ __device__ void rc_net_tile(const RcArgs& a, int net, char* ws, int n, int* sh, 
     g_edges[eb + e] = make_int2(par_, ch);
   }
   __syncthreads();
+  PHASE(6);
   // ---- T6: preorder and depth from the down-arc bitmap
   {
     const int KW = tile_items(NDW, T);
@@ -473,6 +481,7 @@ __device__ void rc_net_tile(const RcArgs& a, int net, char* ws, int n, int* sh, 
     if (lane == 0 && dmax) atomicMax(s_maxd, dmax);
   }
   __syncthreads();
+  PHASE(7);
   // ---- T7: BFS slots: stable sort by depth of the ids in descending order
   {
     Ix* nas = bpre;  // BFS slot -> id, then BFS slot -> preorder
@@ -494,6 +503,7 @@ __device__ void rc_net_tile(const RcArgs& a, int net, char* ws, int n, int* sh, 
     __syncthreads();
   }
 
+  PHASE(8);
   // ---- E: Elmore per corner pair
   for (int cp = 0; cp < 2; ++cp) {
     long long* wtl0 = shl;
@@ -515,6 +525,7 @@ __device__ void rc_net_tile(const RcArgs& a, int net, char* ws, int n, int* sh, 
         },
         wtl0);
     __syncthreads();
+    PHASE(10);
     // E2: load = prefix difference over the subtree's preorder range
     {
       const int KE = tile_items(n, T);
@@ -532,6 +543,7 @@ __device__ void rc_net_tile(const RcArgs& a, int net, char* ws, int n, int* sh, 
       commit_max(mw1, smx + 5);
     }
     __syncthreads();
+    PHASE(11);
     // E3: delay terms W = fx(R * load) into Ip; load out in BFS order
     float upw[2], dnw[2];
     fx_scale(__uint_as_float(smx[4]), n, upw[0], dnw[0]);
@@ -549,6 +561,7 @@ __device__ void rc_net_tile(const RcArgs& a, int net, char* ws, int n, int* sh, 
     }
     if (tid < 2) smx[6 + tid] = 0u;
     __syncthreads();
+    PHASE(12);
     // E4: delay = prefix over the signed tour of W; emitted at down arcs
     {
       float md0 = 0.f, md1 = 0.f;
@@ -574,6 +587,7 @@ __device__ void rc_net_tile(const RcArgs& a, int net, char* ws, int n, int* sh, 
       if (tid == 0) Y[0] = make_float2(0.f, 0.f);
     }
     __syncthreads();
+    PHASE(13);
     // E5: ldelay scan over the preorder of cap * delay (scale from the
     // bound max|cap| * max|delay|); delay out in BFS order
     float upd[2], dnd[2];
@@ -597,6 +611,7 @@ __device__ void rc_net_tile(const RcArgs& a, int net, char* ws, int n, int* sh, 
         wtl0);
     if (tid < 2) smx[8 + tid] = 0u;
     __syncthreads();
+    PHASE(14);
     // E6: ldelay = prefix difference over the subtree range
     {
       const int KE = tile_items(n, T);
@@ -614,6 +629,7 @@ __device__ void rc_net_tile(const RcArgs& a, int net, char* ws, int n, int* sh, 
       commit_max(mw1, smx + 9);
     }
     __syncthreads();
+    PHASE(15);
     // E7: beta terms into Ip; ldelay out
     fx_scale(__uint_as_float(smx[8]), n, upw[0], dnw[0]);
     fx_scale(__uint_as_float(smx[9]), n, upw[1], dnw[1]);
@@ -629,6 +645,7 @@ __device__ void rc_net_tile(const RcArgs& a, int net, char* ws, int n, int* sh, 
       for (int r = tid; r < n; r += T) out[2 * (size_t)(b + r) + cp] = X[bpre[r]];
     }
     __syncthreads();
+    PHASE(16);
     // E8: beta over the signed tour -> impulse = 2 beta - delay^2 (into X)
     scan_pair<T>(
         A,
@@ -648,6 +665,7 @@ __device__ void rc_net_tile(const RcArgs& a, int net, char* ws, int n, int* sh, 
         wtl1);
     if (tid == 0) X[0] = make_float2(0.f, 0.f);
     __syncthreads();
+    PHASE(17);
     // E9: impulse out; sink slews
     {
       float2* out = (float2*)a.impulse;
@@ -668,5 +686,6 @@ __device__ void rc_net_tile(const RcArgs& a, int net, char* ws, int n, int* sh, 
       }
     }
     __syncthreads();
+    PHASE(18);
   }
 }

@@ -308,7 +308,9 @@ def spef(path, rng, nets, rc_nodes=(2, 16), rc_log=False):
     tree of its pins plus internal nodes <net>:<k>, rc_nodes[0]..rc_nodes[1]
     nodes (uniform, or log-uniform with rc_log) but never fewer than its
     pins, a random recursive tree rooted at the driver, R ~ U(0.5, 20) ohm,
-    ground C ~ U(0.1, 3) fF, RES lines shuffled with random orientation.
+    ground C ~ U(0.1, 3) fF (times 16/n on trees of n > 16 nodes, so that a
+    net's load stays within the tables' range), RES lines shuffled with
+    random orientation.
     The random draws are made here; the text is formatted by
     otg_spef_write (the library's SPEF writer)."""
     import ctypes
@@ -349,7 +351,10 @@ def spef(path, rng, nets, rc_nodes=(2, 16), rc_log=False):
     key = np.where(local == 0, -1.0, rng.random(V))
     order = np.lexsort((key, net_of))
     codes = code0[order]
-    caps = rng.uniform(0.1, 3.0, V)
+    # ground caps U(0.1, 3) fF per node on trees of up to 16 nodes; larger
+    # trees share out the same total per net (cap x 16/n), so a net's load
+    # stays in the range of the library's tables (1..100 fF)
+    caps = rng.uniform(0.1, 3.0, V) * np.minimum(1.0, 16.0 / n)[net_of]
     # random recursive tree over the positions: parent of position i in [0, i)
     E = V - N
     child = np.nonzero(local > 0)[0]

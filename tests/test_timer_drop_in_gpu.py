@@ -161,3 +161,43 @@ def test_spef_reader_matches_timer_storage(runs):
         assert np.array_equal(cap, np.stack(S["cap"][name])), name
         k += e - b
     assert k == int(ns[-1]) > 10000
+
+
+def test_second_cuda_update_after_repower(tmp_path, cuda):
+    """The unchanged Timer's second update_timing in CUDA mode, after
+    repower_gate.  Its CUDA path rebuilds the flat storage for every net but
+    re-flattens only the dirty ones (ot/timer/timer.cpp:929-970,
+    ot/timer/net.cpp:499-514): the clean nets reach rct_bfs_and_compute_cuda
+    with zeroed edges and roots.  libotg checks every net, reports them
+    (OTG_ERR_NOT_TREE on stderr) without reading out of range, and still
+    times every re-flattened net: those nets' RC values must match the
+    reference's CPU path after the same resizes."""
+    if not (os.path.exists(EXE_REF) and os.path.exists(EXE_OTG)):
+        pytest.skip("the reference Timer harness (oracle/_ref) is not built")
+    from opentimer_b200.sizing import resize_trace, write_ops
+    d = str(tmp_path)
+    keep = {}
+    designgen.write_design(d, seed=2025, gates=1500, keep=keep)
+    steps = resize_trace(keep, seed=3, steps=1, per_step=30)
+    ops = os.path.join(d, "ops.txt")
+    write_ops(ops, steps)
+    outs = {}
+    for exe, mode in ((EXE_OTG, "cuda"), (EXE_REF, "cpu")):
+        out = os.path.join(d, f"{os.path.basename(exe)}_{mode}_repower.txt")
+        p = subprocess.run([exe, d, mode, out, f"repower={ops}"], capture_output=True, text=True,
+                           timeout=600)
+        assert p.returncode == 0, p.stderr[-2000:]
+        outs[mode] = (p.stderr, out)
+    assert "rct_bfs_and_compute_cuda: OTG_ERR_NOT_TREE" in outs["cuda"][0]
+    conn = {g: c for g, _, c in keep["gates"]}
+    dirty = {n for g, _ in steps[0] for n in conn[g].values()}
+    R = {}
+    for mode in ("cuda", "cpu"):
+        R[mode] = {}
+        with open(outs[mode][1]) as f:
+            for line in f:
+                t = line.split()
+                if t[0] == "R" and t[1] in dirty:
+                    R[mode][(t[1], t[2])] = np.array([float(x) for x in t[3:]], np.float64)
+    assert set(R["cuda"]) == set(R["cpu"]) and len(R["cpu"]) > 50
+    assert rc_ok(R["cuda"], R["cpu"]) <= 1.0
