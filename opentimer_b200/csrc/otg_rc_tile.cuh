@@ -38,7 +38,7 @@
 // ---- layout -------------------------------------------------------------
 struct RcTileLayout {
   // persistent
-  uint32_t pre, psz, bpre, code, pres, nap;
+  uint32_t pre, psz, bpre, code, pres;
   // topology scratch (T1-T7)
   uint32_t E, PX, deg, off, succ, sidx, subrk, spos, sl, db, dbp, depth, par, slot, rbuf, hist;
   // Elmore (E1-E9), overlaying the topology scratch
@@ -63,7 +63,6 @@ __host__ __device__ inline RcTileLayout rc_tile_layout(int n, int T) {
   OTG_TAKE(bpre, 2u * N);
   OTG_TAKE(code, 2u * A);
   OTG_TAKE(pres, 4u * N);
-  OTG_TAKE(nap, 2u * N);
   const uint32_t scratch = o;
   // topology
   OTG_TAKE(E, 4u * M);
@@ -221,7 +220,6 @@ __device__ void rc_net_tile(const RcArgs& a, int net, char* ws, int n, int* sh, 
   Ix* bpre = (Ix*)(ws + L.bpre);
   int16_t* code = (int16_t*)(ws + L.code);
   float* pres = (float*)(ws + L.pres);
-  Ix* nap = (Ix*)(ws + L.nap);
   unsigned* E = (unsigned*)(ws + L.E);
   unsigned* PX = (unsigned*)(ws + L.PX);
   unsigned* deg = (unsigned*)(ws + L.deg);
@@ -452,7 +450,6 @@ __device__ void rc_net_tile(const RcArgs& a, int net, char* ws, int n, int* sh, 
   if (tid == 0) {
     pre[root] = 0;
     psz[0] = (Ix)n;
-    nap[0] = (Ix)root;
     pres[0] = 0.0f;
     depth[root] = 0;
     par[root] = (Ix)root;
@@ -471,7 +468,6 @@ __device__ void rc_net_tile(const RcArgs& a, int net, char* ws, int n, int* sh, 
       depth[ch] = (Ix)d;
       par[ch] = (Ix)(pc & 0xFFFFu);
       psz[pv] = (Ix)((ex - en + 1) >> 1);
-      nap[pv] = (Ix)ch;
       pres[pv] = g_res[eb + e];
       code[en] = (int16_t)(pv + 1);
       code[ex] = (int16_t)(-(pv + 1));
@@ -482,16 +478,54 @@ __device__ void rc_net_tile(const RcArgs& a, int net, char* ws, int n, int* sh, 
   }
   __syncthreads();
   PHASE(7);
-  // ---- T7: BFS slots: stable sort by depth of the ids in descending order
+  // ---- T7: BFS slots, the rank under (depth asc, local id desc)
   {
     Ix* nas = bpre;  // BFS slot -> id, then BFS slot -> preorder
-    block_radix_sort<T>(
-        n, 32 - __clz(max(*s_maxd, 1)), [&](int j) { return (int)depth[n - 1 - j]; }, rbuf,
-        rbuf + n, nas, hist, wt0);
-    for (int r = tid; r < n; r += T) {
-      const int v = n - 1 - (int)nas[r];
-      nas[r] = (Ix)v;
-      slot[v] = (Ix)r;
+    const int maxd = *s_maxd;
+    const int NWB = (n + 31) >> 5;  // bitmap words per depth
+    const int words = (maxd + 1) * NWB;
+    const int region = (int)(L.hist - L.rbuf) + 4 * (1 << rc_radix_bits(T)) * W;
+    if (words * 6 <= region) {
+      // shallow trees: one bitmap of ids per depth; a node's slot is the
+      // number of set bits before it in (depth asc, word desc, bit desc)
+      // order: a prefix count per word plus the bits above it in its word
+      unsigned* bm = (unsigned*)rbuf;
+      Ix* wp = (Ix*)(bm + words);
+      for (int k = tid; k < words; k += T) bm[k] = 0u;
+      __syncthreads();
+      for (int v = tid; v < n; v += T)
+        atomicOr(&bm[(int)depth[v] * NWB + (v >> 5)], 1u << (v & 31));
+      __syncthreads();
+      // flattened order f = d * NWB + (NWB - 1 - w)
+      const int KW = tile_items(words, T);
+      const int f0 = tid * KW, f1 = min(f0 + KW, words);
+      auto word_of = [&](int f) { const int d = f / NWB; return d * NWB + (NWB - 1 - (f - d * NWB)); };
+      int local = 0;
+      for (int f = f0; f < f1; ++f) local += __popc(bm[word_of(f)]);
+      int run = tile_excl_i32<T>(local, wt0, nullptr);
+      for (int f = f0; f < f1; ++f) {
+        const int k = word_of(f);
+        wp[k] = (Ix)run;
+        run += __popc(bm[k]);
+      }
+      __syncthreads();
+      for (int v = tid; v < n; v += T) {
+        const int k = (int)depth[v] * NWB + (v >> 5);
+        const int r = (int)wp[k] + __popc(bm[k] >> (v & 31) >> 1);
+        slot[v] = (Ix)r;
+        nas[r] = (Ix)v;
+      }
+    } else {
+      // deep trees: stable radix sort by depth of the ids in descending order
+      // (the reference's (distance asc, local id desc) rule, sort.cuh:102-121)
+      block_radix_sort<T>(
+          n, 32 - __clz(max(maxd, 1)), [&](int j) { return (int)depth[n - 1 - j]; }, rbuf,
+          rbuf + n, nas, hist, wt0);
+      for (int r = tid; r < n; r += T) {
+        const int v = n - 1 - (int)nas[r];
+        nas[r] = (Ix)v;
+        slot[v] = (Ix)r;
+      }
     }
     __syncthreads();
     for (int v = tid; v < n; v += T) a.node2bfs[b + v] = (int)slot[v];
@@ -512,11 +546,15 @@ __device__ void rc_net_tile(const RcArgs& a, int net, char* ws, int n, int* sh, 
     fx_scale(__uint_as_float(smx[2 * cp]), n, upc[0], dnc[0]);
     fx_scale(__uint_as_float(smx[2 * cp + 1]), n, upc[1], dnc[1]);
     if (tid < 4) smx[4 + tid] = 0u;  // the pair's sweep maxima (w, delay, w2)
+    // E0: the pair's caps, read once in id order (coalesced), staged by
+    // preorder in Y (free until the delay sweep)
+    for (int v = tid; v < n; v += T) Y[pre[v]] = cap2[2 * (size_t)(b + v) + cp];
+    __syncthreads();
     // E1: load scan over the preorder: Ip[i] = exclusive prefix of cap
     scan_pair<T>(
         n,
         [&](int i) {
-          const float2 c = cap2[2 * (size_t)(b + (int)nap[i]) + cp];
+          const float2 c = Y[i];
           return make_longlong2(to_fx(c.x, upc[0]), to_fx(c.y, upc[1]));
         },
         [&](int i, long long e0, long long e1, longlong2 t) {
@@ -562,7 +600,14 @@ __device__ void rc_net_tile(const RcArgs& a, int net, char* ws, int n, int* sh, 
     if (tid < 2) smx[6 + tid] = 0u;
     __syncthreads();
     PHASE(12);
-    // E4: delay = prefix over the signed tour of W; emitted at down arcs
+    // E4: delay = prefix over the signed tour of W; emitted at down arcs.
+    // First the caps move from Y to X (free since the load went out); the
+    // scan's barrier lies between this copy and the first delay written to Y.
+    {
+      const int KE = tile_items(n, T);
+      const int i0 = tid * KE, i1 = min(i0 + KE, n);
+      for (int i = i0; i < i1; ++i) X[i] = Y[i];
+    }
     {
       float md0 = 0.f, md1 = 0.f;
       scan_pair<T>(
@@ -600,7 +645,7 @@ __device__ void rc_net_tile(const RcArgs& a, int net, char* ws, int n, int* sh, 
     scan_pair<T>(
         n,
         [&](int i) {
-          const float2 c = cap2[2 * (size_t)(b + (int)nap[i]) + cp];
+          const float2 c = X[i];
           const float2 d = Y[i];
           return make_longlong2(to_fx(c.x * d.x, upd[0]), to_fx(c.y * d.y, upd[1]));
         },
