@@ -93,8 +93,12 @@ struct RcLayout {
   uint32_t ns_cap;  // capacity of the splitter arrays
 };
 
-// Sublist splitters of the Euler-tour ranking: about one arc in kSplit.
-constexpr int kSplit = 8;
+// Sublist splitters of the Euler-tour ranking: about one arc in kSplit
+// (a power of two; OTG_KSPLIT overrides it at build time).
+#ifndef OTG_KSPLIT
+#define OTG_KSPLIT 8
+#endif
+constexpr int kSplit = OTG_KSPLIT;
 
 // Radix digit of the block sort: 8 bits, 7 for 1024-thread CTAs (whose
 // 32 per-warp histograms would otherwise take 32 KB of shared memory).

@@ -8,8 +8,7 @@
 // (rct.cu:314-359) and compute_net_timing (rct.cu:11-59).
 //
 // Topology (T1-T7) works edge by edge and needs no adjacency list:
-//   T1  edges in (validated), packed 16-bit degree counters by atomics,
-//       and the per-corner maxima of the caps;
+//   T1  edges in (validated), packed 16-bit degree counters by atomics;
 //   T2  degree scan -> each node's arc range [off(v), off(v+1));
 //   T3  one atomic per arc end places the arc in its node's range, and
 //       since the twin's place is known in the same step, the Euler-tour
@@ -251,7 +250,6 @@ __device__ void rc_net_tile(const RcArgs& a, int net, char* ws, int n, int* sh, 
   // the forest's pointers in registers (a lives in shared memory)
   int2* __restrict__ g_edges = a.edges;
   const float* __restrict__ g_res = a.res;
-  const float4* __restrict__ g_cap = a.cap;
   const float2* __restrict__ cap2 = (const float2*)a.cap;
 
   auto fail = [&]() -> bool {
@@ -262,7 +260,7 @@ __device__ void rc_net_tile(const RcArgs& a, int net, char* ws, int n, int* sh, 
   };
 
   PHASE_BEGIN();
-  // ---- T1: edges, degrees, cap maxima
+  // ---- T1: edges and degrees
   if (tid == 0) {
     *s_flag = ((unsigned)root >= (unsigned)n) ? OTG_ERR_INVALID : 0;
     *s_ns = 0;
@@ -282,20 +280,6 @@ __device__ void rc_net_tile(const RcArgs& a, int net, char* ws, int n, int* sh, 
     E[e] = (unsigned)ed.x | ((unsigned)ed.y << 16);
     atomicAdd(&deg[ed.x >> 1], 1u << ((ed.x & 1) << 4));
     atomicAdd(&deg[ed.y >> 1], 1u << ((ed.y & 1) << 4));
-  }
-  {
-    float m0 = 0.f, m1 = 0.f, m2 = 0.f, m3 = 0.f;
-    for (int v = tid; v < n; v += T) {
-      const float4 c = g_cap[b + v];
-      m0 = fmaxf(m0, fabsf(c.x));
-      m1 = fmaxf(m1, fabsf(c.y));
-      m2 = fmaxf(m2, fabsf(c.z));
-      m3 = fmaxf(m3, fabsf(c.w));
-    }
-    commit_max(m0, smx + 0);
-    commit_max(m1, smx + 1);
-    commit_max(m2, smx + 2);
-    commit_max(m3, smx + 3);
   }
   if (fail()) return;
 
@@ -542,14 +526,24 @@ __device__ void rc_net_tile(const RcArgs& a, int net, char* ws, int n, int* sh, 
   for (int cp = 0; cp < 2; ++cp) {
     long long* wtl0 = shl;
     long long* wtl1 = shl + 2 * W;
+    if (tid < 4) smx[4 + tid] = 0u;  // the pair's sweep maxima (w, delay, w2)
+    // E0: the pair's caps, read once in id order (coalesced), staged by
+    // preorder in Y (free until the delay sweep), and their maxima
+    {
+      float m0 = 0.f, m1 = 0.f;
+      for (int v = tid; v < n; v += T) {
+        const float2 c = cap2[2 * (size_t)(b + v) + cp];
+        Y[pre[v]] = c;
+        m0 = fmaxf(m0, fabsf(c.x));
+        m1 = fmaxf(m1, fabsf(c.y));
+      }
+      commit_max(m0, smx + 2 * cp);
+      commit_max(m1, smx + 2 * cp + 1);
+    }
+    __syncthreads();
     float upc[2], dnc[2];
     fx_scale(__uint_as_float(smx[2 * cp]), n, upc[0], dnc[0]);
     fx_scale(__uint_as_float(smx[2 * cp + 1]), n, upc[1], dnc[1]);
-    if (tid < 4) smx[4 + tid] = 0u;  // the pair's sweep maxima (w, delay, w2)
-    // E0: the pair's caps, read once in id order (coalesced), staged by
-    // preorder in Y (free until the delay sweep)
-    for (int v = tid; v < n; v += T) Y[pre[v]] = cap2[2 * (size_t)(b + v) + cp];
-    __syncthreads();
     // E1: load scan over the preorder: Ip[i] = exclusive prefix of cap
     scan_pair<T>(
         n,
