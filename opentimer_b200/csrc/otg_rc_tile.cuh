@@ -96,9 +96,7 @@ __host__ __device__ inline RcTileLayout rc_tile_layout(int n, int T) {
 }
 
 // ---- scans --------------------------------------------------------------
-#ifndef OTG_SCAN_UNROLL
-#define OTG_SCAN_UNROLL 3
-#endif
+
 // Items per thread for a one-tile scan of C items: odd, so that consecutive
 // threads' strided accesses of 8- and 16-byte elements fall in different
 // banks.
@@ -178,7 +176,7 @@ __device__ __forceinline__ void scan_pair(int C, TermF term, EmitF emit, long lo
   const int i0 = threadIdx.x * KE;
   const int i1 = min(i0 + KE, C);
   long long s0 = 0, s1 = 0;
-#pragma unroll OTG_SCAN_UNROLL
+#pragma unroll 3
   for (int i = i0; i < i1; ++i) {
     const longlong2 t = term(i);
     s0 += t.x;
@@ -186,7 +184,7 @@ __device__ __forceinline__ void scan_pair(int C, TermF term, EmitF emit, long lo
   }
   long long e0, e1;
   tile_excl_i64x2<T>(s0, s1, wt, e0, e1);
-#pragma unroll OTG_SCAN_UNROLL
+#pragma unroll 3
   for (int i = i0; i < i1; ++i) {
     const longlong2 t = term(i);
     emit(i, e0, e1, t);
