@@ -152,8 +152,11 @@ otg_status otg_rc_status(const void* workspace, otg_stream_t stream, int32_t* ba
  *   level_ends[n+2] level_ends[0]=0, level_ends[k+1] = end of level k
  *   counts[2]       counts[0] = number of levels, counts[1] = pins emitted
  * level(v) = 1 + max over candidate fanouts (longest path to a sink).  All
- * levels run inside one cooperative launch (no host round trip per level);
- * its grid barrier is bounded and reports OTG_ERR_TIMEOUT instead of hanging.
+ * levels run inside one launch (no host round trip per level): a single
+ * thread-block cluster for graphs of up to about a million pins with a seed
+ * level of at most 8192 pins, a cooperative grid otherwise, whose grid
+ * barrier is bounded and reports OTG_ERR_TIMEOUT instead of hanging.  Both
+ * give identical outputs.
  */
 otg_status otg_levelize_workspace_size(int32_t n, int32_t num_edges, size_t* bytes);
 otg_status otg_levelize(int32_t n, int32_t num_edges, const int32_t* fanin_start,

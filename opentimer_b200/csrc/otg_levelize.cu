@@ -26,12 +26,20 @@
 // global memory whose waits are bounded by %globaltimer: a wait that runs
 // past the limit raises an abort flag that every other wait also watches,
 // so the kernel always returns and the host sees OTG_ERR_TIMEOUT.
+//
+// Graphs of up to about a million pins whose seed level is narrow run
+// instead in ONE thread-block cluster (levelize_cluster_kernel below):
+// the same rule and the same outputs, with the ready bitmaps and counts in
+// distributed shared memory, the hardware cluster barrier between levels,
+// and the next level's fanin ranges gathered while the counters are
+// decremented.
 #include <cooperative_groups.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
 #include <algorithm>
 #include <climits>
+#include <cstdlib>
 
 #include "../../include/otg.h"
 #include "otg_internal.cuh"
@@ -278,10 +286,395 @@ __global__ void __launch_bounds__(LT) levelize_kernel(int n, const int* fanin_st
   }
 }
 
+// ---- the cluster path --------------------------------------------------
+//
+// Graphs whose two ready bitmaps fit in the shared memory of one thread-
+// block cluster (up to 16 CTAs, 8 or fewer where the device cannot place
+// 16) run the same frontier rule inside one cluster: CTA r owns the bitmap
+// words [r*C, (r+1)*C) of both levels in its own shared memory, and a pin
+// whose fanout counter reaches zero sets its bit and bumps its owner's
+// count through distributed shared memory.  A level ends at the hardware
+// cluster barrier (barrier.cluster, release/acquire) instead of the global
+// barrier, and the counts and bitmaps never leave the SMs, so a level costs
+// the three dependent global accesses of its expansion (fanin_start,
+// fanin, the counter) plus on-chip work.  The emission rule is the one
+// above (seed order, then ascending pin index per level, CTA ranges in rank
+// order), so both paths give identical outputs.
+//
+// No wait in this path polls memory: the cluster barrier is hardware, and
+// every CTA takes the same number of barriers (the loop ends on the level
+// total, which every CTA computes from the same counts).
+
+// CTA widths of the cluster path: a level of a narrow graph has a few pins
+// per CTA, and every warp of the CTA takes part in each of its scans and
+// barriers, so narrow graphs run narrow CTAs.
+constexpr int kCtMax = 1024;
+
+// Optional per-segment cycle accounting of the level loop (build with
+// -DOTG_PHASE_TIMING): thread 0 of CTA 0 sums the clock64() deltas of each
+// segment and stores them after the counts, in counts[2..9] (the caller
+// then passes a counts array of 10).
+#ifdef OTG_PHASE_TIMING
+#define LV_PHASE_BEGIN() long long _ph_t = clock64(), _ph[8] = {0, 0, 0, 0, 0, 0, 0, 0}
+#define LV_PHASE(k)                        \
+  do {                                     \
+    if (gtid == 0) {                       \
+      const long long _t = clock64();      \
+      _ph[k] += _t - _ph_t;                \
+      _ph_t = _t;                          \
+    }                                      \
+  } while (0)
+#define LV_PHASE_END(c)                                                   \
+  do {                                                                    \
+    if (gtid == 0)                                                        \
+      for (int _k = 0; _k < 8; ++_k) (c)[2 + _k] = (int)(_ph[_k] >> 10); \
+  } while (0)
+#else
+#define LV_PHASE_BEGIN() \
+  do {                   \
+  } while (0)
+#define LV_PHASE(k) \
+  do {              \
+  } while (0)
+#define LV_PHASE_END(c) \
+  do {                  \
+  } while (0)
+#endif
+
+namespace cg = cooperative_groups;
+
+// Where a pin that becomes ready goes: its owner's bitmap word and count
+// (distributed shared memory), and the readying CTA's own list of fanin
+// ranges for the next level's expansion.
+struct ClNext {
+  unsigned* bm;  // next level's bitmap (this CTA's address; mapped to the owner)
+  int cshift;    // log2 of the words per CTA range: the owner of word w is w >> cshift
+  int* rc;       // next level's per-owner counts [16] (every CTA keeps a copy)
+  int2* lst;     // this CTA's list of (fanin start, fanin count) for the next level
+  int* lcnt;     // its length
+  int* ovf;      // next level's overflow flag (set in every CTA)
+  int cap;       // list capacity
+};
+
+// One fanin edge per lane (as decrement above).  The leader lane of each
+// distinct pin v also loads v's fanin range, in flight with the decrement,
+// so a pin that becomes ready is expanded next level without another
+// global round trip; a full list raises the next level's overflow flag in
+// every CTA, and that level then expands from the bitmaps instead.
+__device__ __forceinline__ void decrement_cl(int v, bool ok, const int* fanin_start, int* cnt,
+                                             const ClNext& nx, const cg::cluster_group& cl) {
+  const int lane = threadIdx.x & 31;
+  const unsigned peers = __match_any_sync(FULL, ok ? v : -2 - lane);
+  if (ok && (__ffs(peers) - 1 == lane)) {
+    const int k = __popc(peers);
+    const int s0 = __ldg(fanin_start + v), s1 = __ldg(fanin_start + v + 1);
+    const int old = atomicSub(&cnt[v], k);
+    if (old > 0 && old - k <= 0) {
+      const int w = v >> 5, owner = w >> nx.cshift;
+      atomicOr(cl.map_shared_rank(nx.bm, owner) + (w - (owner << nx.cshift)), 1u << (v & 31));
+      const int S = (int)cl.num_blocks();
+      for (int i = 0; i < S; ++i) atomicAdd(cl.map_shared_rank(nx.rc + owner, i), 1);
+      const int slot = atomicAdd(nx.lcnt, 1);
+      if (slot < nx.cap) {
+        nx.lst[slot] = make_int2(s0, s1 - s0);
+      } else {
+        for (int i = 0; i < (int)cl.num_blocks(); ++i) *cl.map_shared_rank(nx.ovf, i) = 1;
+      }
+    }
+  }
+}
+
+// Expansion of m fanin ranges (range(k) -> (start, count)) with no block
+// barrier: 32 ranges at a time, every warp scans the same 32 counts with
+// shuffles and takes its own slice of their edges (warp w: edges w*32 +
+// lane, stepping by the CTA width), the edge's range found by a binary
+// search over the lanes' exclusive starts.
+template <int CT, class RangeF>
+__device__ __forceinline__ void expand_warps(int m, RangeF range, const int* fanin_start,
+                                             const int* fanin, int* cnt, int n, const ClNext& nx,
+                                             const cg::cluster_group& cl) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (int c0 = 0; c0 < m; c0 += 32) {
+    int2 en = make_int2(0, 0);
+    if (c0 + lane < m) en = range(c0 + lane);
+    int y = en.y;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const int z = __shfl_up_sync(FULL, y, d);
+      if (lane >= d) y += z;
+    }
+    const int excl = y - en.y;
+    const int etot = __shfl_sync(FULL, y, 31);
+    for (int q0 = w * 32; q0 < etot; q0 += CT) {
+      const int q = q0 + lane;
+      int lo = 0;  // the last lane whose start is <= q
+#pragma unroll
+      for (int step = 16; step >= 1; step >>= 1) {
+        const int cand = lo + step;
+        const int ex = __shfl_sync(FULL, excl, cand & 31);
+        if (cand < 32 && ex <= q) lo = cand;
+      }
+      const int e0 = __shfl_sync(FULL, en.x, lo), ex0 = __shfl_sync(FULL, excl, lo);
+      const int v = q < etot ? fanin[e0 + (q - ex0)] : -1;
+      decrement_cl(v, (unsigned)v < (unsigned)n, fanin_start, cnt, nx, cl);
+    }
+  }
+}
+
+template <int CT>
+__global__ void __launch_bounds__(CT, 1) levelize_cluster_kernel(
+    int n, const int* fanin_start, const int* fanin, const int* out_deg, const int* frontier0,
+    int first_size, int* order, int* level, int* level_ends, int* counts, LvCtl* ctl, int* cnt,
+    int cshift, int lst_cap) {
+  const int C = 1 << cshift;  // bitmap words per CTA range
+  extern __shared__ unsigned lv_sm[];
+  unsigned* const bm0 = lv_sm;  // level L's ready pins: bm0 for even L, bm1 for odd
+  unsigned* const bm1 = lv_sm + C;
+  int2* const lst0 = (int2*)(lv_sm + 2 * C);  // fanin ranges to expand at even / odd levels
+  int2* const lst1 = lst0 + lst_cap;
+  // per-level scalars in three rotating slots (this level, the next, the
+  // one after): a slot is cleared a level before anything adds to it, so
+  // no block barrier orders the clear
+  __shared__ int rc[3][16];  // ready pins of every CTA's range (each CTA keeps a copy)
+  __shared__ int lcnt[3];  // length of the list of fanin ranges
+  __shared__ int ovf[3];   // some CTA's list overflowed
+  __shared__ int wsum[2][2 * (CT / 32)];  // warp totals of the level's scans, by level parity
+  __shared__ int s_excl[CT], s_e0[CT];    // list entries: warp-exclusive edge start, fanin start
+  const cg::cluster_group cl = cg::this_cluster();
+  const int S = (int)cl.num_blocks(), r = (int)cl.block_rank(), tid = threadIdx.x;
+  const int gtid = r * CT + tid, gstride = S * CT;
+  const int nw = (n + 31) >> 5;
+  const int lane = tid & 31, w = tid >> 5;
+
+  for (int v = gtid; v < n; v += gstride) {
+    cnt[v] = out_deg[v];
+    level[v] = -1;
+  }
+  for (int i = tid; i < 2 * C; i += CT) lv_sm[i] = 0u;
+  if (tid < 48) rc[tid / 16][tid % 16] = 0;
+  if (tid < 3) { lcnt[tid] = 0; ovf[tid] = 0; }
+  cl.sync();
+  for (int k = gtid; k < first_size; k += gstride) {
+    const int v = frontier0[k];
+    order[k] = v;
+    if ((unsigned)v < (unsigned)n) {
+      level[v] = 0;
+      cnt[v] = INT_MAX;  // after the counters' fill (cluster barrier above)
+    } else {
+      atomicCAS(&ctl->status, 0, (int)OTG_ERR_INVALID);
+    }
+  }
+  if (gtid == 0) {
+    level_ends[0] = 0;
+    if (first_size > 0) level_ends[1] = first_size;
+  }
+  if (first_size == 0) {  // uniform: no CTA has touched another's memory
+    if (gtid == 0) { counts[0] = 0; counts[1] = 0; }
+    return;
+  }
+  cl.sync();
+  // expand the seed into level 1 (bm1, slot 1, lst1)
+  {
+    const ClNext nx{bm1, cshift, rc[1], lst1, &lcnt[1], &ovf[1], lst_cap};
+    for (int k0 = r * CT; k0 < first_size; k0 += gstride) {
+      const int k = k0 + tid;
+      const bool act = k < first_size && (unsigned)order[k] < (unsigned)n;
+      const int u = act ? order[k] : 0;
+      int e = act ? fanin_start[u] : 0;
+      const int e1 = act ? fanin_start[u + 1] : 0;
+      while (__any_sync(FULL, e < e1)) {
+        const bool has = e < e1;
+        const int v = has ? fanin[e] : -1;
+        decrement_cl(v, has && (unsigned)v < (unsigned)n, fanin_start, cnt, nx, cl);
+        e += has ? 1 : 0;
+      }
+    }
+  }
+  int emitted = first_size;
+  int L = 1;
+  const int w0 = min(nw, r * C), w1 = min(nw, (r + 1) * C);
+  // this thread's words of the range: KW consecutive ones
+  const int KW = max(1, (w1 - w0 + CT - 1) / CT);
+  const int i0 = min(w1, w0 + tid * KW), i1 = min(w1, i0 + KW);
+  int q_now = 1, q_next = 2, q_free = 0;
+  LV_PHASE_BEGIN();
+  while (true) {
+    cl.sync();
+    LV_PHASE(0);
+    const int par = L & 1;
+    unsigned* cur = par ? bm1 : bm0;
+    int2* lcur = par ? lst1 : lst0;
+    const ClNext nx{par ? bm0 : bm1, cshift, rc[q_next], par ? lst0 : lst1, &lcnt[q_next],
+                    &ovf[q_next], lst_cap};
+    if (tid < 16) rc[q_free][tid] = 0;  // read a level ago; added to from the next level on
+    if (tid == 0) {
+      lcnt[q_free] = 0;
+      ovf[q_free] = 0;
+    }
+    // every warp: the level total and this CTA's offset from the counts
+    const int x = lane < S ? rc[q_now][lane] : 0;
+    const int before = __reduce_add_sync(FULL, lane < r ? x : 0);
+    const int total = __reduce_add_sync(FULL, x);
+    if (total == 0) break;  // uniform: every CTA read the same counts
+    const int run = emitted + before;
+    const int m = lcnt[q_now];          // appended before the cluster barrier
+    const bool over = ovf[q_now] != 0;  // likewise; the same in every CTA
+    LV_PHASE(3);
+    // the emission writes the range's pins in ascending order into `order`
+    // with their level and clears the words for reuse two levels on
+    auto emit = [&](int pos) {
+      for (int i = i0; i < i1; ++i) {
+        unsigned bits = cur[i - r * C];
+        while (bits) {
+          const int bit = __ffs(bits) - 1;
+          bits &= bits - 1;
+          const int v = (i << 5) + bit;
+          if (pos < n) order[pos] = v;
+          else atomicCAS(&ctl->status, 0, (int)OTG_ERR_INVALID);  // duplicate seeds
+          ++pos;
+          level[v] = L;
+        }
+        cur[i - r * C] = 0u;
+      }
+    };
+    int pc = 0;
+    for (int i = i0; i < i1; ++i) pc += __popc(cur[i - r * C]);
+    constexpr int W = CT / 32;
+    if (!over && m <= CT) {
+      // the common level, one list entry per thread: ONE block scan serves
+      // both the emission (popcounts) and the expansion (fanin counts).  An
+      // edge q finds its warp by a shuffle search over the warps' edge
+      // totals, then its entry by a binary search over that warp's
+      // exclusive starts; the emission runs while the first fanin loads
+      // are in flight.
+      const int2 en = tid < m ? lcur[tid] : make_int2(0, 0);
+      int y1 = en.y, y2 = pc;
+#pragma unroll
+      for (int d = 1; d < 32; d <<= 1) {
+        const int z1 = __shfl_up_sync(FULL, y1, d), z2 = __shfl_up_sync(FULL, y2, d);
+        if (lane >= d) {
+          y1 += z1;
+          y2 += z2;
+        }
+      }
+      s_excl[tid] = y1 - en.y;
+      s_e0[tid] = en.x;
+      if (lane == 31) {
+        wsum[par][w] = y1;
+        wsum[par][W + w] = y2;
+      }
+      __syncthreads();
+      const int tE = lane < W ? wsum[par][lane] : 0;
+      const int tP = lane < W ? wsum[par][W + lane] : 0;
+      const int wbP = __reduce_add_sync(FULL, lane < w ? tP : 0);
+      int inclE = tE;  // lane u: edges of warps 0..u
+#pragma unroll
+      for (int d = 1; d < 32; d <<= 1) {
+        const int z = __shfl_up_sync(FULL, inclE, d);
+        if (lane >= d) inclE += z;
+      }
+      const int etot = __shfl_sync(FULL, inclE, 31);
+      bool pending = true;
+      for (int q0 = 0; q0 < etot; q0 += CT) {
+        const int q = q0 + tid;
+        const int qc = min(q, etot - 1);  // every lane searches (the shuffles are warp-wide)
+        int u = 0;                        // warps whose edges all lie before qc
+#pragma unroll
+        for (int step = 16; step >= 1; step >>= 1) {
+          const int ic = __shfl_sync(FULL, inclE, (u + step - 1) & 31);
+          if (ic <= qc) u += step;
+        }
+        const int base = __shfl_sync(FULL, inclE, (u - 1) & 31);
+        const int ql = qc - (u > 0 ? base : 0);
+        const int* xs = s_excl + u * 32;
+        int j = 0;  // the last entry of warp u whose start is <= ql
+#pragma unroll
+        for (int step = 16; step >= 1; step >>= 1)
+          if (xs[j + step] <= ql) j += step;
+        const int v = q < etot ? fanin[s_e0[u * 32 + j] + (ql - xs[j])] : -1;
+        if (pending) {
+          emit(run + wbP + y2 - pc);
+          pending = false;
+        }
+        decrement_cl(v, (unsigned)v < (unsigned)n, fanin_start, cnt, nx, cl);
+      }
+      if (pending) emit(run + wbP + y2 - pc);
+      LV_PHASE(1);
+    } else {
+      // a longer list, or a list overflowed last level
+      int y2 = pc;
+#pragma unroll
+      for (int d = 1; d < 32; d <<= 1) {
+        const int z2 = __shfl_up_sync(FULL, y2, d);
+        if (lane >= d) y2 += z2;
+      }
+      if (lane == 31) wsum[par][W + w] = y2;
+      __syncthreads();
+      const int tP = lane < W ? wsum[par][W + lane] : 0;
+      const int wbP = __reduce_add_sync(FULL, lane < w ? tP : 0);
+      const int tt = min(__reduce_add_sync(FULL, tP), n - run);
+      emit(run + wbP + y2 - pc);
+      if (!over) {
+        expand_warps<CT>(m, [&](int k) { return lcur[k]; }, fanin_start, fanin, cnt, n, nx, cl);
+      } else {
+        // every CTA expands its own range's pins of this level, read back
+        // from `order`, their fanin ranges from global memory
+        __syncthreads();  // this range's slice of `order` is written
+        expand_warps<CT>(
+            tt,
+            [&](int k) {
+              const int u = __ldcg(order + run + k);
+              const int e0 = fanin_start[u];
+              return make_int2(e0, fanin_start[u + 1] - e0);
+            },
+            fanin_start, fanin, cnt, n, nx, cl);
+      }
+    }
+    emitted += total;
+    if (emitted > n) {  // only reachable with duplicate seeds; stop cleanly
+      if (gtid == 0) atomicCAS(&ctl->status, 0, (int)OTG_ERR_INVALID);
+      emitted = n;
+      break;
+    }
+    if (gtid == 0) level_ends[L + 1] = emitted;
+    ++L;
+    const int q = q_free;
+    q_free = q_now;
+    q_now = q_next;
+    q_next = q;
+    LV_PHASE(2);
+  }
+  if (gtid == 0) {
+    counts[0] = L;
+    counts[1] = emitted;
+  }
+  LV_PHASE_END(counts);
+  cl.sync();  // no CTA leaves while another may still read its counts
+}
+
+// Dynamic shared memory of the cluster path: both bitmaps (C words each)
+// and two lists of at least kLstMin fanin ranges (8 bytes each); the lists
+// take what is left of kClusterSmemMax.
+constexpr size_t kClusterSmemMax = 200 * 1024;
+constexpr int kLstMin = kCtMax;
+size_t lv_cluster_smem(int C) { return (size_t)(2 * C + 4 * kLstMin) * 4; }
+int lv_lst_cap(int C) { return ((int)(kClusterSmemMax / 4) - 2 * C) / 4; }
+
+constexpr int kWidths[4] = {128, 256, 512, 1024};
+const void* cluster_fn(int wi) {
+  switch (wi) {
+    case 0: return (const void*)levelize_cluster_kernel<128>;
+    case 1: return (const void*)levelize_cluster_kernel<256>;
+    case 2: return (const void*)levelize_cluster_kernel<512>;
+    default: return (const void*)levelize_cluster_kernel<1024>;
+  }
+}
+
 struct LvDev {
   int sms = 0;
   int occ = 0;
   bool init = false;
+  int max_cluster[4] = {0, 0, 0, 0};  // per CTA width: largest cluster (power of two <= 16) placed
 };
 LvDev g_lv[64];
 
@@ -293,9 +686,83 @@ LvDev& lv_dev() {
     cudaDeviceGetAttribute(&x.sms, cudaDevAttrMultiProcessorCount, d);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&x.occ, levelize_kernel, LT, 0);
     x.occ = std::max(1, std::min(x.occ, 2));
+    // the cluster path: allow its largest shared memory and 16-CTA clusters,
+    // then keep, per CTA width, the largest cluster size the device places
+    for (int wi = 0; wi < 4; ++wi) {
+      const void* fn = cluster_fn(wi);
+      if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)kClusterSmemMax) != cudaSuccess ||
+          cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
+              cudaSuccess)
+        continue;
+      for (int s = 16; s >= 1 && !x.max_cluster[wi]; s >>= 1) {
+        cudaLaunchConfig_t cfg = {};
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = (unsigned)s;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.gridDim = dim3(s);
+        cfg.blockDim = dim3(kWidths[wi]);
+        cfg.dynamicSmemBytes = kClusterSmemMax;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        int nc = 0;
+        if (cudaOccupancyMaxActiveClusters(&nc, fn, &cfg) == cudaSuccess && nc >= 1)
+          x.max_cluster[wi] = s;
+      }
+    }
+    cudaGetLastError();  // a refused attribute or query leaves no sticky error
     x.init = true;
   }
   return x;
+}
+
+// The cluster path's shape for an n-pin graph: S CTAs of kWidths[wi]
+// threads, each owning 2^cshift bitmap words.  S = 0: the cooperative path.
+struct ClPlan {
+  int S = 0, wi = 0, cshift = 0;
+};
+// Default: the largest cluster the device places (16 CTAs on B200) of 256
+// threads each, for graphs whose ranges then hold at most kClusterMaxWords
+// words (about a million pins) and whose seed level has at most
+// kClusterMaxSeed pins.  Larger graphs, and graphs whose wide seed level
+// announces wide levels, take the cooperative path, which spreads a level
+// over every SM.  On B200: a 165k-pin graph of 600 levels took 1.84 ms in
+// the cluster path and 3.61 ms in the cooperative one, one of 1M pins and
+// 2000 levels 13.3 and 15.3 ms; one of 100k pins in 3 levels 0.25 and
+// 0.07 ms.  OTG_LEVELIZE_CLUSTER=0
+// turns the cluster path off, =1|2|4|8|16 asks for that size;
+// OTG_LEVELIZE_CT=128|256|512|1024 asks for that width (both only where
+// the graph fits and the device places the cluster).
+constexpr int kClusterMaxWords = 2048;
+constexpr int kClusterMaxSeed = 8192;
+ClPlan lv_cluster_plan(int n, int first_size, const LvDev& d) {
+  ClPlan p;
+  const int nw = std::max(1, (n + 31) / 32);
+  p.wi = 1;
+  if (const char* e = std::getenv("OTG_LEVELIZE_CT")) {
+    const int want = std::atoi(e);
+    for (int wi = 0; wi < 4; ++wi)
+      if (kWidths[wi] == want) p.wi = wi;
+  }
+  const int maxc = d.max_cluster[p.wi];
+  if (maxc < 1) return ClPlan{};
+  int s = maxc;
+  if (const char* e = std::getenv("OTG_LEVELIZE_CLUSTER")) {
+    const int want = std::atoi(e);
+    if (want <= 0) return ClPlan{};
+    s = 1;
+    while (s < want && s < maxc) s <<= 1;
+  } else if ((nw + s - 1) / s > kClusterMaxWords || first_size > kClusterMaxSeed) {
+    return ClPlan{};  // large or wide graphs: the whole GPU (the cooperative path)
+  }
+  int cs = 0;
+  while ((1 << cs) * s < nw) ++cs;
+  if (lv_cluster_smem(1 << cs) > kClusterSmemMax) return ClPlan{};
+  p.S = s;
+  p.cshift = cs;
+  return p;
 }
 
 size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
@@ -346,6 +813,34 @@ otg_status otg_levelize(int32_t n, int32_t num_edges, const int32_t* fanin_start
   const otg::LvWs l = otg::lv_ws(n, G);
   if (workspace_bytes < l.total) return OTG_ERR_WORKSPACE;
   const int nw = (n + 31) / 32;
+  const otg::ClPlan pl = otg::lv_cluster_plan(n, first_size, d);
+  if (pl.S > 0) {
+    char* ws = (char*)workspace;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (cudaMemsetAsync(ws + l.ctl, 0, sizeof(otg::LvCtl), s) != cudaSuccess) return OTG_ERR_CUDA;
+    otg::LvCtl* ctl = (otg::LvCtl*)(ws + l.ctl);
+    int* cnt = (int*)(ws + l.cnt);
+    int cshift = pl.cshift;
+    int lst_cap = otg::lv_lst_cap(1 << pl.cshift);
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = (unsigned)pl.S;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.gridDim = dim3(pl.S);
+    cfg.blockDim = dim3(otg::kWidths[pl.wi]);
+    cfg.dynamicSmemBytes = otg::kClusterSmemMax;
+    cfg.stream = s;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    void* args[] = {&n,          (void*)&fanin_start, (void*)&fanin, (void*)&out_deg,
+                    (void*)&frontier0, &first_size, &order, &level, &level_ends, &counts,
+                    &ctl,        &cnt,        &cshift,       &lst_cap};
+    const cudaError_t e = cudaLaunchKernelExC(&cfg, otg::cluster_fn(pl.wi), args);
+    otg::count_launch();
+    return e == cudaSuccess ? OTG_OK : OTG_ERR_CUDA;
+  }
   // Small graphs take fewer CTAs: a range of at least kWordsPerCta bitmap
   // words each, so that fewer CTAs meet at every level's grid barrier.  On a
   // 165k-pin, 600-level graph, 81 CTAs took 4.16 ms where 296 took 4.50

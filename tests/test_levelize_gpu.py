@@ -35,7 +35,7 @@ def check_vs_oracle(cuda, fs, fi, od, f0):
 
 
 @pytest.mark.parametrize("seed,n,e,L", [(1, 1000, 2500, 10), (2, 20000, 48000, 60),
-                                        (3, 200000, 480000, 200)])
+                                        (3, 200000, 480000, 200), (4, 100000, 240000, 3)])
 def test_random_dags(cuda, seed, n, e, L):
     fs, fi, od, f0 = rcgen.pin_dag(seed, n, e, L)
     check_vs_oracle(cuda, fs, fi, od, f0)
@@ -106,3 +106,21 @@ def test_host_path_and_reference_symbol(cuda):
     assert np.array_equal(order, o_order) and np.array_equal(ends, o_ends)
     # drop-in toposort_compute_cuda needs a std::vector<int>&: exercised
     # through a tiny C++ shim in the C++ integration test instead.
+
+
+@pytest.mark.parametrize("seed,n,e,L", [(5, 100000, 240000, 3), (6, 60000, 120000, 400)])
+def test_every_path_same_levels(cuda, monkeypatch, seed, n, e, L):
+    """The cluster path (one thread-block cluster, ready bitmaps in
+    distributed shared memory) and the cooperative path give identical
+    outputs, at every cluster size and CTA width.  A cluster of one CTA on
+    the 3-level graph readies more pins per level than its on-chip list of
+    fanin ranges holds, so the next level takes the overflow expansion."""
+    fs, fi, od, f0 = rcgen.pin_dag(seed, n, e, L)
+    ref = None
+    for cl, ct in (("0", "256"), ("1", "256"), ("4", "128"), ("16", "256"), ("16", "1024")):
+        monkeypatch.setenv("OTG_LEVELIZE_CLUSTER", cl)
+        monkeypatch.setenv("OTG_LEVELIZE_CT", ct)
+        out = check_vs_oracle(cuda, fs, fi, od, f0)
+        if ref is None:
+            ref = out
+        assert all(np.array_equal(a, b) for a, b in zip(out, ref)), (cl, ct)
