@@ -108,10 +108,10 @@ __host__ __device__ inline uint32_t rc_max3(uint32_t a, uint32_t b, uint32_t c) 
   return a > b ? (a > c ? a : c) : (b > c ? b : c);
 }
 
-__host__ __device__ inline RcLayout rc_layout(int n, int T, int K, int ib) {
+__host__ __device__ inline RcLayout rc_layout(int n, int T, int K, int ib, int S = 1) {
   RcLayout l;
   const uint32_t N = (uint32_t)n, M = n > 0 ? (uint32_t)(n - 1) : 0u, A = 2u * M;
-  const uint32_t W = (uint32_t)T / 32u;
+  const uint32_t W = (uint32_t)(S * T) / 32u;  // warps of the group (S CTAs of T threads)
   (void)K;
   const uint32_t I = (uint32_t)ib;
   l.ns_cap = 2u * (A / (uint32_t)kSplit) + 64u;

@@ -25,6 +25,7 @@
 //     down the Euler tour (path sums: delay, beta).
 //
 // BFS order is bit-exact with the reference: (distance asc, local id desc).
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -42,6 +43,7 @@ namespace otg {
 namespace {
 
 constexpr unsigned FULL = 0xffffffffu;
+namespace cg = cooperative_groups;
 
 // ------------------------------------------------------------------ args
 
@@ -382,120 +384,6 @@ __device__ __forceinline__ int block_excl_scan(int v, int& total, int* wsum) {
   return base + x - v;
 }
 
-// Exclusive scan over `count` items: val(i) gives item i, out(i, prefix, v)
-// receives it.  K consecutive items per thread per tile.  Returns the total.
-template <int T, int K, class ValF, class OutF>
-__device__ int block_scan_items(int count, ValF val, OutF out, int* wsum) {
-  int carry = 0;
-  for (int base = 0; base < count; base += T * K) {
-    int v[K];
-    int local = 0;
-    const int i0 = base + threadIdx.x * K;
-#pragma unroll
-    for (int k = 0; k < K; ++k) {
-      v[k] = (i0 + k < count) ? val(i0 + k) : 0;
-      local += v[k];
-    }
-    int tot;
-    int run = carry + block_excl_scan<T>(local, tot, wsum);
-#pragma unroll
-    for (int k = 0; k < K; ++k) {
-      if (i0 + k < count) out(i0 + k, run, v[k]);
-      run += v[k];
-    }
-    carry += tot;
-  }
-  return carry;
-}
-
-// Stable LSD radix sort of the items 0..N-1 by key(i) (nbits bits,
-// rc_radix_bits(T) bits per pass).  The final order lands in `out`
-// (out[rank] = item); b0/b1 are ping-pong buffers of N entries; hist holds
-// (1 << rc_radix_bits(T)) * (T/32) ints.  Each
-// warp owns a contiguous range of the current sequence, so ranks inside a
-// warp follow sequence order (match_any + popc) and the digit-major scan of
-// the per-warp counts keeps the sort stable.
-template <int T, class Ix, class KeyF>
-__device__ void block_radix_sort(int N, int nbits, KeyF key, Ix* b0, Ix* b1, Ix* out, int* hist,
-                                 int* wsum) {
-  constexpr int W = T / 32;
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const unsigned lt = (1u << lane) - 1u;
-  const int per = ((N + W - 1) / W + 31) & ~31;
-  constexpr int DB = rc_radix_bits(T);
-  if (nbits < 1) nbits = 1;
-  const int passes = (nbits + DB - 1) / DB;
-  for (int p = 0; p < passes; ++p) {
-    const int shift = DB * p;
-    const int db = min(DB, nbits - shift);
-    const int nb = 1 << db;
-    const unsigned mask = (unsigned)nb - 1u;
-    const Ix* src = (p == 0) ? nullptr : ((p - 1) % 2 == 0 ? b0 : b1);
-    Ix* dst = (p == passes - 1) ? out : (p % 2 == 0 ? b0 : b1);
-    for (int i = threadIdx.x; i < nb * W; i += T) hist[i] = 0;
-    __syncthreads();
-    for (int j = 0; j < per; j += 32) {
-      const int idx = w * per + j + lane;
-      const bool valid = idx < N;
-      const int item = valid ? (src ? (int)src[idx] : idx) : 0;
-      const int d = valid ? (int)(((unsigned)key(item) >> shift) & mask) : (256 + lane);
-      const unsigned peers = __match_any_sync(FULL, d);
-      if (valid && (__ffs(peers) - 1 == lane)) hist[d * W + w] += __popc(peers);
-      __syncwarp();
-    }
-    __syncthreads();
-    block_scan_items<T, 4>(
-        nb * W, [&](int i) { return hist[i]; }, [&](int i, int pre, int) { hist[i] = pre; },
-        wsum);
-    __syncthreads();
-    for (int j = 0; j < per; j += 32) {
-      const int idx = w * per + j + lane;
-      const bool valid = idx < N;
-      const int item = valid ? (src ? (int)src[idx] : idx) : 0;
-      const int d = valid ? (int)(((unsigned)key(item) >> shift) & mask) : (256 + lane);
-      const unsigned peers = __match_any_sync(FULL, d);
-      const int base = valid ? hist[d * W + w] : 0;
-      __syncwarp();
-      if (valid) {
-        dst[base + __popc(peers & lt)] = (Ix)item;
-        if (__ffs(peers) - 1 == lane) hist[d * W + w] = base + __popc(peers);
-      }
-      __syncwarp();
-    }
-    __syncthreads();
-  }
-}
-
-__device__ __forceinline__ float2 f2mul(float2 a, float2 b) { return make_float2(a.x * b.x, a.y * b.y); }
-__device__ __forceinline__ float2 f2scale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
-
-// ------------------------------------------------ exact fixed-point sums
-// Every fp32 term x of a sweep is mapped to the integer rint(x * 2^s), with
-// one power of two per net, corner and sweep chosen from n * max|x| so that
-// no partial sum reaches 2^62.  int64 sums of those integers are exact, so
-// a subtree sum taken as a difference of two prefixes has no cancellation
-// error and no result depends on the order of the terms -- the tour may
-// visit children in any order and every output is still bit-reproducible.
-// Each term is rounded once to a grid of 2^-s (relative to n * max|x| that
-// is 2^-61), each result once back to fp32.
-
-__device__ __forceinline__ float pow2f(int e) { return __int_as_float((e + 127) << 23); }
-
-// 2^s and 2^-s for terms with |x| <= mx over n positions.
-__device__ __forceinline__ void fx_scale(float mx, int n, float& up, float& dn) {
-  const float bound = mx * (float)n;
-  int s = 0;
-  if (bound > 0.f) {
-    // bound < 2^e with e from the exponent field; s leaves one bit of margin
-    const int e = ((__float_as_int(bound) >> 23) & 0xff) - 126;
-    s = min(max(61 - e, -126), 126);
-  }
-  up = pow2f(s);
-  dn = pow2f(-s);
-}
-__device__ __forceinline__ long long to_fx(float x, float up) { return __float2ll_rn(x * up); }
-__device__ __forceinline__ float from_fx(long long v, float dn) { return __ll2float_rn(v) * dn; }
-
 // Warp-inclusive int64 scan of two values; ex gets the warp-exclusive prefix.
 __device__ __forceinline__ void warp_i64_scan2(long long (&v)[2], long long (&ex)[2]) {
   const int lane = threadIdx.x & 31;
@@ -540,13 +428,232 @@ __device__ __forceinline__ void tile_i64_bases(const long long (&v)[2], long lon
   }
 }
 
+// ---- thread groups of the block path.  A net of the block path is run by
+// a group of threads: one CTA (CtaGroup), or -- for nets above the shared-
+// memory classes -- a thread-block cluster of S CTAs acting as one virtual
+// block over the net's global-memory workspace slice (ClusterGroup).  The
+// group gives each thread its rank, its barrier and an exclusive scan; the
+// net's shared scalars (error flag, maximum depth, sweep maxima) live in
+// the shared memory of the group's first CTA.
+template <int T>
+struct CtaGroup {
+  int* flag = nullptr;
+  int* maxd = nullptr;
+  unsigned* smx = nullptr;
+  __device__ static constexpr int vt() { return T; }
+  __device__ int rank() const { return (int)threadIdx.x; }
+  __device__ void sync() const { __syncthreads(); }
+  __device__ int excl_scan(int v, int& total, int* wsum) const {
+    return block_excl_scan<T>(v, total, wsum);
+  }
+  __device__ void i64_bases(const long long (&v)[2], long long (&wb)[2], long long (&tt)[2],
+                            long long* shl) const {
+    tile_i64_bases<T>(v, wb, tt, shl);
+  }
+};
+
+template <int T>
+struct ClusterGroup {
+  int S = 1, r = 0;         // CTAs in the cluster, this CTA's rank
+  int* flag = nullptr;      // in rank 0's shared memory
+  int* maxd = nullptr;
+  unsigned* smx = nullptr;
+  long long* xch = nullptr;  // this CTA's exchange slot [2] (its own shared memory)
+  __device__ int vt() const { return S * T; }
+  __device__ int rank() const { return r * T + (int)threadIdx.x; }
+  // The cluster barrier orders the workspace writes of every CTA (release
+  // at arrive, acquire at wait); the fence after it also keeps each SM from
+  // serving a later read of the workspace from a line it cached before.
+  __device__ void sync() const {
+    cg::this_cluster().sync();
+    __threadfence();
+  }
+  // the CTAs' totals of a pair of values: this CTA's exclusive base and the
+  // group total (two cluster barriers: publish, then free the slot again)
+  __device__ void cta_bases(long long t0, long long t1, long long (&base)[2],
+                            long long (&tot)[2]) const {
+    const cg::cluster_group cl = cg::this_cluster();
+    if (threadIdx.x == 0) {
+      xch[0] = t0;
+      xch[1] = t1;
+    }
+    cl.sync();
+    const int lane = threadIdx.x & 31;
+    long long x0 = 0, x1 = 0;
+    if (lane < S) {
+      const long long* o = cl.map_shared_rank(xch, lane);
+      x0 = o[0];
+      x1 = o[1];
+    }
+    long long b0 = lane < r ? x0 : 0, b1 = lane < r ? x1 : 0;
+#pragma unroll
+    for (int d = 16; d >= 1; d >>= 1) {
+      x0 += __shfl_xor_sync(FULL, x0, d);
+      x1 += __shfl_xor_sync(FULL, x1, d);
+      b0 += __shfl_xor_sync(FULL, b0, d);
+      b1 += __shfl_xor_sync(FULL, b1, d);
+    }
+    base[0] = b0;
+    base[1] = b1;
+    tot[0] = x0;
+    tot[1] = x1;
+    cl.sync();
+  }
+  __device__ int excl_scan(int v, int& total, int* wsum) const {
+    int t_cta;
+    const int e = block_excl_scan<T>(v, t_cta, wsum);
+    long long base[2], tot[2];
+    cta_bases(t_cta, 0, base, tot);
+    total = (int)tot[0];
+    return (int)base[0] + e;
+  }
+  __device__ void i64_bases(const long long (&v)[2], long long (&wb)[2], long long (&tt)[2],
+                            long long* shl) const {
+    long long cw[2], ct[2];
+    tile_i64_bases<T>(v, cw, ct, shl);
+    __syncthreads();  // shl is reused by the next tile only after every warp read it
+    long long base[2], tot[2];
+    cta_bases(ct[0], ct[1], base, tot);
+    wb[0] = base[0] + cw[0];
+    wb[1] = base[1] + cw[1];
+    tt[0] = tot[0];
+    tt[1] = tot[1];
+  }
+};
+
+// Exclusive scan over `count` items: val(i) gives item i, out(i, prefix, v)
+// receives it.  K consecutive items per thread per tile.  Returns the total.
+template <int K, class G, class ValF, class OutF>
+__device__ int group_scan_items(const G& g, int count, ValF val, OutF out, int* wsum) {
+  int carry = 0;
+  const int VT = g.vt();
+  for (int base = 0; base < count; base += VT * K) {
+    int v[K];
+    int local = 0;
+    const int i0 = base + g.rank() * K;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      v[k] = (i0 + k < count) ? val(i0 + k) : 0;
+      local += v[k];
+    }
+    int tot;
+    int run = carry + g.excl_scan(local, tot, wsum);
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      if (i0 + k < count) out(i0 + k, run, v[k]);
+      run += v[k];
+    }
+    carry += tot;
+  }
+  return carry;
+}
+template <int T, int K, class ValF, class OutF>
+__device__ int block_scan_items(int count, ValF val, OutF out, int* wsum) {
+  return group_scan_items<K>(CtaGroup<T>{}, count, val, out, wsum);
+}
+
+// Stable LSD radix sort of the items 0..N-1 by key(i) (nbits bits,
+// rc_radix_bits(T) bits per pass) over the group's threads.  The final
+// order lands in `out` (out[rank] = item); b0/b1 are ping-pong buffers of N
+// entries; hist holds (1 << rc_radix_bits(T)) * (the group's warps) ints.
+// Each warp owns a contiguous range of the current sequence, so ranks
+// inside a warp follow sequence order (match_any + popc) and the
+// digit-major scan of the per-warp counts keeps the sort stable.
+template <int T, class G, class Ix, class KeyF>
+__device__ void group_radix_sort(const G& g, int N, int nbits, KeyF key, Ix* b0, Ix* b1, Ix* out,
+                                 int* hist, int* wsum) {
+  const int VT = g.vt(), W = VT / 32;
+  const int lane = threadIdx.x & 31, w = g.rank() >> 5;
+  const unsigned lt = (1u << lane) - 1u;
+  const int per = ((N + W - 1) / W + 31) & ~31;
+  constexpr int DB = rc_radix_bits(T);
+  if (nbits < 1) nbits = 1;
+  const int passes = (nbits + DB - 1) / DB;
+  for (int p = 0; p < passes; ++p) {
+    const int shift = DB * p;
+    const int db = min(DB, nbits - shift);
+    const int nb = 1 << db;
+    const unsigned mask = (unsigned)nb - 1u;
+    const Ix* src = (p == 0) ? nullptr : ((p - 1) % 2 == 0 ? b0 : b1);
+    Ix* dst = (p == passes - 1) ? out : (p % 2 == 0 ? b0 : b1);
+    for (int i = g.rank(); i < nb * W; i += VT) hist[i] = 0;
+    g.sync();
+    for (int j = 0; j < per; j += 32) {
+      const int idx = w * per + j + lane;
+      const bool valid = idx < N;
+      const int item = valid ? (src ? (int)src[idx] : idx) : 0;
+      const int d = valid ? (int)(((unsigned)key(item) >> shift) & mask) : (256 + lane);
+      const unsigned peers = __match_any_sync(FULL, d);
+      if (valid && (__ffs(peers) - 1 == lane)) hist[d * W + w] += __popc(peers);
+      __syncwarp();
+    }
+    g.sync();
+    group_scan_items<4>(
+        g, nb * W, [&](int i) { return hist[i]; }, [&](int i, int pre, int) { hist[i] = pre; },
+        wsum);
+    g.sync();
+    for (int j = 0; j < per; j += 32) {
+      const int idx = w * per + j + lane;
+      const bool valid = idx < N;
+      const int item = valid ? (src ? (int)src[idx] : idx) : 0;
+      const int d = valid ? (int)(((unsigned)key(item) >> shift) & mask) : (256 + lane);
+      const unsigned peers = __match_any_sync(FULL, d);
+      const int base = valid ? hist[d * W + w] : 0;
+      __syncwarp();
+      if (valid) {
+        dst[base + __popc(peers & lt)] = (Ix)item;
+        if (__ffs(peers) - 1 == lane) hist[d * W + w] = base + __popc(peers);
+      }
+      __syncwarp();
+    }
+    g.sync();
+  }
+}
+template <int T, class Ix, class KeyF>
+__device__ void block_radix_sort(int N, int nbits, KeyF key, Ix* b0, Ix* b1, Ix* out, int* hist,
+                                 int* wsum) {
+  group_radix_sort<T>(CtaGroup<T>{}, N, nbits, key, b0, b1, out, hist, wsum);
+}
+
+__device__ __forceinline__ float2 f2mul(float2 a, float2 b) { return make_float2(a.x * b.x, a.y * b.y); }
+__device__ __forceinline__ float2 f2scale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
+
+// ------------------------------------------------ exact fixed-point sums
+// Every fp32 term x of a sweep is mapped to the integer rint(x * 2^s), with
+// one power of two per net, corner and sweep chosen from n * max|x| so that
+// no partial sum reaches 2^62.  int64 sums of those integers are exact, so
+// a subtree sum taken as a difference of two prefixes has no cancellation
+// error and no result depends on the order of the terms -- the tour may
+// visit children in any order and every output is still bit-reproducible.
+// Each term is rounded once to a grid of 2^-s (relative to n * max|x| that
+// is 2^-61), each result once back to fp32.
+
+__device__ __forceinline__ float pow2f(int e) { return __int_as_float((e + 127) << 23); }
+
+// 2^s and 2^-s for terms with |x| <= mx over n positions.
+__device__ __forceinline__ void fx_scale(float mx, int n, float& up, float& dn) {
+  const float bound = mx * (float)n;
+  int s = 0;
+  if (bound > 0.f) {
+    // bound < 2^e with e from the exponent field; s leaves one bit of margin
+    const int e = ((__float_as_int(bound) >> 23) & 0xff) - 126;
+    s = min(max(61 - e, -126), 126);
+  }
+  up = pow2f(s);
+  dn = pow2f(-s);
+}
+__device__ __forceinline__ long long to_fx(float x, float up) { return __float2ll_rn(x * up); }
+__device__ __forceinline__ float from_fx(long long v, float dn) { return __ll2float_rn(v) * dn; }
+
 // Up-sweep over n preorder slots for one corner pair: Ip[p] = exact
 // fixed-point inclusive prefix of x(0..p).  K slots per thread per tile.
-template <int T, int K, class XF>
-__device__ void up_scan_fx(int n, XF x, const float (&up)[2], longlong2* Ip, long long* shl) {
+template <int K, class G, class XF>
+__device__ void up_scan_fx(const G& g, int n, XF x, const float (&up)[2], longlong2* Ip,
+                           long long* shl) {
   long long carry[2] = {0, 0};
-  for (int base = 0; base < n; base += T * K) {
-    const int q0 = base + threadIdx.x * K;
+  const int VT = g.vt();
+  for (int base = 0; base < n; base += VT * K) {
+    const int q0 = base + g.rank() * K;
     long long loc[K][2];
     long long acc[2] = {0, 0};
 #pragma unroll
@@ -561,14 +668,14 @@ __device__ void up_scan_fx(int n, XF x, const float (&up)[2], longlong2* Ip, lon
     }
     long long ex[2], wb[2], tt[2];
     warp_i64_scan2(acc, ex);
-    tile_i64_bases<T>(acc, wb, tt, shl);
+    g.i64_bases(acc, wb, tt, shl);
     const long long b0 = carry[0] + wb[0] + ex[0], b1 = carry[1] + wb[1] + ex[1];
 #pragma unroll
     for (int k = 0; k < K; ++k)
       if (q0 + k < n) Ip[rc_pad16(q0 + k)] = make_longlong2(b0 + loc[k][0], b1 + loc[k][1]);
     carry[0] += tt[0];
     carry[1] += tt[1];
-    __syncthreads();
+    g.sync();
   }
 }
 
@@ -587,11 +694,13 @@ __device__ __forceinline__ float2 up_range_fx(const longlong2* Ip, int lo, int h
 // Inclusive prefix over A tour slots for one corner pair: x(p) is the
 // signed term of slot p; emit(p, v0, v1) receives the exact fixed-point
 // prefix (converted by the callee only where it is used).
-template <int T, int K, class XF, class EmitF>
-__device__ void down_scan_fx(int A, XF x, const float (&up)[2], EmitF emit, long long* shl) {
+template <int K, class G, class XF, class EmitF>
+__device__ void down_scan_fx(const G& g, int A, XF x, const float (&up)[2], EmitF emit,
+                             long long* shl) {
   long long carry[2] = {0, 0};
-  for (int base = 0; base < A; base += T * K) {
-    const int q0 = base + threadIdx.x * K;
+  const int VT = g.vt();
+  for (int base = 0; base < A; base += VT * K) {
+    const int q0 = base + g.rank() * K;
     long long loc[K][2];
     long long acc[2] = {0, 0};
 #pragma unroll
@@ -606,14 +715,14 @@ __device__ void down_scan_fx(int A, XF x, const float (&up)[2], EmitF emit, long
     }
     long long ex[2], wb[2], tt[2];
     warp_i64_scan2(acc, ex);
-    tile_i64_bases<T>(acc, wb, tt, shl);
+    g.i64_bases(acc, wb, tt, shl);
     const long long b0 = carry[0] + wb[0] + ex[0], b1 = carry[1] + wb[1] + ex[1];
 #pragma unroll
     for (int k = 0; k < K; ++k)
       if (q0 + k < A) emit(q0 + k, b0 + loc[k][0], b1 + loc[k][1]);
     carry[0] += tt[0];
     carry[1] += tt[1];
-    __syncthreads();
+    g.sync();
   }
 }
 
@@ -650,12 +759,13 @@ __device__ __forceinline__ bool is_splitter(int arc, int sel, int first) {
   return arc == first || (h & (((unsigned)kSplit << sel) - 1u)) == 0u;
 }
 
-template <int T, int K, class Ix>
-__device__ void rc_net_block(const RcArgs& a, int net, char* ws, int n, int* sh,
-                             long long* shl) {
+template <int T, int K, class Ix, class G>
+__device__ void rc_net_block(const RcArgs& a, int net, char* ws, int n, int* sh, long long* shl,
+                             const G& g) {
   using S = typename IxT<Ix>::S;
   constexpr unsigned NONE = IxT<Ix>::NONE;
-  const int tid = threadIdx.x;
+  const int tid = g.rank();
+  const int VT = g.vt();
   const int b = a.nodes_start[net];
   const int m = n - 1, A = 2 * m, eb = b - net;
   const RcLayout lay = rc_layout(n, T, K, (int)sizeof(Ix));
@@ -684,15 +794,15 @@ __device__ void rc_net_block(const RcArgs& a, int net, char* ws, int n, int* sh,
   float2* X = (float2*)(ws + lay.X);
   float2* Y = (float2*)(ws + lay.Y);
   longlong2* Ip = (longlong2*)(ws + lay.Ip);
-  int* wsum = sh;          // [W]
-  int* s_flag = sh + 32;   // error code
-  int* s_maxd = sh + 33;   // max depth
-  unsigned* smx = (unsigned*)(sh + 40);  // [8] per-sweep maxima (float bits)
+  int* wsum = sh;          // [W] this CTA's warp totals
+  int* s_flag = g.flag;    // error code
+  int* s_maxd = g.maxd;    // max depth
+  unsigned* smx = g.smx;   // [8] per-sweep maxima (float bits)
   const int root = a.roots[net];
   auto src = [&](int arc) -> int { return (arc & 1) ? (int)et[arc >> 1] : (int)es[arc >> 1]; };
   auto dst = [&](int arc) -> int { return (arc & 1) ? (int)es[arc >> 1] : (int)et[arc >> 1]; };
   auto fail = [&]() -> bool {
-    __syncthreads();
+    g.sync();
     const int f = *s_flag;
     if (f && tid == 0) report(a, f, net);
     return f != 0;
@@ -704,9 +814,9 @@ __device__ void rc_net_block(const RcArgs& a, int net, char* ws, int n, int* sh,
     *s_flag = ((unsigned)root >= (unsigned)n) ? OTG_ERR_INVALID : 0;
     *s_maxd = 0;
   }
-  for (int v = tid; v < n; v += T) ends[v] = 0;
-  __syncthreads();
-  for (int e = tid; e < m; e += T) {
+  for (int v = tid; v < n; v += VT) ends[v] = 0;
+  g.sync();
+  for (int e = tid; e < m; e += VT) {
     int2 ed = a.edges[eb + e];
     if ((unsigned)ed.x >= (unsigned)n || (unsigned)ed.y >= (unsigned)n) {
       *s_flag = OTG_ERR_INVALID;
@@ -720,7 +830,8 @@ __device__ void rc_net_block(const RcArgs& a, int net, char* ws, int n, int* sh,
   if (fail()) return;
   PHASE(0);
   // ---- A2: degree -> begin offsets; a node without an edge is no tree node
-  block_scan_items<T, K>(
+  group_scan_items<K>(
+        g,
       n, [&](int v) { return ends[v]; },
       [&](int v, int p, int d) {
         ends[v] = p;
@@ -733,26 +844,27 @@ __device__ void rc_net_block(const RcArgs& a, int net, char* ws, int n, int* sh,
   // decides the tour's child order, which no output depends on (the BFS
   // slots follow (depth, id), the Elmore sums are exact).  After this, node
   // v's arcs are tour[begin(v) .. ends[v]).
-  for (int arc = tid; arc < A; arc += T) tour[atomicAdd(&ends[src(arc)], 1)] = (Ix)arc;
-  __syncthreads();
+  for (int arc = tid; arc < A; arc += VT) tour[atomicAdd(&ends[src(arc)], 1)] = (Ix)arc;
+  g.sync();
   PHASE(2);
   // ---- A4: Euler-tour successor: after (u->v) comes v's next arc after (v->u)
-  for (int j = tid; j < A; j += T) posin[tour[j]] = (Ix)j;
-  __syncthreads();
+  for (int j = tid; j < A; j += VT) posin[tour[j]] = (Ix)j;
+  g.sync();
   const int first = (int)tour[root ? ends[root - 1] : 0];
-  for (int arc = tid; arc < A; arc += T) {
+  for (int arc = tid; arc < A; arc += VT) {
     const int v = dst(arc);
     int k = (int)posin[arc ^ 1] + 1;
     if (k == ends[v]) k = v ? ends[v - 1] : 0;
     const int nx = (int)tour[k];
     r2[arc] = nx == first ? (Ix)NONE : (Ix)nx;
   }
-  __syncthreads();
+  g.sync();
   PHASE(3);
   // ---- A5: tour ranking by sublists
   int sel = 0, ns = 0;
   while (true) {
-    ns = block_scan_items<T, K>(
+    ns = group_scan_items<K>(
+        g,
         A, [&](int arc) { return is_splitter(arc, sel, first) ? 1 : 0; },
         [&](int arc, int p, int f) {
           sub[arc] = (Ix)NONE;
@@ -765,8 +877,8 @@ __device__ void rc_net_block(const RcArgs& a, int net, char* ws, int n, int* sh,
     if (ns <= (int)lay.ns_cap) break;
     ++sel;  // uniform: every thread saw the same total
   }
-  __syncthreads();
-  for (int s = tid; s < ns; s += T) {
+  g.sync();
+  for (int s = tid; s < ns; s += VT) {
     int cur = (int)splarc[s];
     unsigned o = 0, next = 0xFFFFFFFFu;
     for (int step = 0; step < A; ++step) {
@@ -780,29 +892,29 @@ __device__ void rc_net_block(const RcArgs& a, int net, char* ws, int n, int* sh,
     }
     sl[s] = sl_pack(next, o);
   }
-  __syncthreads();
+  g.sync();
   {
     int rounds = 1;
     while ((1 << rounds) < ns) ++rounds;
     for (int r = 0; r <= rounds; ++r) {
-      for (int s = tid; s < ns; s += T) {
+      for (int s = tid; s < ns; s += VT) {
         const unsigned long long p = sl[s];
         if (sl_next(p) != 0xFFFFFFFFu) {
           const unsigned long long q = sl[sl_next(p)];
           sl[s] = sl_pack(sl_next(q), sl_acc(p) + sl_acc(q));
         }
       }
-      __syncthreads();
+      g.sync();
     }
   }
-  for (int s = tid; s < ns; s += T)
+  for (int s = tid; s < ns; s += VT)
     if (sl_next(sl[s]) != 0xFFFFFFFFu) *s_flag = OTG_ERR_NOT_TREE;
-  for (int arc = tid; arc < A; arc += T)
+  for (int arc = tid; arc < A; arc += VT)
     if ((unsigned)sub[arc] == NONE) *s_flag = OTG_ERR_NOT_TREE;
   if (tid == 0 && sl_acc(sl[spl[first]]) != (unsigned)A) *s_flag = OTG_ERR_NOT_TREE;
   if (fail()) return;
   // place every arc; remember each down arc's subtree size by tour slot
-  for (int arc = tid; arc < A; arc += T) {
+  for (int arc = tid; arc < A; arc += VT) {
     const int p = A - (int)sl_acc(sl[sub[arc]]) + (int)off[arc];
     const int q = A - (int)sl_acc(sl[sub[arc ^ 1]]) + (int)off[arc ^ 1];
     if ((unsigned)p >= (unsigned)A) { *s_flag = OTG_ERR_NOT_TREE; continue; }
@@ -812,8 +924,8 @@ __device__ void rc_net_block(const RcArgs& a, int net, char* ws, int n, int* sh,
   if (fail()) return;
   PHASE(4);
   // ---- A6: preorder, depth, parent, subtree size from the down arcs
-  for (int v = tid; v < n; v += T) pre[v] = (Ix)NONE;
-  __syncthreads();
+  for (int v = tid; v < n; v += VT) pre[v] = (Ix)NONE;
+  g.sync();
   if (tid == 0) {
     pre[root] = 0;
     nap[0] = (Ix)root;
@@ -822,8 +934,9 @@ __device__ void rc_net_block(const RcArgs& a, int net, char* ws, int n, int* sh,
     parent[root] = (Ix)root;
     pedge[root] = (Ix)NONE;
   }
-  __syncthreads();
-  block_scan_items<T, K>(
+  g.sync();
+  group_scan_items<K>(
+        g,
       A, [&](int p) { return r2[p] != 0 ? 1 : 0; },
       [&](int p, int ex, int down) {
         if (!down) return;
@@ -839,53 +952,54 @@ __device__ void rc_net_block(const RcArgs& a, int net, char* ws, int n, int* sh,
         atomicMax(s_maxd, d);
       },
       wsum);
-  __syncthreads();
-  for (int v = tid; v < n; v += T) {
+  g.sync();
+  for (int v = tid; v < n; v += VT) {
     const unsigned pv = (unsigned)pre[v];
     if (pv == NONE || (int)nap[pv] != v) *s_flag = OTG_ERR_NOT_TREE;
   }
   if (fail()) return;
-  for (int p = tid; p < A; p += T) {
+  for (int p = tid; p < A; p += VT) {
     const int arc = (int)tour[p];
     const bool down = r2[p] != 0;
     const int v = down ? dst(arc) : src(arc);
     code[p] = (S)(down ? (int)pre[v] + 1 : -((int)pre[v] + 1));
   }
-  __syncthreads();
+  g.sync();
   PHASE(5);
   // ---- A7: BFS slots: stable sort by depth of the ids in DESCENDING order
   {
     Ix* rs0 = r2;
     Ix* rs1 = r2 + n;
-    block_radix_sort<T>(
+    group_radix_sort<T>(
+        g,
         n, 32 - __clz(max(*s_maxd, 1)), [&](int j) { return (int)depth[n - 1 - j]; }, rs0, rs1,
         nas, hist, wsum);
-    for (int r = tid; r < n; r += T) {
+    for (int r = tid; r < n; r += VT) {
       const int v = n - 1 - (int)nas[r];
       nas[r] = (Ix)v;
       slot[v] = (Ix)r;
     }
-    __syncthreads();
+    g.sync();
   }
   PHASE(6);
   // ---- A8: topology outputs, parent resistance by preorder (read in edge
   // order, coalesced, and placed at the child's preorder slot).  From here
   // on nas[r] holds the preorder slot of BFS slot r (bpre).
   Ix* bpre = nas;
-  for (int v = tid; v < n; v += T) a.node2bfs[b + v] = (int)slot[v];
-  for (int r = tid; r < n; r += T) {
+  for (int v = tid; v < n; v += VT) a.node2bfs[b + v] = (int)slot[v];
+  for (int r = tid; r < n; r += VT) {
     const int v = (int)nas[r];
     a.pid[b + r] = r == 0 ? 0 : r - (int)slot[parent[v]];
     bpre[r] = pre[v];
   }
   if (tid == 0) pres[0] = 0.0f;
-  for (int e = tid; e < m; e += T) {
+  for (int e = tid; e < m; e += VT) {
     const int s = (int)es[e], t = (int)et[e];
     const bool down = (int)pedge[t] == e;  // t is the child of edge e
     a.edges[eb + e] = down ? make_int2(s, t) : make_int2(t, s);
     pres[(int)pre[down ? t : s]] = a.res[eb + e];
   }
-  __syncthreads();
+  g.sync();
   PHASE(7);
 
   // ---- B: Elmore, one corner pair at a time (corners 2cp, 2cp+1), with
@@ -904,35 +1018,36 @@ __device__ void rc_net_block(const RcArgs& a, int net, char* ws, int n, int* sh,
       fx_scale(__uint_as_float(smx[2 * k + 1]), n, up[1], dn[1]);
     };
     if (tid < 8) smx[tid] = 0u;
-    __syncthreads();
+    g.sync();
     m[0] = m[1] = 0.f;
-    for (int j = tid; j < n; j += T) {
+    for (int j = tid; j < n; j += VT) {
       const float2 c = cap2[2 * (size_t)(b + j) + cp];
       Y[rc_pad8((int)pre[j])] = c;
       max2_accumulate(c, m);
     }
     max2_commit(m, smx + 0);
-    __syncthreads();
+    g.sync();
     // load (up): cap summed over the subtree
     scale(0);
-    up_scan_fx<T, K>(n, [&](int i) { return Y[rc_pad8(i)]; }, up, Ip, shl);
+    up_scan_fx<K>(g, n, [&](int i) { return Y[rc_pad8(i)]; }, up, Ip, shl);
     m[0] = m[1] = 0.f;
-    for (int i = tid; i < n; i += T) {
+    for (int i = tid; i < n; i += VT) {
       const float2 v = up_range_fx(Ip, i, i + (int)size[i] - 1, dn);
       X[rc_pad8(i)] = v;
       max2_accumulate(f2scale(v, pres[i]), m);
     }
     max2_commit(m, smx + 2);
-    __syncthreads();
+    g.sync();
     out = (float2*)a.load;
-    for (int r = tid; r < n; r += T) out[2 * (size_t)(b + r) + cp] = X[rc_pad8(bpre[r])];
-    for (int i = tid; i < n; i += T) capI[2 * rc_pad16(i)] = Y[rc_pad8(i)];  // Ip is free until the ldelay sweep
-    __syncthreads();
+    for (int r = tid; r < n; r += VT) out[2 * (size_t)(b + r) + cp] = X[rc_pad8(bpre[r])];
+    for (int i = tid; i < n; i += VT) capI[2 * rc_pad16(i)] = Y[rc_pad8(i)];  // Ip is free until the ldelay sweep
+    g.sync();
     PHASE(8);
     // delay (down): +pres*load entering a node, - leaving it
     scale(1);
     if (tid == 0) Y[rc_pad8(0)] = make_float2(0.f, 0.f);
-    down_scan_fx<T, K>(
+    down_scan_fx<K>(
+        g,
         A,
         [&](int p) {
           const int c = (int)code[p];
@@ -947,35 +1062,36 @@ __device__ void rc_net_block(const RcArgs& a, int net, char* ws, int n, int* sh,
         shl);
     m[0] = m[1] = 0.f;
     out = (float2*)a.delay;
-    for (int r = tid; r < n; r += T) {
+    for (int r = tid; r < n; r += VT) {
       const int i = (int)bpre[r];
       const float2 d = Y[rc_pad8(i)];
       out[2 * (size_t)(b + r) + cp] = d;
       max2_accumulate(f2mul(capI[2 * rc_pad16(i)], d), m);
     }
     max2_commit(m, smx + 4);
-    __syncthreads();
+    g.sync();
     PHASE(9);
     // ldelay (up): cap*delay over the subtree
     scale(2);
     // each thread reads its own slots' caps before it writes their sums
-    up_scan_fx<T, K>(n, [&](int i) { return f2mul(capI[2 * rc_pad16(i)], Y[rc_pad8(i)]); }, up, Ip, shl);
+    up_scan_fx<K>(g, n, [&](int i) { return f2mul(capI[2 * rc_pad16(i)], Y[rc_pad8(i)]); }, up, Ip, shl);
     m[0] = m[1] = 0.f;
-    for (int i = tid; i < n; i += T) {
+    for (int i = tid; i < n; i += VT) {
       const float2 v = up_range_fx(Ip, i, i + (int)size[i] - 1, dn);
       X[rc_pad8(i)] = v;
       max2_accumulate(f2scale(v, pres[i]), m);
     }
     max2_commit(m, smx + 6);
-    __syncthreads();
+    g.sync();
     out = (float2*)a.ldelay;
-    for (int r = tid; r < n; r += T) out[2 * (size_t)(b + r) + cp] = X[rc_pad8(bpre[r])];
+    for (int r = tid; r < n; r += VT) out[2 * (size_t)(b + r) + cp] = X[rc_pad8(bpre[r])];
     PHASE(10);
     // beta (down) -> impulse = 2*beta - delay^2, kept where Ip was
     scale(3);
     float2* imp = (float2*)Ip;
     if (tid == 0) imp[2 * rc_pad16(0)] = make_float2(0.f, 0.f);
-    down_scan_fx<T, K>(
+    down_scan_fx<K>(
+        g,
         A,
         [&](int p) {
           const int c = (int)code[p];
@@ -993,19 +1109,19 @@ __device__ void rc_net_block(const RcArgs& a, int net, char* ws, int n, int* sh,
         },
         shl);
     out = (float2*)a.impulse;
-    for (int r = tid; r < n; r += T) out[2 * (size_t)(b + r) + cp] = imp[2 * rc_pad16(bpre[r])];
+    for (int r = tid; r < n; r += VT) out[2 * (size_t)(b + r) + cp] = imp[2 * rc_pad16(bpre[r])];
     if (a.sinks_start) {
       const int s0 = a.sinks_start[net], s1 = a.sinks_start[net + 1];
       const float2 si = ((const float2*)a.driver_slew)[2 * (size_t)net + cp];
       float2* so = (float2*)a.sink_slew;
-      for (int k = s0 + tid; k < s1; k += T) {
+      for (int k = s0 + tid; k < s1; k += VT) {
         const int v = a.sink_nodes[k];
         if ((unsigned)v >= (unsigned)n) { report(a, OTG_ERR_INVALID, net); continue; }
         const float2 iv = imp[2 * rc_pad16(pre[v])];
         so[2 * (size_t)k + cp] = make_float2(sink_slew1(si.x, iv.x), sink_slew1(si.y, iv.y));
       }
     }
-    __syncthreads();
+    g.sync();
     PHASE(11);
   }
 }
@@ -1017,9 +1133,12 @@ __host__ __device__ inline uint32_t rc_smem_bytes(int n, int T, int K, bool tile
   return tile ? rc_tile_layout(n, T).total : rc_layout(n, T, K, 2).total;
 }
 
+// `few`: a class of at most this many items is left to the cluster kernel
+// (the huge-net class; 0 elsewhere).
 template <int T, int K, class Ix, bool SMEM, bool TILE = false>
 __global__ void __launch_bounds__(T) rc_block_kernel(RcJob job, const int* list, const int* count,
-                                                     int* work, char* gws, size_t ws_stride) {
+                                                     int* work, char* gws, size_t ws_stride,
+                                                     int few) {
   extern __shared__ __align__(16) char dsm[];
   __shared__ int sh[96];
   __shared__ long long shl[4 * (T / 32) + 4];
@@ -1027,6 +1146,7 @@ __global__ void __launch_bounds__(T) rc_block_kernel(RcJob job, const int* list,
   __shared__ RcArgs s_args;  // the current net's forest
   char* ws = SMEM ? dsm : gws + (size_t)blockIdx.x * ws_stride;
   const int cnt = *count;
+  if (cnt <= few) return;
   while (true) {
     if (threadIdx.x == 0) {
       const int item = atomicAdd(work, 1);
@@ -1044,8 +1164,54 @@ __global__ void __launch_bounds__(T) rc_block_kernel(RcJob job, const int* list,
     if (item >= cnt) break;
     const int n = s_args.nodes_start[net + 1] - s_args.nodes_start[net];
     if constexpr (TILE) rc_net_tile<T>(s_args, net, ws, n, sh, shl);
-    else rc_net_block<T, K, Ix>(s_args, net, ws, n, sh, shl);
+    else rc_net_block<T, K, Ix>(s_args, net, ws, n, sh, shl,
+                                CtaGroup<T>{sh + 32, sh + 33, (unsigned*)(sh + 40)});
     __syncthreads();
+  }
+}
+
+// Nets above the shared-memory classes, one thread-block cluster per net:
+// the cluster's S CTAs run rc_net_block as ONE virtual block of S*T
+// threads over the cluster's workspace slice (32-bit indices), with the
+// cluster barrier between phases and the CTAs' scan totals exchanged
+// through distributed shared memory.  Items go to the clusters in turn
+// (cluster c takes items c, c + C, c + 2C, ...), so every CTA of a cluster
+// walks the same items without a shared fetch.  A class of more than
+// `few` items is left to the one-CTA-per-net kernel (many huge nets keep
+// every SM busy on their own; a few finish sooner on clusters).
+template <int T, int K>
+__global__ void __launch_bounds__(T) rc_cluster_kernel(RcJob job, const int* list,
+                                                       const int* count, char* gws,
+                                                       size_t ws_stride, int few) {
+  __shared__ int sh[96];
+  __shared__ long long shl[4 * (T / 32) + 4];
+  __shared__ long long xch[2];
+  __shared__ RcArgs s_args;  // the current net's forest
+  const cg::cluster_group cl = cg::this_cluster();
+  const int S = (int)cl.num_blocks();
+  const int cid = (int)blockIdx.x / S, ncl = (int)gridDim.x / S;
+  char* ws = gws + (size_t)cid * ws_stride;
+  ClusterGroup<T> g;
+  g.S = S;
+  g.r = (int)cl.block_rank();
+  g.flag = cl.map_shared_rank(sh + 32, 0);
+  g.maxd = cl.map_shared_rank(sh + 33, 0);
+  g.smx = (unsigned*)cl.map_shared_rank(sh + 40, 0);
+  g.xch = xch;
+  const int cnt = *count;
+  if (cnt > few) return;  // uniform: no CTA has touched another's memory
+  for (int item = cid; item < cnt; item += ncl) {
+    if (threadIdx.x == 0) {
+      int f, net;
+      job_item(job, list[item], f, net);
+      s_args = job_forest(job, f);
+      sh[34] = net;
+    }
+    __syncthreads();
+    const int net = sh[34];
+    const int n = s_args.nodes_start[net + 1] - s_args.nodes_start[net];
+    rc_net_block<T, K, int>(s_args, net, ws, n, sh, shl, g);
+    g.sync();  // the slice, s_args and rank 0's scalars are reused by the next item
   }
 }
 
@@ -1232,6 +1398,74 @@ int huge_ctas(int sms, size_t stride) {
   return (int)std::max<size_t>(1, std::min<size_t>((size_t)sms * 2, cap));
 }
 
+// The huge-net path: one CTA per net, and clusters of S CTAs of 512
+// threads per net.  Both are launched; the device-side count of huge nets
+// picks one: clusters for at most kClusterNetsPerCluster nets per cluster,
+// one CTA per net for more.  S defaults to 8 (the portable cluster size),
+// capped by what the device places; OTG_RC_HUGE_CLUSTER=2|4|8|16 asks for
+// another size, =1 turns the clusters off.
+constexpr int kHugeT = 512, kHugeK = 8;
+constexpr int kClusterNetsPerCluster = 2;
+struct HugePlan {
+  int S = 1;            // CTAs per cluster (1: no cluster launch)
+  int clusters = 0;     // clusters launched, one workspace slice each
+  size_t stride_c = 0;  // bytes per cluster slice
+  int ctas = 0;         // CTAs of the one-CTA-per-net launch, one slice each
+  size_t stride = 0;    // bytes per slice of that launch
+  size_t bytes() const { return stride * (size_t)ctas + stride_c * (size_t)clusters; }
+};
+
+int max_clusters(int S) {  // clusters of S CTAs the device holds at once (0: none)
+  static std::mutex mu;
+  static int cache[64][5];
+  static bool done[64][5];
+  int d = 0;
+  cudaGetDevice(&d);
+  int si = 0;
+  while ((1 << si) < S && si < 4) ++si;
+  std::lock_guard<std::mutex> lk(mu);
+  if (!done[d & 63][si]) {
+    auto kern = rc_cluster_kernel<kHugeT, kHugeK>;
+    int nc = 0;
+    if (S > 8) cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = (unsigned)S;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.gridDim = dim3(S);
+    cfg.blockDim = dim3(kHugeT);
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    if (cudaOccupancyMaxActiveClusters(&nc, (const void*)kern, &cfg) != cudaSuccess) nc = 0;
+    cudaGetLastError();
+    cache[d & 63][si] = nc;
+    done[d & 63][si] = true;
+  }
+  return cache[d & 63][si];
+}
+
+HugePlan huge_plan(int max_net_nodes, int sms) {
+  HugePlan h;
+  h.stride = align256(rc_layout(max_net_nodes, kHugeT, kHugeK, 4).total);
+  h.ctas = huge_ctas(sms, h.stride);
+  int S = 8;
+  if (const char* e = std::getenv("OTG_RC_HUGE_CLUSTER")) S = std::atoi(e);
+  int s2 = 1;
+  while (s2 * 2 <= std::min(std::max(S, 1), 16)) s2 *= 2;
+  S = s2;
+  int ncl = 0;
+  while (S > 1 && (ncl = max_clusters(S)) < 1) S /= 2;
+  if (S > 1) {
+    h.S = S;
+    h.stride_c = align256(rc_layout(max_net_nodes, kHugeT, kHugeK, 4, S).total);
+    const size_t cap = ((size_t)4 << 30) / std::max<size_t>(h.stride_c, 1);
+    h.clusters = (int)std::max<size_t>(1, std::min<size_t>((size_t)ncl, cap));
+  }
+  return h;
+}
+
 }  // namespace
 
 // Workspace: [status 64 B][counters 64 B][lists C x N ints][huge slices]
@@ -1245,8 +1479,9 @@ size_t rc_workspace_bytes_for(const RcTune& t, int num_nets, int max_net_nodes, 
   *off_huge = o;
   *huge_stride = 0;
   if (max_net_nodes > c.nmax[6]) {
-    *huge_stride = align256(rc_layout(max_net_nodes, 512, 8, 4).total);
-    o += *huge_stride * (size_t)huge_ctas(sms, *huge_stride);
+    const HugePlan h = huge_plan(max_net_nodes, sms);
+    *huge_stride = h.stride;
+    o += h.bytes();
   }
   return o;
 }
@@ -1273,7 +1508,7 @@ cudaError_t launch_smem_class(const RcJob& job, const int* list, int* count, int
   if (err == cudaSuccess) err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, T, smem);
   if (err != cudaSuccess) return err;
   occ = std::max(occ, 1);
-  kern<<<sms * occ, T, smem, stream>>>(job, list, count, work, nullptr, 0);
+  kern<<<sms * occ, T, smem, stream>>>(job, list, count, work, nullptr, 0, 0);
   count_launch();
   return cudaGetLastError();
 }
@@ -1379,10 +1614,30 @@ otg_status rc_launch_job(RcJob job, int cap, int max_net_nodes, void* workspace,
   }
   // Largest nets first so the long tail overlaps the small ones.
   if (err == cudaSuccess && max_net_nodes > cls.nmax[6]) {
-    rc_block_kernel<512, 8, int, false><<<huge_ctas(di.sms, stride), 512, 0, next_stream()>>>(
-        job, L(7), counters + 7, work + 7, ws + off_huge, stride);
+    const HugePlan h = huge_plan(max_net_nodes, di.sms);
+    const int few = h.S > 1 ? kClusterNetsPerCluster * h.clusters : 0;
+    cudaStream_t hs = next_stream();
+    rc_block_kernel<kHugeT, kHugeK, int, false><<<h.ctas, kHugeT, 0, hs>>>(
+        job, L(7), counters + 7, work + 7, ws + off_huge, stride, few);
     count_launch();
     err = cudaGetLastError();
+    if (err == cudaSuccess && h.S > 1) {
+      cudaLaunchConfig_t cfg = {};
+      cudaLaunchAttribute at[1];
+      at[0].id = cudaLaunchAttributeClusterDimension;
+      at[0].val.clusterDim.x = (unsigned)h.S;
+      at[0].val.clusterDim.y = 1;
+      at[0].val.clusterDim.z = 1;
+      cfg.gridDim = dim3(h.clusters * h.S);
+      cfg.blockDim = dim3(kHugeT);
+      cfg.stream = hs;
+      cfg.attrs = at;
+      cfg.numAttrs = 1;
+      err = cudaLaunchKernelEx(&cfg, rc_cluster_kernel<kHugeT, kHugeK>, job, (const int*)L(7),
+                               (const int*)(counters + 7), ws + off_huge + stride * (size_t)h.ctas,
+                               h.stride_c, few);
+      count_launch();
+    }
   }
   for (int c = tn.num; c >= 1 && err == cudaSuccess; --c) {
     if (max_net_nodes <= cls.nmax[c - 1]) continue;

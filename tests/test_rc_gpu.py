@@ -77,6 +77,46 @@ def test_global_workspace_path(cuda):
     assert_parity(f, run(f, cuda))
 
 
+HUGE_SIZES = [5000, 20000, 12000, 7000, 30, 600, 16000, 9000, 20000, 5500]
+HUGE_KINDS = ["chain", "rrt", "path", "star", "rrt", "chain", "chain", "rrt", "path", "rrt"]
+
+
+@pytest.mark.parametrize("cl", ["8", "16", "2"])
+def test_huge_nets_cluster_path(cuda, monkeypatch, cl):
+    """Nets of 5k-20k nodes (random trees, chains with side branches, bare
+    paths, stars) run on a thread-block cluster per net, the cluster's CTAs
+    acting as one block over the net's workspace slice.  BFS slots, pid and
+    directed edges are bit-exact with the oracle; load, delay and ldelay are
+    within the tolerance of the reference's fp32 recursion; every quantity
+    is at least as close to the FP64 oracle as that recursion (4x slack, as
+    test_error_against_fp64).  Impulse is held to the FP64 bar only: on the
+    12k-node bare path the fp32 recursion's own impulse (2 beta - delay^2,
+    a difference of two ~1e10 terms) lies 1.4 tolerance units from FP64.
+    Every output is bit-identical to the one-CTA-per-net path (the sums are
+    exact, so the thread count changes no bit)."""
+    f = rcgen.forest(31, HUGE_SIZES, HUGE_KINDS)
+    monkeypatch.setenv("OTG_RC_HUGE_CLUSTER", "1")
+    one = run(f, cuda)
+    monkeypatch.setenv("OTG_RC_HUGE_CLUSTER", cl)
+    b = run(f, cuda)
+    for q in ["node2bfs", "pid", "edges"] + Q:
+        assert np.array_equal(getattr(b, q).cpu().numpy(), getattr(one, q).cpu().numpy()), q
+    st, e, n2b, pid, depth = O.bfs(f)
+    assert st == 0
+    got_n2b = b.node2bfs.cpu().numpy()
+    assert np.array_equal(got_n2b, n2b)
+    assert np.array_equal(b.pid.cpu().numpy(), pid)
+    assert np.array_equal(b.edges.cpu().numpy(), e)
+    st, ex = O.elmore_f64(f)
+    st2, ref = O.elmore_cpu_f32(f)
+    for q, x, r in zip(Q, ex, ref):
+        got = bfs_local(f.nodes_start, got_n2b, getattr(b, q).cpu().numpy())
+        if q != "impulse":
+            assert elmore_err(f.nodes_start, got, r) <= 1.0, q
+        assert max_rel_vs_f64(f.nodes_start, got, x) <= 4 * max_rel_vs_f64(f.nodes_start, r, x) \
+            + 1e-7, q
+
+
 @pytest.mark.parametrize("name", ["rc_cpu_small.npz", "rc_cpu_c17.npz", "rc_cpu_s27.npz"])
 def test_reference_cpu_fixtures(cuda, name):
     d = np.load(os.path.join(GOLD, name))
