@@ -427,6 +427,8 @@ def run_ours(args, world, rank, local):
         line["spef_ingest"] = _section(run_spef, base)
     if world == 1 and not args.no_full_update:
         line["full_update"] = _section(run_full_update, baseline=base if rank == 0 else None)
+    if world == 1 and not args.no_huge:
+        line["huge_nets"] = _section(run_huge)
     return line
 
 
@@ -1180,6 +1182,62 @@ def _incremental_spef(d, keep, f0, caps, batch, graph, names, baseline=None):
     return out
 
 
+def run_huge():
+    """Nets above the shared-memory classes (the seeded generator's trees
+    and chains at 20k and 5k-20k nodes): the cluster path (one thread-block
+    cluster of 8 CTAs per net, chosen on the device when there are at most
+    two nets per cluster) against one CTA per net over a workspace slice
+    (OTG_RC_HUGE_CLUSTER=1), CUDA events, median of 5 passes after 2; the
+    two paths' outputs are compared bit for bit."""
+    import torch
+    import opentimer_b200 as otg
+    from opentimer_b200 import workloads
+    out = {}
+    cases = [("8 nets x 20000 nodes", np.arange(9, dtype=np.int32) * 20000),
+             ("1 net x 20000 nodes", np.array([0, 20000], np.int32)),
+             ("200 nets, 5000..20000 nodes", workloads.net_sizes(SEED + 11, 200, 5000, 20000))]
+    for name, ns_np in cases:
+        ns = torch.from_numpy(ns_np).cuda()
+        g = otg.synth_forest(SEED + 11, ns)
+        V = int(ns_np[-1])
+        res, outs = {}, {}
+        for path, env in (("one_cta_per_net", "1"), ("default", None)):
+            if env is None:
+                os.environ.pop("OTG_RC_HUGE_CLUSTER", None)
+            else:
+                os.environ["OTG_RC_HUGE_CLUSTER"] = env
+            try:
+                b = otg.RcBatch(ns, g["edges"].clone(), g["roots"], g["res"], g["cap"],
+                                max_net_nodes=int(np.diff(ns_np).max()))
+                for _ in range(2):
+                    b.run()
+                b.check()
+                times = []
+                for _ in range(5):
+                    e0 = torch.cuda.Event(enable_timing=True)
+                    e1 = torch.cuda.Event(enable_timing=True)
+                    e0.record()
+                    b.run()
+                    e1.record()
+                    torch.cuda.synchronize()
+                    times.append(e0.elapsed_time(e1))
+                b.check()
+                ms = float(np.median(times))
+                res[path] = {"ms": ms, "nodes_per_s": V / ms * 1e3}
+                outs[path] = [getattr(b, q).cpu() for q in ("node2bfs", "pid", "load", "delay",
+                                                             "ldelay", "impulse")]
+                del b
+            finally:
+                os.environ.pop("OTG_RC_HUGE_CLUSTER", None)
+        res["speedup"] = res["one_cta_per_net"]["ms"] / res["default"]["ms"]
+        res["outputs_identical"] = all(torch.equal(x, y) for x, y in
+                                       zip(outs["one_cta_per_net"], outs["default"]))
+        out[name] = res
+    out["what"] = ("default: clusters of 8 CTAs per net when the device-side count of huge nets "
+                   "is at most 2 per cluster, else one CTA per net")
+    return out
+
+
 def reference_gpu_rc(ns_np, seed, budget_s=8.0):
     """The reference's own sm_100a RC kernels (rct_bfs_and_compute_cuda,
     ot/cuda/rct.cu:361-397, oracle/_ref) on the first nets of the headline
@@ -1276,6 +1334,7 @@ def main():
     ap.add_argument("--no-spef", action="store_true")
     ap.add_argument("--no-full-update", action="store_true")
     ap.add_argument("--no-parity", action="store_true")
+    ap.add_argument("--no-huge", action="store_true")
     ap.add_argument("--inc-gates", type=int, default=INC_GATES,
                     help="gates of the incremental sizing loop's design (smaller: quick runs)")
     ap.add_argument("--inc-iters", type=int, default=INC_ITERS)
