@@ -153,8 +153,8 @@ otg_status otg_rc_status(const void* workspace, otg_stream_t stream, int32_t* ba
  *   counts[2]       counts[0] = number of levels, counts[1] = pins emitted
  * level(v) = 1 + max over candidate fanouts (longest path to a sink).  All
  * levels run inside one launch (no host round trip per level): a single
- * thread-block cluster for graphs of up to about a million pins with a seed
- * level of at most 8192 pins, a cooperative grid otherwise, whose grid
+ * thread-block cluster for graphs of up to about a million pins, a
+ * cooperative grid otherwise, whose grid
  * barrier is bounded and reports OTG_ERR_TIMEOUT instead of hanging.  Both
  * give identical outputs.
  */

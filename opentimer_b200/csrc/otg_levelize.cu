@@ -27,8 +27,8 @@
 // past the limit raises an abort flag that every other wait also watches,
 // so the kernel always returns and the host sees OTG_ERR_TIMEOUT.
 //
-// Graphs of up to about a million pins whose seed level is narrow run
-// instead in ONE thread-block cluster (levelize_cluster_kernel below):
+// Graphs of up to about a million pins run instead in ONE thread-block
+// cluster (levelize_cluster_kernel below):
 // the same rule and the same outputs, with the ready bitmaps and counts in
 // distributed shared memory, the hardware cluster barrier between levels,
 // and the next level's fanin ranges gathered while the counters are
@@ -344,14 +344,17 @@ constexpr int kCtMax = 1024;
 namespace cg = cooperative_groups;
 
 // Where a pin that becomes ready goes: its owner's bitmap word and count
-// (distributed shared memory), and the readying CTA's own list of fanin
-// ranges for the next level's expansion.
+// (distributed shared memory), and the list of fanin ranges that one CTA,
+// chosen by a hash of the pin, expands next level.  (Hashing keeps the
+// lists even: a CTA that readied a whole level -- a buffer tree readies
+// its levels from one place -- would otherwise expand the next one alone.)
 struct ClNext {
   unsigned* bm;  // next level's bitmap (this CTA's address; mapped to the owner)
   int cshift;    // log2 of the words per CTA range: the owner of word w is w >> cshift
+  int sshift;    // log2 of the cluster size
   int* rc;       // next level's per-owner counts [16] (every CTA keeps a copy)
-  int2* lst;     // this CTA's list of (fanin start, fanin count) for the next level
-  int* lcnt;     // its length
+  int2* lst;     // next level's list of (fanin start, fanin count) (mapped to the target)
+  int* lcnt;     // its length (likewise)
   int* ovf;      // next level's overflow flag (set in every CTA)
   int cap;       // list capacity
 };
@@ -374,49 +377,13 @@ __device__ __forceinline__ void decrement_cl(int v, bool ok, const int* fanin_st
       atomicOr(cl.map_shared_rank(nx.bm, owner) + (w - (owner << nx.cshift)), 1u << (v & 31));
       const int S = (int)cl.num_blocks();
       for (int i = 0; i < S; ++i) atomicAdd(cl.map_shared_rank(nx.rc + owner, i), 1);
-      const int slot = atomicAdd(nx.lcnt, 1);
+      const int t = nx.sshift ? (int)(((unsigned)v * 0x9E3779B1u) >> (32 - nx.sshift)) : 0;
+      const int slot = atomicAdd(cl.map_shared_rank(nx.lcnt, t), 1);
       if (slot < nx.cap) {
-        nx.lst[slot] = make_int2(s0, s1 - s0);
+        *cl.map_shared_rank(nx.lst + slot, t) = make_int2(s0, s1 - s0);
       } else {
         for (int i = 0; i < (int)cl.num_blocks(); ++i) *cl.map_shared_rank(nx.ovf, i) = 1;
       }
-    }
-  }
-}
-
-// Expansion of m fanin ranges (range(k) -> (start, count)) with no block
-// barrier: 32 ranges at a time, every warp scans the same 32 counts with
-// shuffles and takes its own slice of their edges (warp w: edges w*32 +
-// lane, stepping by the CTA width), the edge's range found by a binary
-// search over the lanes' exclusive starts.
-template <int CT, class RangeF>
-__device__ __forceinline__ void expand_warps(int m, RangeF range, const int* fanin_start,
-                                             const int* fanin, int* cnt, int n, const ClNext& nx,
-                                             const cg::cluster_group& cl) {
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  for (int c0 = 0; c0 < m; c0 += 32) {
-    int2 en = make_int2(0, 0);
-    if (c0 + lane < m) en = range(c0 + lane);
-    int y = en.y;
-#pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-      const int z = __shfl_up_sync(FULL, y, d);
-      if (lane >= d) y += z;
-    }
-    const int excl = y - en.y;
-    const int etot = __shfl_sync(FULL, y, 31);
-    for (int q0 = w * 32; q0 < etot; q0 += CT) {
-      const int q = q0 + lane;
-      int lo = 0;  // the last lane whose start is <= q
-#pragma unroll
-      for (int step = 16; step >= 1; step >>= 1) {
-        const int cand = lo + step;
-        const int ex = __shfl_sync(FULL, excl, cand & 31);
-        if (cand < 32 && ex <= q) lo = cand;
-      }
-      const int e0 = __shfl_sync(FULL, en.x, lo), ex0 = __shfl_sync(FULL, excl, lo);
-      const int v = q < etot ? fanin[e0 + (q - ex0)] : -1;
-      decrement_cl(v, (unsigned)v < (unsigned)n, fanin_start, cnt, nx, cl);
     }
   }
 }
@@ -442,6 +409,7 @@ __global__ void __launch_bounds__(CT, 1) levelize_cluster_kernel(
   __shared__ int s_excl[CT], s_e0[CT];    // list entries: warp-exclusive edge start, fanin start
   const cg::cluster_group cl = cg::this_cluster();
   const int S = (int)cl.num_blocks(), r = (int)cl.block_rank(), tid = threadIdx.x;
+  const int sshift = 31 - __clz(S);  // cluster sizes are powers of two
   const int gtid = r * CT + tid, gstride = S * CT;
   const int nw = (n + 31) >> 5;
   const int lane = tid & 31, w = tid >> 5;
@@ -475,7 +443,7 @@ __global__ void __launch_bounds__(CT, 1) levelize_cluster_kernel(
   cl.sync();
   // expand the seed into level 1 (bm1, slot 1, lst1)
   {
-    const ClNext nx{bm1, cshift, rc[1], lst1, &lcnt[1], &ovf[1], lst_cap};
+    const ClNext nx{bm1, cshift, sshift, rc[1], lst1, &lcnt[1], &ovf[1], lst_cap};
     for (int k0 = r * CT; k0 < first_size; k0 += gstride) {
       const int k = k0 + tid;
       const bool act = k < first_size && (unsigned)order[k] < (unsigned)n;
@@ -504,8 +472,8 @@ __global__ void __launch_bounds__(CT, 1) levelize_cluster_kernel(
     const int par = L & 1;
     unsigned* cur = par ? bm1 : bm0;
     int2* lcur = par ? lst1 : lst0;
-    const ClNext nx{par ? bm0 : bm1, cshift, rc[q_next], par ? lst0 : lst1, &lcnt[q_next],
-                    &ovf[q_next], lst_cap};
+    const ClNext nx{par ? bm0 : bm1, cshift,        sshift,        rc[q_next],
+                    par ? lst0 : lst1, &lcnt[q_next], &ovf[q_next], lst_cap};
     if (tid < 16) rc[q_free][tid] = 0;  // read a level ago; added to from the next level on
     if (tid == 0) {
       lcnt[q_free] = 0;
@@ -519,6 +487,10 @@ __global__ void __launch_bounds__(CT, 1) levelize_cluster_kernel(
     const int run = emitted + before;
     const int m = lcnt[q_now];          // appended before the cluster barrier
     const bool over = ovf[q_now] != 0;  // likewise; the same in every CTA
+#ifdef OTG_PHASE_TIMING
+    if (tid == 0 && L < 4096) counts[16 + L * 16 + r] = m;
+    const long long _lt0 = clock64();
+#endif
     LV_PHASE(3);
     // the emission writes the range's pins in ascending order into `order`
     // with their level and clears the words for reuse two levels on
@@ -540,68 +512,83 @@ __global__ void __launch_bounds__(CT, 1) levelize_cluster_kernel(
     int pc = 0;
     for (int i = i0; i < i1; ++i) pc += __popc(cur[i - r * C]);
     constexpr int W = CT / 32;
-    if (!over && m <= CT) {
-      // the common level, one list entry per thread: ONE block scan serves
-      // both the emission (popcounts) and the expansion (fanin counts).  An
-      // edge q finds its warp by a shuffle search over the warps' edge
-      // totals, then its entry by a binary search over that warp's
-      // exclusive starts; the emission runs while the first fanin loads
-      // are in flight.
-      const int2 en = tid < m ? lcur[tid] : make_int2(0, 0);
-      int y1 = en.y, y2 = pc;
+    // Expansion of fanin ranges range(k), k < mm, CT at a time: ONE block
+    // scan per chunk hands one edge to each thread -- an edge q finds its
+    // warp by a shuffle search over the warps' edge totals, then its range
+    // by a binary search over that warp's exclusive starts.  With `emit_on`
+    // the first chunk's scan also gives the emission offsets (popcounts),
+    // and the emission runs while the first fanin loads are in flight.
+    auto expand = [&](int mm, auto range, bool emit_on) {
+      bool pending = emit_on;
+      int c0 = 0;
+      do {
+        const int k = c0 + tid;
+        const int2 en = k < mm ? range(k) : make_int2(0, 0);
+        int y1 = en.y, y2 = (emit_on && c0 == 0) ? pc : 0;
 #pragma unroll
-      for (int d = 1; d < 32; d <<= 1) {
-        const int z1 = __shfl_up_sync(FULL, y1, d), z2 = __shfl_up_sync(FULL, y2, d);
-        if (lane >= d) {
-          y1 += z1;
-          y2 += z2;
+        for (int d = 1; d < 32; d <<= 1) {
+          const int z1 = __shfl_up_sync(FULL, y1, d), z2 = __shfl_up_sync(FULL, y2, d);
+          if (lane >= d) {
+            y1 += z1;
+            y2 += z2;
+          }
         }
-      }
-      s_excl[tid] = y1 - en.y;
-      s_e0[tid] = en.x;
-      if (lane == 31) {
-        wsum[par][w] = y1;
-        wsum[par][W + w] = y2;
-      }
-      __syncthreads();
-      const int tE = lane < W ? wsum[par][lane] : 0;
-      const int tP = lane < W ? wsum[par][W + lane] : 0;
-      const int wbP = __reduce_add_sync(FULL, lane < w ? tP : 0);
-      int inclE = tE;  // lane u: edges of warps 0..u
-#pragma unroll
-      for (int d = 1; d < 32; d <<= 1) {
-        const int z = __shfl_up_sync(FULL, inclE, d);
-        if (lane >= d) inclE += z;
-      }
-      const int etot = __shfl_sync(FULL, inclE, 31);
-      bool pending = true;
-      for (int q0 = 0; q0 < etot; q0 += CT) {
-        const int q = q0 + tid;
-        const int qc = min(q, etot - 1);  // every lane searches (the shuffles are warp-wide)
-        int u = 0;                        // warps whose edges all lie before qc
-#pragma unroll
-        for (int step = 16; step >= 1; step >>= 1) {
-          const int ic = __shfl_sync(FULL, inclE, (u + step - 1) & 31);
-          if (ic <= qc) u += step;
+        s_excl[tid] = y1 - en.y;
+        s_e0[tid] = en.x;
+        if (lane == 31) {
+          wsum[par][w] = y1;
+          wsum[par][W + w] = y2;
         }
-        const int base = __shfl_sync(FULL, inclE, (u - 1) & 31);
-        const int ql = qc - (u > 0 ? base : 0);
-        const int* xs = s_excl + u * 32;
-        int j = 0;  // the last entry of warp u whose start is <= ql
+        __syncthreads();
+        const int tE = lane < W ? wsum[par][lane] : 0;
+        const int tP = lane < W ? wsum[par][W + lane] : 0;
+        const int epos = run + __reduce_add_sync(FULL, lane < w ? tP : 0) + y2 - pc;
+        int inclE = tE;  // lane u: edges of warps 0..u
 #pragma unroll
-        for (int step = 16; step >= 1; step >>= 1)
-          if (xs[j + step] <= ql) j += step;
-        const int v = q < etot ? fanin[s_e0[u * 32 + j] + (ql - xs[j])] : -1;
+        for (int d = 1; d < 32; d <<= 1) {
+          const int z = __shfl_up_sync(FULL, inclE, d);
+          if (lane >= d) inclE += z;
+        }
+        const int etot = __shfl_sync(FULL, inclE, 31);
+        for (int q0 = 0; q0 < etot; q0 += CT) {
+          const int q = q0 + tid;
+          const int qc = min(q, etot - 1);  // every lane searches (the shuffles are warp-wide)
+          int u = 0;                        // warps whose edges all lie before qc
+#pragma unroll
+          for (int step = 16; step >= 1; step >>= 1) {
+            const int ic = __shfl_sync(FULL, inclE, (u + step - 1) & 31);
+            if (ic <= qc) u += step;
+          }
+          const int base = __shfl_sync(FULL, inclE, (u - 1) & 31);
+          const int ql = qc - (u > 0 ? base : 0);
+          const int* xs = s_excl + u * 32;
+          int j = 0;  // the last range of warp u whose start is <= ql
+#pragma unroll
+          for (int step = 16; step >= 1; step >>= 1)
+            if (xs[j + step] <= ql) j += step;
+          const int v = q < etot ? fanin[s_e0[u * 32 + j] + (ql - xs[j])] : -1;
+          if (pending) {
+            emit(epos);
+            pending = false;
+          }
+          decrement_cl(v, (unsigned)v < (unsigned)n, fanin_start, cnt, nx, cl);
+        }
         if (pending) {
-          emit(run + wbP + y2 - pc);
+          emit(epos);
           pending = false;
         }
-        decrement_cl(v, (unsigned)v < (unsigned)n, fanin_start, cnt, nx, cl);
-      }
-      if (pending) emit(run + wbP + y2 - pc);
+        c0 += CT;
+        if (c0 < mm) __syncthreads();  // the next chunk reuses s_excl, s_e0 and wsum
+      } while (c0 < mm);
+    };
+    if (!over) {
+      // the fanin ranges this CTA collected last level
+      expand(m, [&](int k) { return lcur[k]; }, true);
       LV_PHASE(1);
     } else {
-      // a longer list, or a list overflowed last level
+      // a list overflowed last level: every CTA emits its own range's pins
+      // of this level and expands them, read back from `order`, their
+      // fanin ranges from global memory
       int y2 = pc;
 #pragma unroll
       for (int d = 1; d < 32; d <<= 1) {
@@ -614,21 +601,15 @@ __global__ void __launch_bounds__(CT, 1) levelize_cluster_kernel(
       const int wbP = __reduce_add_sync(FULL, lane < w ? tP : 0);
       const int tt = min(__reduce_add_sync(FULL, tP), n - run);
       emit(run + wbP + y2 - pc);
-      if (!over) {
-        expand_warps<CT>(m, [&](int k) { return lcur[k]; }, fanin_start, fanin, cnt, n, nx, cl);
-      } else {
-        // every CTA expands its own range's pins of this level, read back
-        // from `order`, their fanin ranges from global memory
-        __syncthreads();  // this range's slice of `order` is written
-        expand_warps<CT>(
-            tt,
-            [&](int k) {
-              const int u = __ldcg(order + run + k);
-              const int e0 = fanin_start[u];
-              return make_int2(e0, fanin_start[u + 1] - e0);
-            },
-            fanin_start, fanin, cnt, n, nx, cl);
-      }
+      __syncthreads();  // this range's slice of `order` is written; wsum is reused
+      expand(
+          tt,
+          [&](int k) {
+            const int u = __ldcg(order + run + k);
+            const int e0 = fanin_start[u];
+            return make_int2(e0, fanin_start[u + 1] - e0);
+          },
+          false);
     }
     emitted += total;
     if (emitted > n) {  // only reachable with duplicate seeds; stop cleanly
@@ -637,6 +618,9 @@ __global__ void __launch_bounds__(CT, 1) levelize_cluster_kernel(
       break;
     }
     if (gtid == 0) level_ends[L + 1] = emitted;
+#ifdef OTG_PHASE_TIMING
+    if (tid == 0 && L < 4096) counts[16 + 65536 + L * 16 + r] = (int)(clock64() - _lt0);
+#endif
     ++L;
     const int q = q_free;
     q_free = q_now;
@@ -725,19 +709,13 @@ struct ClPlan {
 };
 // Default: the largest cluster the device places (16 CTAs on B200) of 256
 // threads each, for graphs whose ranges then hold at most kClusterMaxWords
-// words (about a million pins) and whose seed level has at most
-// kClusterMaxSeed pins.  Larger graphs, and graphs whose wide seed level
-// announces wide levels, take the cooperative path, which spreads a level
-// over every SM.  On B200: a 165k-pin graph of 600 levels took 1.84 ms in
-// the cluster path and 3.61 ms in the cooperative one, one of 1M pins and
-// 2000 levels 13.3 and 15.3 ms; one of 100k pins in 3 levels 0.25 and
-// 0.07 ms.  OTG_LEVELIZE_CLUSTER=0
-// turns the cluster path off, =1|2|4|8|16 asks for that size;
-// OTG_LEVELIZE_CT=128|256|512|1024 asks for that width (both only where
-// the graph fits and the device places the cluster).
+// words (about a million pins); larger graphs take the cooperative path,
+// which spreads a level over every SM.  OTG_LEVELIZE_CLUSTER=0 turns the
+// cluster path off, =1|2|4|8|16 asks for that size; OTG_LEVELIZE_CT=
+// 128|256|512|1024 asks for that width (both only where the graph fits and
+// the device places the cluster).
 constexpr int kClusterMaxWords = 2048;
-constexpr int kClusterMaxSeed = 8192;
-ClPlan lv_cluster_plan(int n, int first_size, const LvDev& d) {
+ClPlan lv_cluster_plan(int n, const LvDev& d) {
   ClPlan p;
   const int nw = std::max(1, (n + 31) / 32);
   p.wi = 1;
@@ -754,8 +732,8 @@ ClPlan lv_cluster_plan(int n, int first_size, const LvDev& d) {
     if (want <= 0) return ClPlan{};
     s = 1;
     while (s < want && s < maxc) s <<= 1;
-  } else if ((nw + s - 1) / s > kClusterMaxWords || first_size > kClusterMaxSeed) {
-    return ClPlan{};  // large or wide graphs: the whole GPU (the cooperative path)
+  } else if ((nw + s - 1) / s > kClusterMaxWords) {
+    return ClPlan{};  // large graphs: the whole GPU (the cooperative path)
   }
   int cs = 0;
   while ((1 << cs) * s < nw) ++cs;
@@ -813,7 +791,7 @@ otg_status otg_levelize(int32_t n, int32_t num_edges, const int32_t* fanin_start
   const otg::LvWs l = otg::lv_ws(n, G);
   if (workspace_bytes < l.total) return OTG_ERR_WORKSPACE;
   const int nw = (n + 31) / 32;
-  const otg::ClPlan pl = otg::lv_cluster_plan(n, first_size, d);
+  const otg::ClPlan pl = otg::lv_cluster_plan(n, d);
   if (pl.S > 0) {
     char* ws = (char*)workspace;
     cudaStream_t s = (cudaStream_t)stream;
