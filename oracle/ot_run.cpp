@@ -13,9 +13,14 @@
 // repower=<ops>: after the first update, a sequence of gate resizes, one
 // "<gate> <cell>" per line, steps separated by lines holding "=": each step
 // is Timer::repower_gate for its lines, then update_timing (the dirty nets
-// and the affected cone only, as the Timer does).  The seconds of every
-// step go to stdout ("repower_step_s <k> <s>"); with dump_every=<k> the
-// pins (P lines) after every k-th step go to <out>.step<k>.
+// and the affected cone only, as the Timer does).  The Timer clears all of
+// its state bits, CUDA_ENABLED among them, at the end of every update
+// (_remove_state() in Timer::_update_timing, ot/timer/timer.cpp), so in
+// "cuda" mode each step calls cuda(true) again before its update_timing;
+// otherwise every step after the first would run the CPU path.  The
+// seconds of every step go to stdout ("repower_step_s <k> <s>"); with
+// dump_every=<k> the pins (P lines) after every k-th step go to
+// <out>.step<k>.
 // The same Timer sources are linked twice (oracle/Makefile): with the
 // reference's own CUDA module (ot_run_ref) and with libotg in its place
 // (ot_run_otg), so "cuda" runs either the reference kernels or ours behind
@@ -221,6 +226,7 @@ int main(int argc, char** argv) {
     int step = 0, pending = 0;
     double total = 0.0;
     auto finish_step = [&]() {
+      if (cuda) timer.cuda(true);  // the previous update cleared the flag
       const auto t1 = std::chrono::steady_clock::now();
       timer.update_timing();
       const double s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t1).count();

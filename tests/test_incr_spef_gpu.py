@@ -8,9 +8,15 @@ nets' new trees in, and re-times only those (otg_rc_timing_subset).
 
 * The result equals a full pass over the final forest, bit for bit.
 * RC values at every pin node and every pin's AT/slew/RAT/slack match the
-  reference Timer after read_spef(change) + update_timing, on its CPU and
-  CUDA paths (RC: 1e-5 relative with a 1e-6 x net-max floor; pins: the
-  propagation tolerance of test_prop_gpu).
+  reference Timer after read_spef(change) + update_timing, in two runs: one
+  whose first full update took its CPU path and one whose first full update
+  took its CUDA path (RC: 1e-5 relative with a 1e-6 x net-max floor; pins:
+  the propagation tolerance of test_prop_gpu).  The incremental update
+  itself takes the Timer's CPU path in both runs: the Timer clears all its
+  state bits, CUDA_ENABLED among them, at the end of every update
+  (_remove_state() in Timer::_update_timing, ot/timer/timer.cpp), and the
+  reference's CUDA kernels are not run on the zeroed clean nets that a
+  second CUDA update would hand them.
 """
 import os
 import subprocess

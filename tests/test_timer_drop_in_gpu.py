@@ -169,7 +169,8 @@ def test_second_cuda_update_after_repower(tmp_path, cuda):
     re-flattens only the dirty ones (ot/timer/timer.cpp:929-970,
     ot/timer/net.cpp:499-514): the clean nets reach rct_bfs_and_compute_cuda
     with zeroed edges and roots.  libotg checks every net, reports them
-    (OTG_ERR_NOT_TREE on stderr) without reading out of range, and still
+    (OTG_ERR_NOT_TREE, printed as "rct_bfs_and_compute_cuda: RC net is not
+    a spanning tree") without reading out of range, and still
     times every re-flattened net: those nets' RC values must match the
     reference's CPU path after the same resizes."""
     if not (os.path.exists(EXE_REF) and os.path.exists(EXE_OTG)):
@@ -188,7 +189,7 @@ def test_second_cuda_update_after_repower(tmp_path, cuda):
                            timeout=600)
         assert p.returncode == 0, p.stderr[-2000:]
         outs[mode] = (p.stderr, out)
-    assert "rct_bfs_and_compute_cuda: OTG_ERR_NOT_TREE" in outs["cuda"][0]
+    assert "rct_bfs_and_compute_cuda: RC net is not a spanning tree" in outs["cuda"][0]
     conn = {g: c for g, _, c in keep["gates"]}
     dirty = {n for g, _ in steps[0] for n in conn[g].values()}
     R = {}
