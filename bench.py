@@ -34,11 +34,13 @@ LV_PINS, LV_EDGES, LV_LEVELS = 5_000_000, 12_000_000, 200
 TUNE_NETS = 50_000
 SPEF_NETS = 20_000
 # DRAM bytes per node of one RC pass (dram__bytes_read.sum + dram__bytes_write.sum
-# over every launch of the pass), from an ncu capture of 100k nets of the same
-# net-size distribution with the autotuned table: 7.736 GB / 52,964,231 nodes
-# (profiles/rc_pass_dram_traffic_100k_nets.md).  The pass's traffic grows with
-# its nodes, so a step's traffic is this times the step's nodes.
-RC_DRAM_BYTES_PER_NODE = 146.06
+# over the 8 launches of one pass), from an ncu capture of 30k nets of the same
+# net-size distribution with the autotuned table: 2.204 GB / 15,951,150 nodes
+# (profiles/rc_pass_dram_traffic_30k_nets.md).  The pass's traffic grows with
+# its nodes, so a step's traffic is this times the step's nodes.  (At 30k nets
+# part of the small classes' writes is still in L2 when the capture ends; the
+# dominant kernel alone moves 152.8 B/node.)
+RC_DRAM_BYTES_PER_NODE = 138.2
 FU_GATES = 50_000
 FU_REPS = 5
 FU_CHANGE = 0.01  # fraction of the nets a change SPEF re-draws
@@ -388,7 +390,7 @@ def run_ours(args, world, rank, local):
         if tuning else "off",
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": RC_DRAM_BYTES_PER_NODE * V,
-                     "traffic_source": "ncu dram bytes per node of the pass (100k-net capture) "
+                     "traffic_source": "ncu dram bytes per node of one pass (30k-net capture) "
                                        "x this step's nodes",
                      "kernel": "otg_rc_timing fused pass (classify + size-class launches)",
                      "algorithmic_bytes_per_step": abytes, "peak_kind": peak_kind},
