@@ -48,7 +48,9 @@ FU_CHANGE = 0.01  # fraction of the nets a change SPEF re-draws
 INC_GATES, INC_ITERS, INC_FRAC, INC_PLAIN_ITERS, INC_REF_ITERS = 200_000, 1000, 0.005, 100, 3
 # serving
 SRV_DESIGNS, SRV_PINS_LO, SRV_PINS_HI = 16, 10_000, 2_000_000
-SRV_RATES, SRV_MAX_REQ, SRV_SAT_REQ, SRV_REF_REQ = (2_000, 10_000, 50_000), 2_000, 3_000, 12
+# offered rates: below both paths' capacity, between the plain path's (about
+# 180 req/s on the 16 designs) and the batched one's (about 450), and above both
+SRV_RATES, SRV_MAX_REQ, SRV_SAT_REQ, SRV_REF_REQ = (100, 300, 1_000), 2_000, 3_000, 12
 SRV_PINS_PER_GATE = 2.75  # designgen: pins per gate of a design
 
 
@@ -867,7 +869,7 @@ def run_serving(baseline=None):
         srv.replay(warm)
         srv.replay(warm, plain=True)
         for rate in SRV_RATES:
-            n = min(SRV_MAX_REQ, int(rate * 0.5))
+            n = min(SRV_MAX_REQ, max(300, int(rate * 3)))  # about 3 s of arrivals
             tr = request_trace(keeps, SEED + int(rate), n, rate)
             lat_b, span_b, _ = srv.replay(tr)
             lat_p, span_p, _ = srv.replay(tr, plain=True)

@@ -448,6 +448,18 @@ otg_status otg_propagate_groups(const otg_prop_graph* graph, const otg_prop_rc* 
                                 const int32_t* pin_group, const uint8_t* group_active,
                                 float* at, float* slew, float* rat, float* slack,
                                 void* workspace, size_t workspace_bytes, otg_stream_t stream);
+/* The same over a list of pins only: items[num_items] (device) are the pins
+ * to propagate, in a backward order as `order` above (every pin after all
+ * of its fanout pins; the forward pass takes it reversed).  The list must
+ * hold, with each pin, every pin it reads that is not final: for a union
+ * of independent designs, the pins of whole designs, e.g. the union's
+ * order regrouped design by design (a stable regrouping keeps each
+ * design's pins in level order).  Only the listed pins are marked pending
+ * and written; the work is in proportion to the list, not to the graph. */
+otg_status otg_propagate_items(const otg_prop_graph* graph, const otg_prop_rc* rc,
+                               const int32_t* items, int32_t num_items, float* at, float* slew,
+                               float* rat, float* slack, void* workspace, size_t workspace_bytes,
+                               otg_stream_t stream);
 
 /*
  * ---- Incremental gate resizing (the device side of Timer::repower_gate,

@@ -488,12 +488,20 @@ __device__ __forceinline__ bool pin_on(const int32_t* pin_group, const uint8_t* 
   return !pin_group || group_active[__ldg(pin_group + v)];
 }
 
+// (items: only the listed pins, see otg_propagate_items; num_pins is then
+// the list's length.)
 __global__ void prop_init_kernel(float4* at, float4* slew, int num_pins, GridCtl* ctl,
-                                 const int32_t* pin_group, const uint8_t* group_active) {
+                                 const int32_t* pin_group, const uint8_t* group_active,
+                                 const int32_t* items, int all_pins) {
   const int i0 = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i0 == 0) *ctl = GridCtl{0u, 0u, 0, 0};
+  if (i0 == 0 && !items) *ctl = GridCtl{0u, 0u, 0, 0};
   const float p = __uint_as_float(kPending);
-  for (int i = i0; i < num_pins; i += gridDim.x * blockDim.x) {
+  for (int k = i0; k < num_pins; k += gridDim.x * blockDim.x) {
+    const int i = items ? __ldg(items + k) : k;
+    if (items && (unsigned)i >= (unsigned)all_pins) {
+      atomicCAS(&ctl->status, 0, (int)OTG_ERR_INVALID);  // reported; the passes skip it
+      continue;
+    }
     if (!pin_on(pin_group, group_active, i)) continue;
     at[i] = make_float4(p, p, p, p);
     slew[i] = make_float4(p, p, p, p);
@@ -521,6 +529,7 @@ __global__ void __launch_bounds__(256) prop_kernel(G G_, const int* order, const
   bool ok = true;
   for (int j = warp; ok && j < num_pins; j += W) {
     const int v = fwd_order ? __ldg(fwd_order + j) : __ldg(order + num_pins - 1 - j);
+    if ((unsigned)v >= (unsigned)G_.g.num_pins) continue;  // a bad item (reported by the fill)
     if (!pin_on(pin_group, group_active, v)) continue;
     ok = fprop_warp(G_, lutd, v, lane, at, slew, rat, arc_delay, test_rat, ctl);
   }
@@ -528,6 +537,7 @@ __global__ void __launch_bounds__(256) prop_kernel(G G_, const int* order, const
   if (!grid_barrier(ctl) || !ok) return;
   for (int j = warp; ok && j < num_pins; j += W) {
     const int v = __ldg(order + j);
+    if ((unsigned)v >= (unsigned)G_.g.num_pins) continue;
     if (!pin_on(pin_group, group_active, v)) continue;
     ok = bprop_warp(G_, v, lane, at, rat, slack, arc_delay, test_rat, ctl);
   }
@@ -559,11 +569,19 @@ otg_status otg_prop_workspace_size(int32_t num_pins, int32_t num_arcs, int32_t n
   return OTG_OK;
 }
 
+// items (with num_items): propagate only the listed pins, `order` and
+// fwd_order unused (see otg_propagate_items).
 static otg_status propagate_impl(const otg_prop_graph* g, const otg_prop_rc* rc,
                                  const int32_t* order, const int32_t* fwd_order,
                                  const int32_t* pin_group, const uint8_t* group_active, float* at,
                                  float* slew, float* rat, float* slack, void* workspace,
-                                 size_t workspace_bytes, otg_stream_t stream) {
+                                 size_t workspace_bytes, otg_stream_t stream,
+                                 const int32_t* items = nullptr, int num_items = 0) {
+  if (items) {
+    if (num_items < 0) return OTG_ERR_INVALID;
+    order = items;
+    fwd_order = nullptr;
+  }
   if (!g || !rc || !order || !at || !slew || !rat || !slack || !workspace || g->num_pins < 0)
     return OTG_ERR_INVALID;
   // lut_meta rows and the per-pin [4] rows are read and written as 16-byte vectors
@@ -573,14 +591,17 @@ static otg_status propagate_impl(const otg_prop_graph* g, const otg_prop_rc* rc,
   size_t need = 0;
   otg_prop_workspace_size(g->num_pins, g->num_arcs, g->num_tests, &need);
   if (workspace_bytes < need) return OTG_ERR_WORKSPACE;
-  const int P = g->num_pins;
+  const int P = items ? num_items : g->num_pins;  // the items the two passes take
   char* ws = (char*)workspace;
   otg::GridCtl* ctl = (otg::GridCtl*)ws;
   float* arc_delay = (float*)(ws + 256);
   float* test_rat = (float*)(ws + 256 + otg::align256p(32 * (size_t)g->num_arcs));
   cudaStream_t st = (cudaStream_t)stream;
+  // with items, the fill may record a bad item, so the control block is
+  // cleared before it (without items the fill clears it itself)
+  if (items && cudaMemsetAsync(ctl, 0, sizeof(otg::GridCtl), st) != cudaSuccess) return OTG_ERR_CUDA;
   otg::prop_init_kernel<<<std::max(1, std::min(1184, (P + 255) / 256)), 256, 0, st>>>(
-      (float4*)at, (float4*)slew, P, ctl, pin_group, group_active);
+      (float4*)at, (float4*)slew, P, ctl, pin_group, group_active, items, g->num_pins);
   otg::count_launch();
   if (cudaGetLastError() != cudaSuccess) return OTG_ERR_CUDA;
   if (P == 0) return OTG_OK;
@@ -633,6 +654,22 @@ otg_status otg_propagate_groups(const otg_prop_graph* g, const otg_prop_rc* rc,
   if (!pin_group || !group_active) return OTG_ERR_INVALID;
   return propagate_impl(g, rc, order, fwd_order, pin_group, group_active, at, slew, rat, slack,
                         workspace, workspace_bytes, stream);
+}
+
+otg_status otg_propagate_items(const otg_prop_graph* g, const otg_prop_rc* rc,
+                               const int32_t* items, int32_t num_items, float* at, float* slew,
+                               float* rat, float* slack, void* workspace, size_t workspace_bytes,
+                               otg_stream_t stream) {
+  if (!items && num_items > 0) return OTG_ERR_INVALID;
+  if (num_items <= 0) {  // nothing to propagate; the status word still reads OK
+    if (num_items < 0 || !workspace) return OTG_ERR_INVALID;
+    return cudaMemsetAsync(workspace, 0, sizeof(otg::GridCtl), (cudaStream_t)stream) ==
+                   cudaSuccess
+               ? OTG_OK
+               : OTG_ERR_CUDA;
+  }
+  return propagate_impl(g, rc, nullptr, nullptr, nullptr, nullptr, at, slew, rat, slack,
+                        workspace, workspace_bytes, stream, items, num_items);
 }
 
 otg_status otg_prop_status(const void* workspace, otg_stream_t stream) {

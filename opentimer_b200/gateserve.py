@@ -16,7 +16,8 @@ oldest pending one -- so every request sees exactly the state its design's
 earlier requests left, whatever else is in the batch: its result is the
 same alone and in the mix.  A batch is one launch set on one stream:
 otg_apply_updates (all its resizes), otg_rc_timing_subset (all their dirty
-nets), otg_propagate_groups (only the batch's designs), and
+nets), otg_propagate_items over only the batch's designs' pins (the union's
+level order filtered to them, so their level chains run side by side), and
 otg_worst_slack_groups (one row per design), copied back into pinned host
 memory.  Requests that arrive while batches run are taken into the next
 batch (continuous batching); two batches can be in flight, queued in
@@ -111,8 +112,21 @@ class DesignSet:
                              t(np.concatenate([f["roots"] for f in fz]).astype(np.int32)),
                              t(np.concatenate([f["res"] for f in fz]).astype(np.float32)),
                              t(np.concatenate([f["cap"] for f in fz]).astype(np.float32)))
-        self.pin_group = t(np.repeat(np.arange(G, dtype=np.int32), P))
+        group = np.repeat(np.arange(G, dtype=np.int32), P)
+        self.pin_group = t(group)
         self.G, self.P, self.device = G, int(self.p_off[-1]), device
+        # the union's level order regrouped design by design (stable, so each
+        # design keeps its level order): design d's pins are the slice
+        # seg[d]:seg[d+1], which one design alone propagates.  Several
+        # designs take the union's order filtered to their pins instead, so
+        # their level chains run side by side (consecutive slices would run
+        # one design's chain after another's).
+        order = self.graph.order.cpu().numpy()
+        by_design = order[np.argsort(group[order], kind="stable")]
+        self.dorder = t(by_design.astype(np.int32))
+        self.order_group = t(group[order].astype(np.int64))
+        self.seg = np.concatenate([[0], np.cumsum(np.bincount(group[order], minlength=G))]
+                                  ).astype(np.int64)
         self.status = torch.zeros(1, dtype=torch.int32, device=device)
         self.batch.run()
         self.graph.propagate(self.batch)
@@ -159,6 +173,7 @@ class _Slot:
         self.d = {k: torch.empty(v.shape, dtype=v.dtype, device=dev)
                   for k, v in self.h.items() if k != "wns"}
         self.d["wns"] = torch.empty((G, NC), dtype=torch.float32, device=dev)
+        self.items = torch.empty(int(ds.seg[-1]) + 1, dtype=torch.int32, device=dev)
         self.scratch = torch.empty(4 * G, dtype=torch.int32, device=dev)
         self.event = torch.cuda.Event()
         self.reqs = None
@@ -204,6 +219,21 @@ class GateServer:
                          ("active", ds.G)):
                 if n:
                     dv[k][:n].copy_(h[k][:n], non_blocking=True)
+        # the pins to propagate: one design's slice of the grouped order, or
+        # the union's order filtered to the batch's designs (an
+        # order-preserving compaction on the device; its size is known here)
+        designs = sorted(d for _, d, _ in reqs)
+        if len(designs) == 1:
+            d0 = designs[0]
+            items = ds.dorder[int(ds.seg[d0]):int(ds.seg[d0 + 1])]
+        else:
+            k = int(sum(ds.seg[d + 1] - ds.seg[d] for d in designs))
+            with torch.cuda.stream(s):
+                keep = dv["active"][ds.order_group].to(torch.int32)
+                pos = torch.cumsum(keep, 0, dtype=torch.int32) - 1
+                idx = torch.where(keep.bool(), pos, k).long()  # the rest to the spare slot k
+                slot.items.scatter_(0, idx, ds.graph.order)
+            items = slot.items[:k]
         L, b, g = lib(), ds.batch, ds.graph
         st = _stream(s)
         check("otg_apply_updates", L.otg_apply_updates(
@@ -218,10 +248,10 @@ class GateServer:
         rc = PropRc(_ptr(b.nodes_start).value, _ptr(b.node2bfs).value, _ptr(b.load).value,
                     _ptr(b.delay).value, _ptr(b.impulse).value)
         o = g.out
-        check("otg_propagate_groups", L.otg_propagate_groups(
-            ctypes.byref(g.graph), ctypes.byref(rc), _ptr(g.order), _ptr(g.fwd_order),
-            _ptr(ds.pin_group), _ptr(dv["active"]), _ptr(o["at"]), _ptr(o["slew"]),
-            _ptr(o["rat"]), _ptr(o["slack"]), _ptr(g.workspace), g.workspace.numel(), st))
+        check("otg_propagate_items", L.otg_propagate_items(
+            ctypes.byref(g.graph), ctypes.byref(rc), _ptr(items), int(items.numel()),
+            _ptr(o["at"]), _ptr(o["slew"]), _ptr(o["rat"]), _ptr(o["slack"]),
+            _ptr(g.workspace), g.workspace.numel(), st))
         check("otg_worst_slack_groups", L.otg_worst_slack_groups(
             _ptr(o["slack"]), ds.P, _ptr(ds.pin_group), _ptr(dv["active"]), ds.G,
             _ptr(slot.scratch), _ptr(dv["wns"]), st))

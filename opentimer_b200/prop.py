@@ -152,6 +152,20 @@ class TimingGraph:
             _stream(stream)))
         return self
 
+    def propagate_items(self, batch, items, stream=None):
+        """Propagation of the listed pins only (items: a CUDA int32 tensor
+        in backward level order holding, with each pin, every pin it reads
+        that is not final -- e.g. whole designs of a union, see
+        otg_propagate_items); every other pin keeps its values."""
+        rc = PropRc(_ptr(batch.nodes_start).value, _ptr(batch.node2bfs).value,
+                    _ptr(batch.load).value, _ptr(batch.delay).value, _ptr(batch.impulse).value)
+        o = self.out
+        check("otg_propagate_items", lib().otg_propagate_items(
+            ctypes.byref(self.graph), ctypes.byref(rc), _ptr(items), int(items.numel()),
+            _ptr(o["at"]), _ptr(o["slew"]), _ptr(o["rat"]), _ptr(o["slack"]),
+            _ptr(self.workspace), self.workspace.numel(), _stream(stream)))
+        return self
+
     def change_nets(self, nets, node_of, pin_names):
         """After RcBatch.replace_nets(nets, ...) with change_nets' output:
         points the net arcs into those nets at their sinks' new local ids.

@@ -70,3 +70,29 @@ def test_alone_and_in_the_mix_and_against_the_reference(designs):
         worst[di] = pin_err(ds_b.pins(di), read_ref_pins(f"{out}.step{len(mine)}"))
     print(f"served designs: pins err/tol vs the reference after their requests: {worst}")
     assert max(worst.values()) <= 1.0
+
+
+def test_propagate_items(designs):
+    """otg_propagate_items over one design's slice of the union's order
+    writes exactly that design's pins, with the bits of a full propagation;
+    every other pin keeps its values; an item out of range is reported."""
+    import torch
+    from opentimer_b200._lib import OtgError
+    from opentimer_b200.gateserve import DesignSet, build_design
+    ds = DesignSet([build_design(d, keep) for d, keep in designs])
+    g = ds.graph
+    full = g.propagate(ds.batch).result()
+    for v in g.out.values():
+        v.fill_(7.0)
+    d = 1
+    a0, a1 = int(ds.seg[d]), int(ds.seg[d + 1])
+    part = g.propagate_items(ds.batch, ds.dorder[a0:a1]).result()
+    mine = np.zeros(ds.P, bool)
+    mine[ds.dorder[a0:a1].cpu().numpy()] = True
+    assert mine[int(ds.p_off[d]):int(ds.p_off[d + 1])].sum() == a1 - a0
+    for k in full:
+        assert np.array_equal(part[k][mine].view(np.int32), full[k][mine].view(np.int32)), k
+        assert np.all(part[k][~mine] == 7.0), k
+    bad = torch.tensor([0, ds.P + 5], dtype=torch.int32, device="cuda")
+    with pytest.raises(OtgError):
+        g.propagate_items(ds.batch, bad).check()
