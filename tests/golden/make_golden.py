@@ -5,7 +5,7 @@
                                                   # oracle/_ref/libotref.so)
     python tests/golden/make_golden.py --gpu      # adds the fixtures of the
                                                   # reference's own CUDA path
-                                                  # (run on a GPU box)
+                                                  # (run on a machine with a B200)
 
 CPU fixtures: Rct::update_rc_timing (ot/timer/net.cpp:101-193) on
   * a seeded synthetic forest with random recursive trees, chains, stars,
