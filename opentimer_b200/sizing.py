@@ -109,7 +109,16 @@ class SizingDesign:
         self.names = names
         cap, node_of = rc_inputs(f, designgen.pin_caps(keep))
         self.table = ResizeTable(keep, arrays, f, node_of)
-        self.graph = TimingGraph(attach_nets(arrays, names, pin_net, f, node_of), device=device)
+        attached = attach_nets(arrays, names, pin_net, f, node_of)
+        self.graph = TimingGraph(attached, device=device)
+        # what the Timer-style queries need: endpoints (primary outputs and
+        # the constrained pins of the timing tests), nets by name, pin nodes
+        po = np.where(np.any(~np.isnan(np.asarray(attached["po_rat"])), axis=1))[0]
+        tests = np.asarray(attached["arc_to"])[np.asarray(attached["test_arc"], np.int64)]
+        self.endpoints = np.unique(np.concatenate([po, tests]).astype(np.int64))
+        self.net_names = list(f["net_names"])
+        self.nodes_start = np.asarray(f["nodes_start"], np.int64)
+        self.node_of = node_of  # (net index, pin name) -> local RC node
         t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(device)  # noqa: E731
         self.batch = RcBatch(t(f["nodes_start"]), t(f["edges"].copy()), t(f["roots"]),
                              t(f["res"]), t(cap))

@@ -30,6 +30,8 @@
 //   R <net> <node> load[4] delay[4] ldelay[4] impulse[4]   (per RC node)
 //   B <net> <node> <bfs slot> <pid of that slot>            (cuda only)
 //   K <pin> cap[4]                                          (pin caps)
+//   L <net> report_load[4]
+//   N <split> <tran> report_wns report_tns                   (per corner)
 //   S <net> <num nodes> <root id>                           (cuda only:
 //   E <net> <edge k> <s> <t> <res>                           the flat
 //   C <net> <id> cap[4]                                      storage)
@@ -283,6 +285,20 @@ int main(int argc, char** argv) {
       for (auto rf : trans) std::fprintf(f, " %.9g", pin.cap(el, rf));
     std::fprintf(f, "\n");
   }
+  for (auto& [nname, net] : timer._nets) {
+    (void)net;
+    std::fprintf(f, "L %s", nname.c_str());
+    for (auto el : splits)
+      for (auto rf : trans) put(f, timer.report_load(nname, el, rf));
+    std::fprintf(f, "\n");
+  }
+  for (auto el : splits)
+    for (auto rf : trans) {
+      std::fprintf(f, "N %d %d", (int)el, (int)rf);
+      put(f, timer.report_wns(el, rf));
+      put(f, timer.report_tns(el, rf));
+      std::fprintf(f, "\n");
+    }
   for (auto& [nname, net] : timer._nets) {
     if (const ot::Rct* rct = std::get_if<ot::Rct>(&net._rct)) {
       for (auto& [node, rn] : rct->_nodes) {

@@ -1,0 +1,120 @@
+"""The Timer-style host layer (opentimer_b200.timer.Timer) against the
+reference Timer (oracle/_ref/ot_run_ref, its CPU path) on the same design,
+after the first full update and after a batch of repower_gate calls:
+
+* report_at / report_slew / report_rat / report_slack of every pin within
+  the pin tolerance of tests/helpers.pin_err;
+* report_wns and report_tns of every corner: WNS within the tolerance of
+  the worst endpoint, TNS within the sum of the endpoints' tolerances (the
+  two sum the same terms in different orders);
+* report_load of every net and rc_node values of the pins' RC nodes within
+  the RC tolerance (1e-5 relative, floor 1e-6 x the net's max |value|).
+"""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from helpers import pin_err, read_ref_pins
+from opentimer_b200 import designgen
+
+pytestmark = pytest.mark.gpu
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+EXE_REF = os.path.join(ROOT, "oracle", "_ref", "ot_run_ref")
+
+
+def read_ref(path):
+    N, L, R = {}, {}, {}
+    with open(path) as f:
+        for line in f:
+            t = line.split()
+            if t[0] == "N":
+                N[(int(t[1]), int(t[2]))] = (float(t[3]), float(t[4]))
+            elif t[0] == "L":
+                L[t[1]] = np.array([float(x) for x in t[2:]])
+            elif t[0] == "R":
+                R[(t[1], t[2])] = np.array([float(x) for x in t[3:]]).reshape(4, 4)
+    return read_ref_pins(path), N, L, R
+
+
+def check_against(t, ref):
+    from opentimer_b200.timer import MAX, MIN
+    pins, N, L, R = ref
+    ours = {}
+    for name in pins:
+        v = np.full((4, 4), np.nan)
+        for c, (el, rf) in enumerate([(0, 0), (0, 1), (1, 0), (1, 1)]):
+            for q, f in enumerate((t.report_at, t.report_slew, t.report_rat, t.report_slack)):
+                x = f(name, el, rf)
+                v[q, c] = np.nan if x is None else x
+        ours[name] = v
+    assert pin_err(ours, pins) <= 1.0
+    # endpoints: the facade's set, tolerances from the reference's pins
+    d = t._d
+    for (el, rf), (wns, tns) in N.items():
+        c = el * 2 + rf
+        tol = []
+        for i in d.endpoints:
+            r = pins[d.names[i]]
+            if not np.isnan(r[3][c]):
+                tol.append(1e-5 * max(abs(r[3][c]), abs(np.nan_to_num(r[0][c]))) + 1e-5)
+        assert abs(t.report_wns(el, rf) - wns) <= max(tol), (el, rf)
+        assert abs(t.report_tns(el, rf) - tns) <= sum(tol), (el, rf)
+    assert t.report_wns() == min(t.report_wns(a, b) for a in (MIN, MAX) for b in (0, 1))
+    # net loads and RC nodes
+    loads = 0
+    for net, l in L.items():
+        if t.report_load(net, 0, 0) is None:  # a net without parasitics (no RC tree here)
+            continue
+        got = np.array([t.report_load(net, el, rf) for el in (0, 1) for rf in (0, 1)])
+        assert np.all(np.abs(got - l) <= 1e-5 * np.abs(l) + 1e-6 * np.abs(l).max()), net
+        loads += 1
+    assert loads > 0.9 * len(L)
+    nets = {}
+    for (net, node), v in R.items():
+        nets.setdefault(net, []).append((node, v))
+    checked = 0
+    for net, rows in nets.items():
+        mx = np.abs(np.stack([v for _, v in rows])).max(axis=0)
+        for node, v in rows:
+            got = t.rc_node(net, node)
+            if got is None:  # an internal node: the facade answers by pin name
+                continue
+            g = np.stack([got[k].reshape(4) for k in ("load", "delay", "ldelay", "impulse")])
+            assert np.all(np.abs(g - v) <= 1e-5 * np.abs(v) + 1e-6 * mx), (net, node)
+            checked += 1
+    assert checked > 1000
+
+
+@pytest.fixture(scope="module")
+def design(tmp_path_factory, cuda):
+    if not os.path.exists(EXE_REF):
+        pytest.skip("the reference Timer harness (oracle/_ref) is not built")
+    d = str(tmp_path_factory.mktemp("timer_api"))
+    keep = {}
+    designgen.write_design(d, seed=2041, gates=1500, keep=keep)
+    return d, keep
+
+
+def test_reports_match_the_reference(design):
+    from opentimer_b200.sizing import resize_trace, write_ops
+    from opentimer_b200.timer import Timer
+    d, keep = design
+    steps = resize_trace(keep, seed=11, steps=1, per_step=40)
+    out0 = os.path.join(d, "ref0.txt")
+    p = subprocess.run([EXE_REF, d, "cpu", out0], capture_output=True, text=True, timeout=600)
+    assert p.returncode == 0, p.stderr[-2000:]
+    ops = os.path.join(d, "ops.txt")
+    write_ops(ops, steps)
+    out1 = os.path.join(d, "ref1.txt")
+    p = subprocess.run([EXE_REF, d, "cpu", out1, f"repower={ops}"], capture_output=True,
+                       text=True, timeout=600)
+    assert p.returncode == 0, p.stderr[-2000:]
+    t = Timer(d, keep)
+    check_against(t, read_ref(out0))
+    for gate, cell in steps[0]:
+        t.repower_gate(gate, cell)
+    check_against(t, read_ref(out1))  # the queries apply the queued resizes first
+    with pytest.raises(ValueError):
+        t.repower_gate(steps[0][0][0], "DFF_X1")
