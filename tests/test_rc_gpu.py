@@ -95,12 +95,19 @@ def test_huge_nets_cluster_path(cuda, monkeypatch, cl):
     Every output is bit-identical to the one-CTA-per-net path (the sums are
     exact, so the thread count changes no bit)."""
     f = rcgen.forest(31, HUGE_SIZES, HUGE_KINDS)
+    ss, sn = rcgen.sinks_of(f)
+    slew = np.random.default_rng(3).uniform(5, 200, (f.num_nets, 4)).astype(np.float32)
+    slew[::3] *= -1
     monkeypatch.setenv("OTG_RC_HUGE_CLUSTER", "1")
-    one = run(f, cuda)
+    one = run(f, cuda, sinks=(ss, sn), slew=slew)
     monkeypatch.setenv("OTG_RC_HUGE_CLUSTER", cl)
-    b = run(f, cuda)
-    for q in ["node2bfs", "pid", "edges"] + Q:
+    b = run(f, cuda, sinks=(ss, sn), slew=slew)
+    for q in ["node2bfs", "pid", "edges", "sink_slew"] + Q:
         assert np.array_equal(getattr(b, q).cpu().numpy(), getattr(one, q).cpu().numpy()), q
+    # the sink slews are the reference's formula on our own impulses, bit for bit
+    imp = bfs_local(f.nodes_start, b.node2bfs.cpu().numpy(), b.impulse.cpu().numpy())
+    want = O.sink_slew(f, ss, sn, slew, imp)
+    assert np.array_equal(b.sink_slew.cpu().numpy().view(np.int32), want.view(np.int32))
     st, e, n2b, pid, depth = O.bfs(f)
     assert st == 0
     got_n2b = b.node2bfs.cpu().numpy()
