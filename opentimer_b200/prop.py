@@ -236,14 +236,16 @@ def _ranges(starts, sizes):
         np.repeat(np.asarray(starts, np.int64), sizes)
 
 
-def change_nets(spef_change, net_index, pin_caps):
+def change_nets(spef_change, net_index, pin_caps, with_ground=False):
     """Reads a change SPEF (read_spef output) against a design whose forest
     nets are named by net_index {name: forest net}.  Returns (nets, forest,
     node_of): the forest indices of the nets it names (unknown names are
     skipped, as Timer::_read_spef does, ot/timer/spef.cpp:40-53), their new
     trees as a forest in file order (nodes_start, edges, roots, res, cap
     with the pin caps added) for RcBatch.replace_nets, and node_of
-    {(forest net, pin name): local node} for the arcs into them."""
+    {(forest net, pin name): local node} for the arcs into them.  With
+    with_ground, a fourth item: the trees' SPEF ground caps alone [V', 4]
+    (the forest's cap before the pin caps were added)."""
     f = spef_change
     ns = np.asarray(f["nodes_start"], np.int64)
     keep = np.array([i for i, n in enumerate(f["net_names"]) if n in net_index], np.int64)
@@ -259,6 +261,8 @@ def change_nets(spef_change, net_index, pin_caps):
     forest = (sub_ns.astype(np.int32), f["edges"][edge_rows].copy(),
               np.asarray(f["roots"])[keep].astype(np.int32), f["res"][edge_rows].copy(),
               cap[node_rows].copy())
+    if with_ground:
+        return nets, forest, node_of, np.asarray(f["cap"], np.float32)[node_rows].copy()
     return nets, forest, node_of
 
 

@@ -27,7 +27,7 @@ import os
 import numpy as np
 
 from . import RcBatch, _ptr, _stream, check, designgen, lib
-from .prop import TimingGraph, attach_nets, rc_inputs
+from .prop import TimingGraph, attach_nets, change_nets, rc_inputs
 from .spef import read_spef
 
 NC = 4
@@ -70,6 +70,44 @@ class ResizeTable:
     def reset(self):
         """Every gate back at the cell the design was built with."""
         self.cell_of = list(self.cell0)
+
+    def current_pin_caps(self, design):
+        """pin_caps (designgen.pin_caps) for the gates' current cells."""
+        return designgen.pin_caps(dict(design, gates=[
+            (g, c, conn) for (g, _, conn), c in zip(design["gates"], self.cell_of)]))
+
+    def relayout(self, ns_old, ns_new, nets, ground, node_of_new):
+        """After a change SPEF replaced the trees of forest nets `nets`
+        (RcBatch.replace_nets: every net moves to the new layout ns_new;
+        the replaced ones have new local ids, node_of_new {(net, pin name):
+        node}, and new ground caps `ground`, their trees' rows in `nets`
+        order): the ground caps and the gate input pins' rows follow."""
+        ns_old, ns_new = np.asarray(ns_old, np.int64), np.asarray(ns_new, np.int64)
+        nets = np.asarray(nets, np.int64)
+        N = len(ns_old) - 1
+        changed = np.zeros(N, bool)
+        changed[nets] = True
+        net_of = np.repeat(np.arange(N), np.diff(ns_old))
+        keep = ~changed[net_of]
+        rows = np.arange(int(ns_old[-1]))[keep]
+        gcap = np.zeros((int(ns_new[-1]), NC), np.float32)
+        gcap[ns_new[net_of[keep]] + (rows - ns_old[net_of[keep]])] = self.gcap[rows]
+        g0 = 0
+        for i in nets.tolist():
+            n = int(ns_new[i + 1] - ns_new[i])
+            gcap[ns_new[i]:ns_new[i] + n] = ground[g0:g0 + n]
+            g0 += n
+        self.gcap = gcap
+        for gi, ins in enumerate(self.gate_inputs):
+            moved = []
+            for cp, row, net in ins:
+                if changed[net]:
+                    node = node_of_new.get((net, f"{self.gates[gi]}:{cp}"))
+                    if node is not None:
+                        moved.append((cp, int(ns_new[net] + node), net))
+                else:
+                    moved.append((cp, int(ns_new[net] + row - ns_old[net]), net))
+            self.gate_inputs[gi] = moved
 
     def updates(self, resizes):
         """Host arrays of one batch of resizes [(gate name or index, cell),
@@ -132,6 +170,36 @@ class SizingDesign:
 
     def updates(self, resizes):
         return self.table.updates(resizes)
+
+    def change_spef(self, path, stream=None):
+        """A change SPEF (Timer::read_spef + update_timing on the nets it
+        names, ot/timer/spef.cpp:40-53): the named nets get their new trees,
+        with the pin caps of the gates' current cells; every other net keeps
+        its tree and results (RcBatch.replace_nets); the net arcs into the
+        changed nets, the resize table's rows and the queries' node map
+        follow the new layout; then the design is propagated again.
+        Returns the forest indices of the changed nets."""
+        f = read_spef(path, r_scale=np.float32(1e-3))
+        net_index = {n: i for i, n in enumerate(self.net_names)}
+        nets, forest, node_of_c, ground = change_nets(
+            f, net_index, self.table.current_pin_caps(self.keep), with_ground=True)
+        if len(nets) == 0:
+            return nets
+        ns_old = self.nodes_start
+        self.batch = self.batch.replace_nets(nets, *forest, stream=stream)
+        ns_new = self.batch.nodes_start.cpu().numpy().astype(np.int64)
+        self.graph.change_nets(nets, node_of_c, self.names)
+        self.table.relayout(ns_old, ns_new, nets, ground, node_of_c)
+        changed = set(np.asarray(nets).tolist())
+        self.node_of = {k: v for k, v in self.node_of.items() if k[0] not in changed}
+        self.node_of.update(node_of_c)
+        self.nodes_start = ns_new
+        self.graph.propagate(self.batch, stream)
+        g = self.graph
+        check("otg_worst_slack", lib().otg_worst_slack(_ptr(g.out["slack"]), self.P,
+                                                       _ptr(self.scratch), _ptr(self.wns),
+                                                       _stream(stream)))
+        return nets
 
     # -------------------------------------------------------------- device
     def _launch(self, cap_row, cap_val, n_cap, arc_slot, arc_rec, n_arc, nets, n_nets_dev,

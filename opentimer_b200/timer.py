@@ -4,14 +4,15 @@ device (ot/timer/timer.hpp:41-140, timer.cpp).
     t = Timer(dirpath, keep)             # designgen.write_design's files + keep
     t.report_at("u12:ZN", MAX, RISE)     # arrival time, or None
     t.repower_gate("u12", "NAND2_X4")    # queued, as the Timer queues it
-    t.update_timing()                    # applies the queued resizes, re-times
+    t.read_spef("change.spef")           # queued: new parasitics of the nets it names
+    t.update_timing()                    # applies the queued operations, re-times
     t.report_wns(), t.report_tns(MAX)    # over the endpoints, as the Timer
     t.report_load("n42", MAX, FALL)      # the net's load (its RC root)
     t.rc_node("n42", "u7:A")             # load/delay/ldelay/impulse [2][2]
 
 Split and Tran are the reference's indices (MIN=0, MAX=1; RISE=0, FALL=1),
 corner c = split * 2 + tran.  A value the reference reports as an empty
-std::optional is None here.  Every query first applies pending resizes, as
+std::optional is None here.  Every query first applies the pending operations, as
 the reference's report_* first runs update_timing (timer.cpp:1705); the
 results come from the device (one read per update, kept until the next).
 
@@ -37,7 +38,7 @@ class Timer:
         self._pin = {n: i for i, n in enumerate(self._d.names)}
         self._net = {n: i for i, n in enumerate(self._d.net_names)}
         self._gate_cell = {g: c for g, c, _ in keep["gates"]}
-        self._pending = []
+        self._pending = []  # queued operations, in order: ("resize", (gate, cell)) | ("spef", path)
         self._res = None  # host copy of the last update's pin results
         self._rc = None   # host copy of the RC outputs, read on demand
 
@@ -51,17 +52,36 @@ class Timer:
         if cell_family(cell) != cell_family(self._gate_cell[gate]):
             raise ValueError(f"{gate}: {self._gate_cell[gate]} -> {cell} changes the function")
         self._gate_cell[gate] = cell
-        self._pending.append((gate, cell))
+        self._pending.append(("resize", (gate, cell)))
+        return self
+
+    def read_spef(self, path):
+        """Queues a change SPEF (Timer::read_spef, ot/timer/spef.cpp:40-53):
+        at the next update the nets it names get their new trees (unknown
+        names are skipped, as the reference does) and only they are re-timed
+        in the RC pass."""
+        self._pending.append(("spef", path))
         return self
 
     def update_timing(self):
-        """Applies the queued resizes as one batch (new pin caps and cell-arc
-        timing on the device, the dirty nets re-timed, propagation) and
-        drops the host copies of older results."""
-        if self._pending:
-            self._d.resize(self._pending)
-            self._pending = []
-            self._res = self._rc = None
+        """Applies the queued operations in order -- each run of resizes as
+        one batch (new pin caps and cell-arc timing on the device, the dirty
+        nets re-timed, propagation), each change SPEF by itself -- and drops
+        the host copies of older results."""
+        if not self._pending:
+            return self
+        run = []
+        for kind, arg in self._pending + [("end", None)]:
+            if kind == "resize":
+                run.append(arg)
+                continue
+            if run:
+                self._d.resize(run)
+                run = []
+            if kind == "spef":
+                self._d.change_spef(arg)
+        self._pending = []
+        self._res = self._rc = None
         return self
 
     def _results(self):

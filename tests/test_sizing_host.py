@@ -73,3 +73,58 @@ def test_resize_trace_keeps_functions_and_changes_drive():
         for g, c in step:
             assert cell_family(c) == cell_family(cur[g]) and c != cur[g]
             cur[g] = c
+
+
+def test_relayout_after_change_spef_equals_a_table_built_on_the_new_trees(tmp_path):
+    """A change SPEF replaces some nets' trees (new node counts, new pin
+    nodes): ResizeTable.relayout must leave the table exactly as one built
+    from the start on the spliced parasitics, and a resize batch after it
+    must write the caps rc_inputs gives for the spliced trees."""
+    from opentimer_b200.prop import change_nets
+    d = str(tmp_path)
+    keep = {}
+    designgen.write_design(d, seed=13, gates=400, keep=keep)
+    arrays, _, _ = designgen.timing_graph(keep)
+    f = read_spef(os.path.join(d, "design.spef"), r_scale=np.float32(1e-3))
+    _, node_of = rc_inputs(f, designgen.pin_caps(keep))
+    table = ResizeTable(keep, arrays, f, node_of)
+    steps = resize_trace(keep, seed=4, steps=2, per_step=30)
+    table.updates(steps[0])  # resizes before the change: its pin caps follow them
+    path = os.path.join(d, "change.spef")
+    designgen.change_spef(keep, path, frac=0.1, seed=9)
+    fc = read_spef(path, r_scale=np.float32(1e-3))
+    net_index = {n: i for i, n in enumerate(f["net_names"])}
+    nets, forest, node_of_c, ground = change_nets(
+        fc, net_index, table.current_pin_caps(keep), with_ground=True)
+    assert len(nets) > 10
+    ns_old = np.asarray(f["nodes_start"], np.int64)
+    sizes = np.diff(ns_old)
+    sizes[nets] = np.diff(forest[0].astype(np.int64))
+    ns_new = np.zeros(len(sizes) + 1, np.int64)
+    np.cumsum(sizes, out=ns_new[1:])
+    table.relayout(ns_old, ns_new, nets, ground, node_of_c)
+    # the spliced parasitics: changed nets' ground caps from the change file
+    sub = np.asarray(forest[0], np.int64)
+    slot = {int(n): k for k, n in enumerate(nets.tolist())}
+    gcap = np.concatenate([ground[sub[slot[i]]:sub[slot[i] + 1]] if i in slot
+                           else f["cap"][ns_old[i]:ns_old[i + 1]] for i in range(len(sizes))])
+    spliced = {"cap": gcap, "nodes_start": ns_new, "net_names": f["net_names"]}
+    node_of2 = {k: v for k, v in node_of.items() if k[0] not in slot}
+    node_of2.update(node_of_c)
+    fresh = ResizeTable(keep, arrays, spliced, node_of2)
+    assert np.array_equal(table.gcap.view(np.int32), fresh.gcap.view(np.int32))
+    assert table.gate_inputs == fresh.gate_inputs
+    # a resize after the change writes what a cap build on the new trees gives
+    cap_row, cap_val, _, _, _ = table.updates(steps[1])
+    cells = {g: c for g, c, _ in keep["gates"]}
+    cells.update(dict(steps[0]))
+    cells.update(dict(steps[1]))
+    keep2 = dict(keep, gates=[(g, cells[g], conn) for g, _, conn in keep["gates"]])
+    pin_caps = designgen.pin_caps(keep2)
+    want = gcap.copy()
+    written = set(cap_row.tolist())
+    for (i, pin), node in node_of2.items():
+        c = pin_caps.get(pin)
+        if c is not None and ns_new[i] + node in written:
+            want[ns_new[i] + node] += np.float32(c)
+    assert np.array_equal(cap_val.view(np.int32), want[cap_row].view(np.int32))

@@ -1,6 +1,7 @@
 """The Timer-style host layer (opentimer_b200.timer.Timer) against the
 reference Timer (oracle/_ref/ot_run_ref, its CPU path) on the same design,
-after the first full update and after a batch of repower_gate calls:
+after the first full update, after a batch of repower_gate calls, and
+after a change SPEF followed by a resize batch:
 
 * report_at / report_slew / report_rat / report_slack of every pin within
   the pin tolerance of tests/helpers.pin_err;
@@ -118,3 +119,34 @@ def test_reports_match_the_reference(design):
     check_against(t, read_ref(out1))  # the queries apply the queued resizes first
     with pytest.raises(ValueError):
         t.repower_gate(steps[0][0][0], "DFF_X1")
+
+
+def test_change_spef_then_resizes(design):
+    """read_spef of a change SPEF (5% of the nets get new trees), then a
+    resize batch on the new layout: every report against the reference
+    Timer after the same two updates."""
+    from opentimer_b200.sizing import resize_trace, write_ops
+    from opentimer_b200.timer import Timer
+    d, keep = design
+    change = os.path.join(d, "change.spef")
+    changed = designgen.change_spef(keep, change, frac=0.05, seed=5)
+    steps = resize_trace(keep, seed=12, steps=1, per_step=40)
+    ops = os.path.join(d, "ops_after_change.txt")
+    write_ops(ops, steps)
+    out1 = os.path.join(d, "ref_change.txt")
+    p = subprocess.run([EXE_REF, d, "cpu", out1, f"change={change}"], capture_output=True,
+                       text=True, timeout=600)
+    assert p.returncode == 0, p.stderr[-2000:]
+    out2 = os.path.join(d, "ref_change_repower.txt")
+    p = subprocess.run([EXE_REF, d, "cpu", out2, f"change={change}", f"repower={ops}"],
+                       capture_output=True, text=True, timeout=600)
+    assert p.returncode == 0, p.stderr[-2000:]
+    t = Timer(d, keep)
+    before = {n: t.report_load(n, 1, 0) for n in changed}
+    t.read_spef(change)
+    check_against(t, read_ref(out1))
+    after = {n: t.report_load(n, 1, 0) for n in changed}
+    assert sum(before[n] != after[n] for n in changed) > 0.9 * len(changed)
+    for gate, cell in steps[0]:
+        t.repower_gate(gate, cell)
+    check_against(t, read_ref(out2))
