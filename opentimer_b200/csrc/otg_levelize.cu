@@ -295,9 +295,12 @@ __global__ void __launch_bounds__(LT) levelize_kernel(int n, const int* fanin_st
 // whose fanout counter reaches zero sets its bit and bumps its owner's
 // count through distributed shared memory.  A level ends at the hardware
 // cluster barrier (barrier.cluster, release/acquire) instead of the global
-// barrier, and the counts and bitmaps never leave the SMs, so a level costs
-// the three dependent global accesses of its expansion (fanin_start,
-// fanin, the counter) plus on-chip work.  The emission rule is the one
+// barrier, and the counts and bitmaps never leave the SMs.  Where the
+// ranges' fanout counters fit beside them (32 ints per bitmap word), the
+// counters live in their owner's shared memory too, and a level costs the
+// dependent global loads of its expansion (the fanin entry; the fanin
+// range, loaded speculatively beside the decrement) plus on-chip work.
+// The emission rule is the one
 // above (seed order, then ascending pin index per level, CTA ranges in rank
 // order), so both paths give identical outputs.
 //
@@ -350,6 +353,8 @@ namespace cg = cooperative_groups;
 // its levels from one place -- would otherwise expand the next one alone.)
 struct ClNext {
   unsigned* bm;  // next level's bitmap (this CTA's address; mapped to the owner)
+  int* scnt;     // the fanin counters of the CTA's range (mapped to the owner), or null:
+                 // the counters are the global cnt[]
   int cshift;    // log2 of the words per CTA range: the owner of word w is w >> cshift
   int sshift;    // log2 of the cluster size
   int* rc;       // next level's per-owner counts [16] (every CTA keeps a copy)
@@ -363,20 +368,28 @@ struct ClNext {
 // distinct pin v also loads v's fanin range, in flight with the decrement,
 // so a pin that becomes ready is expanded next level without another
 // global round trip; a full list raises the next level's overflow flag in
-// every CTA, and that level then expands from the bitmaps instead.
+// every CTA, and that level then expands from the bitmaps instead.  The
+// counter lives in the owner's shared memory where the ranges fit there
+// (a distributed-shared-memory atomic instead of an L2 round trip on every
+// level's critical path).  The warp's pins that became ready add to the
+// per-owner counts of every CTA once per owner.
 __device__ __forceinline__ void decrement_cl(int v, bool ok, const int* fanin_start, int* cnt,
                                              const ClNext& nx, const cg::cluster_group& cl) {
   const int lane = threadIdx.x & 31;
   const unsigned peers = __match_any_sync(FULL, ok ? v : -2 - lane);
+  bool ready = false;
+  int owner = 0;
   if (ok && (__ffs(peers) - 1 == lane)) {
     const int k = __popc(peers);
     const int s0 = __ldg(fanin_start + v), s1 = __ldg(fanin_start + v + 1);
-    const int old = atomicSub(&cnt[v], k);
+    const int w = v >> 5;
+    owner = w >> nx.cshift;
+    int* c = nx.scnt ? cl.map_shared_rank(nx.scnt + (v - (owner << (nx.cshift + 5))), owner)
+                     : cnt + v;
+    const int old = atomicSub(c, k);
     if (old > 0 && old - k <= 0) {
-      const int w = v >> 5, owner = w >> nx.cshift;
+      ready = true;
       atomicOr(cl.map_shared_rank(nx.bm, owner) + (w - (owner << nx.cshift)), 1u << (v & 31));
-      const int S = (int)cl.num_blocks();
-      for (int i = 0; i < S; ++i) atomicAdd(cl.map_shared_rank(nx.rc + owner, i), 1);
       const int t = nx.sshift ? (int)(((unsigned)v * 0x9E3779B1u) >> (32 - nx.sshift)) : 0;
       const int slot = atomicAdd(cl.map_shared_rank(nx.lcnt, t), 1);
       if (slot < nx.cap) {
@@ -386,18 +399,26 @@ __device__ __forceinline__ void decrement_cl(int v, bool ok, const int* fanin_st
       }
     }
   }
+  const unsigned grp = __match_any_sync(FULL, ready ? owner : -1 - lane);
+  if (ready && (__ffs(grp) - 1 == lane)) {
+    const int k = __popc(grp), S = (int)cl.num_blocks();
+    for (int i = 0; i < S; ++i) atomicAdd(cl.map_shared_rank(nx.rc + owner, i), k);
+  }
 }
 
 template <int CT>
 __global__ void __launch_bounds__(CT, 1) levelize_cluster_kernel(
     int n, const int* fanin_start, const int* fanin, const int* out_deg, const int* frontier0,
     int first_size, int* order, int* level, int* level_ends, int* counts, LvCtl* ctl, int* cnt,
-    int cshift, int lst_cap) {
+    int cshift, int lst_cap, int scnt_on) {
   const int C = 1 << cshift;  // bitmap words per CTA range
   extern __shared__ unsigned lv_sm[];
   unsigned* const bm0 = lv_sm;  // level L's ready pins: bm0 for even L, bm1 for odd
   unsigned* const bm1 = lv_sm + C;
-  int2* const lst0 = (int2*)(lv_sm + 2 * C);  // fanin ranges to expand at even / odd levels
+  // with scnt_on: the fanin counters of the range's 32*C pins
+  int* const scnt = scnt_on ? (int*)(lv_sm + 2 * C) : nullptr;
+  // fanin ranges to expand at even / odd levels
+  int2* const lst0 = (int2*)(lv_sm + 2 * C + (scnt_on ? 32 * C : 0));
   int2* const lst1 = lst0 + lst_cap;
   // per-level scalars in three rotating slots (this level, the next, the
   // one after): a slot is cleared a level before anything adds to it, so
@@ -415,9 +436,14 @@ __global__ void __launch_bounds__(CT, 1) levelize_cluster_kernel(
   const int lane = tid & 31, w = tid >> 5;
 
   for (int v = gtid; v < n; v += gstride) {
-    cnt[v] = out_deg[v];
+    if (!scnt) cnt[v] = out_deg[v];
     level[v] = -1;
   }
+  if (scnt)
+    for (int j = tid; j < 32 * C; j += CT) {
+      const int v = (r << (cshift + 5)) + j;
+      scnt[j] = v < n ? out_deg[v] : 0;
+    }
   for (int i = tid; i < 2 * C; i += CT) lv_sm[i] = 0u;
   if (tid < 48) rc[tid / 16][tid % 16] = 0;
   if (tid < 3) { lcnt[tid] = 0; ovf[tid] = 0; }
@@ -427,7 +453,13 @@ __global__ void __launch_bounds__(CT, 1) levelize_cluster_kernel(
     order[k] = v;
     if ((unsigned)v < (unsigned)n) {
       level[v] = 0;
-      cnt[v] = INT_MAX;  // after the counters' fill (cluster barrier above)
+      // after the counters' fill (cluster barrier above)
+      if (scnt) {
+        const int owner = v >> (cshift + 5);
+        *cl.map_shared_rank(scnt + (v - (owner << (cshift + 5))), owner) = INT_MAX;
+      } else {
+        cnt[v] = INT_MAX;
+      }
     } else {
       atomicCAS(&ctl->status, 0, (int)OTG_ERR_INVALID);
     }
@@ -443,7 +475,7 @@ __global__ void __launch_bounds__(CT, 1) levelize_cluster_kernel(
   cl.sync();
   // expand the seed into level 1 (bm1, slot 1, lst1)
   {
-    const ClNext nx{bm1, cshift, sshift, rc[1], lst1, &lcnt[1], &ovf[1], lst_cap};
+    const ClNext nx{bm1, scnt, cshift, sshift, rc[1], lst1, &lcnt[1], &ovf[1], lst_cap};
     for (int k0 = r * CT; k0 < first_size; k0 += gstride) {
       const int k = k0 + tid;
       const bool act = k < first_size && (unsigned)order[k] < (unsigned)n;
@@ -472,7 +504,7 @@ __global__ void __launch_bounds__(CT, 1) levelize_cluster_kernel(
     const int par = L & 1;
     unsigned* cur = par ? bm1 : bm0;
     int2* lcur = par ? lst1 : lst0;
-    const ClNext nx{par ? bm0 : bm1, cshift,        sshift,        rc[q_next],
+    const ClNext nx{par ? bm0 : bm1,   scnt,          cshift,       sshift, rc[q_next],
                     par ? lst0 : lst1, &lcnt[q_next], &ovf[q_next], lst_cap};
     if (tid < 16) rc[q_free][tid] = 0;  // read a level ago; added to from the next level on
     if (tid == 0) {
@@ -636,13 +668,18 @@ __global__ void __launch_bounds__(CT, 1) levelize_cluster_kernel(
   cl.sync();  // no CTA leaves while another may still read its counts
 }
 
-// Dynamic shared memory of the cluster path: both bitmaps (C words each)
-// and two lists of at least kLstMin fanin ranges (8 bytes each); the lists
-// take what is left of kClusterSmemMax.
+// Dynamic shared memory of the cluster path: both bitmaps (C words each),
+// optionally the range's fanin counters (32*C ints), and two lists of at
+// least kLstMin fanin ranges (8 bytes each); the lists take what is left of
+// kClusterSmemMax.
 constexpr size_t kClusterSmemMax = 200 * 1024;
 constexpr int kLstMin = kCtMax;
-size_t lv_cluster_smem(int C) { return (size_t)(2 * C + 4 * kLstMin) * 4; }
-int lv_lst_cap(int C) { return ((int)(kClusterSmemMax / 4) - 2 * C) / 4; }
+size_t lv_cluster_smem(int C, bool scnt) {
+  return (size_t)(2 * C + (scnt ? 32 * C : 0) + 4 * kLstMin) * 4;
+}
+int lv_lst_cap(int C, bool scnt) {
+  return ((int)(kClusterSmemMax / 4) - 2 * C - (scnt ? 32 * C : 0)) / 4;
+}
 
 constexpr int kWidths[4] = {128, 256, 512, 1024};
 const void* cluster_fn(int wi) {
@@ -706,6 +743,7 @@ LvDev& lv_dev() {
 // threads, each owning 2^cshift bitmap words.  S = 0: the cooperative path.
 struct ClPlan {
   int S = 0, wi = 0, cshift = 0;
+  bool scnt = false;  // the fanin counters in shared memory
 };
 // Default: the largest cluster the device places (16 CTAs on B200) of 256
 // threads each, for graphs whose ranges then hold at most kClusterMaxWords
@@ -737,9 +775,15 @@ ClPlan lv_cluster_plan(int n, const LvDev& d) {
   }
   int cs = 0;
   while ((1 << cs) * s < nw) ++cs;
-  if (lv_cluster_smem(1 << cs) > kClusterSmemMax) return ClPlan{};
+  if (lv_cluster_smem(1 << cs, false) > kClusterSmemMax) return ClPlan{};
   p.S = s;
   p.cshift = cs;
+  // the counters go on chip where they fit (ranges of up to 32k pins:
+  // graphs of about half a million pins); OTG_LEVELIZE_SCNT=0 keeps them in
+  // global memory
+  p.scnt = lv_cluster_smem(1 << cs, true) <= kClusterSmemMax;
+  if (const char* e = std::getenv("OTG_LEVELIZE_SCNT"))
+    if (std::atoi(e) == 0) p.scnt = false;
   return p;
 }
 
@@ -799,7 +843,8 @@ otg_status otg_levelize(int32_t n, int32_t num_edges, const int32_t* fanin_start
     otg::LvCtl* ctl = (otg::LvCtl*)(ws + l.ctl);
     int* cnt = (int*)(ws + l.cnt);
     int cshift = pl.cshift;
-    int lst_cap = otg::lv_lst_cap(1 << pl.cshift);
+    int lst_cap = otg::lv_lst_cap(1 << pl.cshift, pl.scnt);
+    int scnt_on = pl.scnt ? 1 : 0;
     cudaLaunchConfig_t cfg = {};
     cudaLaunchAttribute at[1];
     at[0].id = cudaLaunchAttributeClusterDimension;
@@ -814,7 +859,7 @@ otg_status otg_levelize(int32_t n, int32_t num_edges, const int32_t* fanin_start
     cfg.numAttrs = 1;
     void* args[] = {&n,          (void*)&fanin_start, (void*)&fanin, (void*)&out_deg,
                     (void*)&frontier0, &first_size, &order, &level, &level_ends, &counts,
-                    &ctl,        &cnt,        &cshift,       &lst_cap};
+                    &ctl,        &cnt,        &cshift,       &lst_cap,  &scnt_on};
     const cudaError_t e = cudaLaunchKernelExC(&cfg, otg::cluster_fn(pl.wi), args);
     otg::count_launch();
     return e == cudaSuccess ? OTG_OK : OTG_ERR_CUDA;

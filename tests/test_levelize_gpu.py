@@ -112,15 +112,20 @@ def test_host_path_and_reference_symbol(cuda):
 def test_every_path_same_levels(cuda, monkeypatch, seed, n, e, L):
     """The cluster path (one thread-block cluster, ready bitmaps in
     distributed shared memory) and the cooperative path give identical
-    outputs, at every cluster size and CTA width.  A cluster of one CTA on
-    the 3-level graph readies more pins per level than its on-chip list of
-    fanin ranges holds, so the next level takes the overflow expansion."""
+    outputs, at every cluster size and CTA width, with the fanout counters
+    in shared memory (where the ranges fit: 4 and 16 CTAs here) or in
+    global memory.  On the 3-level graph a cluster of one CTA, and one of
+    four with its counters on chip, ready more pins per level than their
+    on-chip lists of fanin ranges hold, so the next level takes the
+    overflow expansion."""
     fs, fi, od, f0 = rcgen.pin_dag(seed, n, e, L)
     ref = None
-    for cl, ct in (("0", "256"), ("1", "256"), ("4", "128"), ("16", "256"), ("16", "1024")):
+    for cl, ct, sc in (("0", "256", "1"), ("1", "256", "1"), ("4", "128", "1"),
+                       ("16", "256", "1"), ("16", "256", "0"), ("16", "1024", "1")):
         monkeypatch.setenv("OTG_LEVELIZE_CLUSTER", cl)
         monkeypatch.setenv("OTG_LEVELIZE_CT", ct)
+        monkeypatch.setenv("OTG_LEVELIZE_SCNT", sc)
         out = check_vs_oracle(cuda, fs, fi, od, f0)
         if ref is None:
             ref = out
-        assert all(np.array_equal(a, b) for a, b in zip(out, ref)), (cl, ct)
+        assert all(np.array_equal(a, b) for a, b in zip(out, ref)), (cl, ct, sc)
