@@ -437,6 +437,16 @@ otg_status otg_propagate(const otg_prop_graph* graph, const otg_prop_rc* rc,
                          float* rat, float* slack, void* workspace, size_t workspace_bytes,
                          otg_stream_t stream);
 otg_status otg_prop_status(const void* workspace, otg_stream_t stream);
+/* The arc delays the last propagation computed, as the Timer keeps them in
+ * Arc::_delay[el][frf][trf] (ot/timer/arc.hpp): *arc_delay is set to a
+ * device array [num_arcs][8] inside the workspace, entry
+ * (el << 2) | (frf << 1) | trf, NaN where the reference's value is empty
+ * (a net arc between different transitions, a transition the cell arc's
+ * timing sense does not have, a constraint arc, no input slew).  Valid
+ * until the next propagation on the same workspace.  The reference's path
+ * reports (Timer::report_timing, ot/timer/path.cpp:365-420) walk these. */
+otg_status otg_prop_arc_delays(const void* workspace, size_t workspace_bytes, int32_t num_arcs,
+                               const float** arc_delay);
 /* The same over a graph that is the union of independent designs (no arc
  * between two of them): pin_group [P] gives each pin its design, and only
  * the pins whose group_active[design] is nonzero are propagated (and

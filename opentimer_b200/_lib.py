@@ -33,7 +33,7 @@ C_SYMBOLS = [
     "otg_prop_status", "otg_rc_move_nets", "otg_spef_names", "otg_apply_updates",
     "otg_worst_slack", "otg_spef_write", "otg_fanin_csr_workspace_size", "otg_fanin_csr",
     "otg_fanin_csr_status", "otg_propagate_groups", "otg_worst_slack_groups",
-    "otg_propagate_items",
+    "otg_propagate_items", "otg_prop_arc_delays",
 ]
 # The reference-compatible C++ entry points (include/otg_compat.hpp), by
 # their Itanium-mangled names.
@@ -148,6 +148,7 @@ def lib():
         L.otg_fanin_csr_status.argtypes = [P, P]
         L.otg_propagate_groups.argtypes = [P, P, P, P, P, P, P, P, P, P, P, S, P]
         L.otg_propagate_items.argtypes = [P, P, P, I32, P, P, P, P, P, S, P]
+        L.otg_prop_arc_delays.argtypes = [P, S, I32, ctypes.POINTER(P)]
         L.otg_worst_slack_groups.argtypes = [P, I32, P, P, I32, P, P, P]
         L.otg_spef_names.argtypes = [P, P, PS]
         L.otg_spef_free.restype = None
@@ -164,7 +165,7 @@ def lib():
                      "otg_rc_move_nets", "otg_spef_names", "otg_apply_updates",
                      "otg_worst_slack", "otg_spef_write", "otg_fanin_csr_workspace_size",
                      "otg_fanin_csr", "otg_fanin_csr_status", "otg_propagate_groups",
-                     "otg_worst_slack_groups", "otg_propagate_items"]:
+                     "otg_worst_slack_groups", "otg_propagate_items", "otg_prop_arc_delays"]:
             getattr(L, name).restype = ctypes.c_int
         _lib = L
     return _lib

@@ -672,6 +672,14 @@ otg_status otg_propagate_items(const otg_prop_graph* g, const otg_prop_rc* rc,
                         workspace, workspace_bytes, stream, items, num_items);
 }
 
+otg_status otg_prop_arc_delays(const void* workspace, size_t workspace_bytes, int32_t num_arcs,
+                               const float** arc_delay) {
+  if (!workspace || !arc_delay || num_arcs < 0) return OTG_ERR_INVALID;
+  if (workspace_bytes < 256 + 32 * (size_t)num_arcs) return OTG_ERR_WORKSPACE;
+  *arc_delay = (const float*)((const char*)workspace + 256);
+  return OTG_OK;
+}
+
 otg_status otg_prop_status(const void* workspace, otg_stream_t stream) {
   if (!workspace) return OTG_ERR_INVALID;
   otg::GridCtl h;

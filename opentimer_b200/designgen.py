@@ -163,7 +163,8 @@ def liberty(seed, scale, name, cells=None):
         text += _arc(rng, "A2", "negative_unate", scale, groups=c["timings"]["ZN"])
         text += "  }\n}\n"
     # DFF_X1
-    ff = cells["DFF_X1"] = {"caps": {"CK": caps[5], "D": caps[6]}, "timings": {"D": [], "Q": []}}
+    ff = cells["DFF_X1"] = {"caps": {"CK": caps[5], "D": caps[6]}, "timings": {"D": [], "Q": []},
+                            "clock": ("CK",)}
     text += "cell(DFF_X1) {\n  area : 5;\n"
     text += '  ff(IQ, IQN) {\n    next_state : "D";\n    clocked_on : "CK";\n  }\n'
     text += _pin_in("CK", caps[5], clock=True) + "  }\n"

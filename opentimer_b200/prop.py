@@ -183,6 +183,19 @@ class TimingGraph:
         self.dev["arc_node"][arcs] = torch.as_tensor(np.asarray(nodes, np.int32),
                                                      device=arcs.device)
 
+    def arc_delays(self):
+        """The arc delays of the last propagation on the host, [A][2][2][2]
+        by (split, from transition, to transition) -- Arc::_delay, NaN where
+        the reference's value is empty (otg_prop_arc_delays)."""
+        import torch
+        self.check()
+        ptr = ctypes.c_void_p()
+        check("otg_prop_arc_delays", lib().otg_prop_arc_delays(
+            _ptr(self.workspace), self.workspace.numel(), self.A, ctypes.byref(ptr)))
+        off = ptr.value - self.workspace.data_ptr()
+        raw = self.workspace[off:off + 32 * self.A]
+        return raw.view(torch.float32).cpu().numpy().reshape(self.A, 2, 2, 2)
+
     def check(self, stream=None):
         """Synchronizes; raises if a bounded wait of the last propagation
         gave up (OTG_ERR_TIMEOUT)."""

@@ -9,6 +9,7 @@ device (ot/timer/timer.hpp:41-140, timer.cpp).
     t.report_wns(), t.report_tns(MAX)    # over the endpoints, as the Timer
     t.report_load("n42", MAX, FALL)      # the net's load (its RC root)
     t.rc_node("n42", "u7:A")             # load/delay/ldelay/impulse [2][2]
+    t.report_timing(10)                  # the 10 worst paths (paths.Path)
 
 Split and Tran are the reference's indices (MIN=0, MAX=1; RISE=0, FALL=1),
 corner c = split * 2 + tran.  A value the reference reports as an empty
@@ -25,6 +26,7 @@ corners' values the same way (report_wns / report_tns, timer.cpp:1456-
 """
 import numpy as np
 
+from .paths import PathGraph
 from .sizing import SizingDesign, cell_family
 
 MIN, MAX = 0, 1
@@ -41,6 +43,8 @@ class Timer:
         self._pending = []  # queued operations, in order: ("resize", (gate, cell)) | ("spef", path)
         self._res = None  # host copy of the last update's pin results
         self._rc = None   # host copy of the RC outputs, read on demand
+        self._pg = None   # the path search's view of the graph (paths.PathGraph)
+        self._pg_fresh = False
 
     # ------------------------------------------------------------- updates
     def repower_gate(self, gate, cell):
@@ -82,6 +86,7 @@ class Timer:
                 self._d.change_spef(arg)
         self._pending = []
         self._res = self._rc = None
+        self._pg_fresh = False
         return self
 
     def _results(self):
@@ -166,3 +171,41 @@ class Timer:
             if len(s):
                 vals.append(float(np.sum(s[s < 0.0], dtype=np.float32)))
         return float(np.sum(np.asarray(vals, np.float32), dtype=np.float32)) if vals else None
+
+    # --------------------------------------------------------------- paths
+    def _path_graph(self):
+        if self._pg is None:
+            d, keep = self._d, self._d.keep
+            g = d.graph
+            frm = g.dev["arc_from"][:g.A].cpu().numpy()
+            to = g.dev["arc_to"][:g.A].cpu().numpy()
+            tests = g.dev["test_arc"][:g.T].cpu().numpy()
+            # data-path sources (Pin::is_datapath_source, ot/timer/pin.cpp:
+            # 170-190): pins without fanin, clock pins of cells, primary inputs
+            source = np.bincount(to, minlength=d.P) == 0
+            lib = keep["libs"]["late"]
+            for inst, cell, _ in keep["gates"]:
+                for cp in lib[cell].get("clock", ()):
+                    i = self._pin.get(f"{inst}:{cp}")
+                    if i is not None:
+                        source[i] = True
+            for p in keep.get("ports_in", ()):
+                if p in self._pin:
+                    source[self._pin[p]] = True
+            self._pg = PathGraph(d.names, frm, to, tests, source, d.endpoints)
+        if not self._pg_fresh:
+            r = self._results()
+            self._pg.values(self._d.graph.arc_delays(), r["at"], r["rat"], r["slack"])
+            self._pg_fresh = True
+        return self._pg
+
+    def report_timing(self, K, el=None, rf=None):
+        """The K worst paths (Timer::report_timing(K[, el][, rf]),
+        ot/timer/path.cpp:365-420), by ascending slack: paths.Path(slack,
+        endpoint (pin, split, transition), points [(pin, transition,
+        arrival)]).  K = 1 gives the worst endpoint's path with the
+        endpoint's slack; larger K the paths of negative slack only, as the
+        reference's prefix-tree search does.  The search runs on the host
+        over the device's arrival times and arc delays (paths.py)."""
+        self.update_timing()
+        return self._path_graph().report_timing(int(K), el, rf)

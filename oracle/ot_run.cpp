@@ -2,11 +2,12 @@
 // dumps its results.  TEST INFRASTRUCTURE ONLY (the full-update parity check).
 //
 //   ot_run <dir> cpu|cuda <out.txt> [graph.txt] [change=<spef>]...
-//          [repower=<ops> [dump_every=<k>]]
+//          [repower=<ops> [dump_every=<k>]] [paths=<K>]
 //
 // graph.txt (optional) is the Timer's timing graph, for the GPU propagation
 // check: pins, arcs (net arcs with their net, cell arcs with one timing
-// record per split), timing records (sense, edge, constraint flag, six
+// record per split; each with the delays of the last update), the
+// data-path sources, timing records (sense, edge, constraint flag, six
 // LUT ids), LUTs (variable order, indices, values), timing tests, the clock
 // period and the primary-input/-output assertions, all by pin index.
 // <dir> holds early.lib, late.lib, design.v, design.spef, design.timing.
@@ -21,6 +22,8 @@
 // seconds of every step go to stdout ("repower_step_s <k> <s>"); with
 // dump_every=<k> the pins (P lines) after every k-th step go to
 // <out>.step<k>.
+// paths=<K>: after the updates, Timer::report_timing(K), the K worst
+// paths, to the output (T and Q lines).
 // The same Timer sources are linked twice (oracle/Makefile): with the
 // reference's own CUDA module (ot_run_ref) and with libotg in its place
 // (ot_run_otg), so "cuda" runs either the reference kernels or ours behind
@@ -32,6 +35,8 @@
 //   K <pin> cap[4]                                          (pin caps)
 //   L <net> report_load[4]
 //   N <split> <tran> report_wns report_tns                   (per corner)
+//   T <k> <slack> <split> <points>                           (paths=K: path k,
+//   Q <k> <pin> <tran> <at>                                   then its points)
 //   S <net> <num nodes> <root id>                           (cuda only:
 //   E <net> <edge k> <s> <t> <res>                           the flat
 //   C <net> <id> cap[4]                                      storage)
@@ -128,8 +133,16 @@ static void dump_graph(ot::Timer& timer, const char* path) {
       auto tv = std::get<ot::TimingView>(arc._handle);
       std::fprintf(f, " cell - %d %d\n", timing_id(tv[ot::MIN]), timing_id(tv[ot::MAX]));
     }
+    // the delays the last update left on the arc, (split, from, to transition)
+    std::fprintf(f, "d %d", k);
+    for (int el = 0; el < 2; ++el)
+      for (int fr = 0; fr < 2; ++fr)
+        for (int tr = 0; tr < 2; ++tr) put(f, arc._delay[el][fr][tr]);
+    std::fprintf(f, "\n");
     ++k;
   }
+  for (size_t i = 0; i < pins.size(); ++i)  // data-path sources of the path search
+    if (pins[i] && pins[i]->is_datapath_source()) std::fprintf(f, "z %zu\n", i);
   for (auto& [name, pin] : timer._pins)
     for (auto* test : pin._tests) std::fprintf(f, "s %d\n", aid[&test->_arc]);
   for (size_t i = 0; i < timings.size(); ++i) {
@@ -176,11 +189,13 @@ int main(int argc, char** argv) {
   std::vector<std::string> changes;
   std::string repower;
   int dump_every = 0;
+  int num_paths = 0;
   for (int a = 4; a < argc; ++a) {
     const std::string s = argv[a];
     if (s.rfind("change=", 0) == 0) changes.push_back(s.substr(7));
     else if (s.rfind("repower=", 0) == 0) repower = s.substr(8);
     else if (s.rfind("dump_every=", 0) == 0) dump_every = std::atoi(s.c_str() + 11);
+    else if (s.rfind("paths=", 0) == 0) num_paths = std::atoi(s.c_str() + 6);
     else graph_path = argv[a];
   }
   ot::Timer timer;
@@ -346,6 +361,16 @@ int main(int argc, char** argv) {
         std::fprintf(f, "B %s %s %d %d\n", nname.c_str(), names[k].c_str(), slot,
                      slot == 0 ? 0 : st.rct_pid[base + slot]);
       }
+    }
+  }
+  if (num_paths > 0) {
+    const std::vector<ot::Path> paths = timer.report_timing((size_t)num_paths);
+    for (size_t k = 0; k < paths.size(); ++k) {
+      const ot::Path& p = paths[k];
+      std::fprintf(f, "T %zu %.9g %d %zu\n", k, p.slack, (int)p.endpoint->_el, p.size());
+      for (const ot::Point& pt : p)
+        std::fprintf(f, "Q %zu %s %d %.9g\n", k, pt.pin.name().c_str(), (int)pt.transition,
+                     pt.at);
     }
   }
   std::fclose(f);

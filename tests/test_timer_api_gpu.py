@@ -1,7 +1,8 @@
 """The Timer-style host layer (opentimer_b200.timer.Timer) against the
 reference Timer (oracle/_ref/ot_run_ref, its CPU path) on the same design,
 after the first full update, after a batch of repower_gate calls, and
-after a change SPEF followed by a resize batch:
+after a change SPEF followed by a resize batch, and report_timing (the K
+worst paths) against the reference's, before and after a resize batch:
 
 * report_at / report_slew / report_rat / report_slack of every pin within
   the pin tolerance of tests/helpers.pin_err;
@@ -150,3 +151,65 @@ def test_change_spef_then_resizes(design):
     for gate, cell in steps[0]:
         t.repower_gate(gate, cell)
     check_against(t, read_ref(out2))
+
+
+def read_ref_paths(path):
+    paths = []
+    with open(path) as f:
+        for line in f:
+            t = line.split()
+            if t[0] == "T":
+                paths.append({"slack": float(t[2]), "el": int(t[3]), "points": []})
+            elif t[0] == "Q":
+                paths[int(t[1])]["points"].append((t[2], int(t[3]), float(t[4])))
+    return paths
+
+
+def check_paths(ours, ref, tol=1e-3):
+    """Same count; slacks pairwise within tol (ps) in ascending order; where
+    a path's slack is more than 2 tol from its neighbours' the path itself
+    (pins, transitions) is the reference's and its arrivals within tol."""
+    assert len(ours) == len(ref) and len(ref) > 0
+    s_ours = [p.slack for p in ours]
+    s_ref = [p["slack"] for p in ref]
+    assert s_ours == sorted(s_ours)
+    assert np.all(np.abs(np.array(s_ours) - np.array(s_ref)) <= tol), (s_ours[:5], s_ref[:5])
+    checked = 0
+    for i, r in enumerate(ref):
+        near = [abs(r["slack"] - ref[j]["slack"]) for j in (i - 1, i + 1) if 0 <= j < len(ref)]
+        if near and min(near) <= 2 * tol:
+            continue
+        o = ours[i]
+        assert [(p.pin, p.transition) for p in o.points] == [(n, t) for n, t, _ in r["points"]]
+        assert np.all(np.abs(np.array([p.at for p in o.points]) -
+                             np.array([a for _, _, a in r["points"]])) <= tol)
+        assert o.endpoint[1] == r["el"] and o.endpoint[0] == r["points"][-1][0]
+        checked += 1
+    return checked
+
+
+def test_report_timing_matches_the_reference(design):
+    """report_timing(K) against Timer::report_timing(K) on the same design,
+    after the first update and after a resize batch."""
+    from opentimer_b200.sizing import resize_trace, write_ops
+    from opentimer_b200.timer import Timer
+    d, keep = design
+    steps = resize_trace(keep, seed=13, steps=1, per_step=40)
+    ops = os.path.join(d, "ops_paths.txt")
+    write_ops(ops, steps)
+    t = Timer(d, keep)
+    for tag, extra in (("0", []), ("1", [f"repower={ops}"])):
+        if tag == "1":
+            for gate, cell in steps[0]:
+                t.repower_gate(gate, cell)
+        for K in (1, 40):
+            out = os.path.join(d, f"ref_paths_{tag}_{K}.txt")
+            p = subprocess.run([EXE_REF, d, "cpu", out, *extra, f"paths={K}"],
+                               capture_output=True, text=True, timeout=600)
+            assert p.returncode == 0, p.stderr[-2000:]
+            ref = read_ref_paths(out)
+            ours = t.report_timing(K)
+            n = check_paths(ours, ref)
+            assert n >= (1 if K == 1 else 10), (tag, K, n)
+            if K == 1:
+                assert len(ours[0].points) > 10
