@@ -9,6 +9,7 @@ device (ot/timer/timer.hpp:41-140, timer.cpp).
     t.report_wns(), t.report_tns(MAX)    # over the endpoints, as the Timer
     t.report_load("n42", MAX, FALL)      # the net's load (its RC root)
     t.rc_node("n42", "u7:A")             # load/delay/ldelay/impulse [2][2]
+    t.rc_slew("n42", "u7:A", MAX, RISE, 30.0)  # the node's slew for a root slew
     t.report_timing(10)                  # the 10 worst paths (paths.Path)
 
 Split and Tran are the reference's indices (MIN=0, MAX=1; RISE=0, FALL=1),
@@ -149,6 +150,17 @@ class Timer:
         slot = b + int(rc["node2bfs"][b + node])
         return {k: rc[k][slot].reshape(2, 2).copy() for k in ("load", "delay", "ldelay",
                                                                "impulse")}
+
+    def rc_slew(self, net, pin, el, rf, si):
+        """The slew at a pin's RC node for input slew si at the net's root
+        (RctNode::slew, ot/timer/net.cpp:30-32): sign(si) * sqrt(si^2 +
+        impulse), in float32; None if the pin has no node."""
+        v = self.rc_node(net, pin)
+        if v is None:
+            return None
+        si = np.float32(si)
+        r = np.sqrt(np.float32(si * si + v["impulse"][el][rf]), dtype=np.float32)
+        return float(-r if si < 0 else r)
 
     def _endpoint_slacks(self, el, rf):
         s = self._results()["slack"][self._d.endpoints, el * 2 + rf]

@@ -85,6 +85,10 @@ def check_against(t, ref):
                 continue
             g = np.stack([got[k].reshape(4) for k in ("load", "delay", "ldelay", "impulse")])
             assert np.all(np.abs(g - v) <= 1e-5 * np.abs(v) + 1e-6 * mx), (net, node)
+            if checked % 97 == 0:  # RctNode::slew from the node's impulse
+                for si in (-40.0, 25.0):
+                    want = np.copysign(np.sqrt(np.float32(si * si + v[3][3])), si)
+                    assert abs(t.rc_slew(net, node, 1, 1, si) - want) <= 1e-5 * abs(want) + 1e-4
             checked += 1
     assert checked > 1000
 
