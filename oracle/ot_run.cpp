@@ -22,8 +22,10 @@
 // seconds of every step go to stdout ("repower_step_s <k> <s>"); with
 // dump_every=<k> the pins (P lines) after every k-th step go to
 // <out>.step<k>.
-// paths=<K>: after the updates, Timer::report_timing(K), the K worst
-// paths, to the output (T and Q lines).
+// paths=<K>[,<split>[,<tran>]]: after the updates, Timer::report_timing(K)
+// (or its split / split-and-transition forms; split -1 with a transition
+// is the transition-only form), the K worst paths, to the output (T and Q
+// lines).
 // The same Timer sources are linked twice (oracle/Makefile): with the
 // reference's own CUDA module (ot_run_ref) and with libotg in its place
 // (ot_run_otg), so "cuda" runs either the reference kernels or ours behind
@@ -189,13 +191,21 @@ int main(int argc, char** argv) {
   std::vector<std::string> changes;
   std::string repower;
   int dump_every = 0;
-  int num_paths = 0;
+  int num_paths = 0, path_el = -1, path_rf = -1;
   for (int a = 4; a < argc; ++a) {
     const std::string s = argv[a];
     if (s.rfind("change=", 0) == 0) changes.push_back(s.substr(7));
     else if (s.rfind("repower=", 0) == 0) repower = s.substr(8);
     else if (s.rfind("dump_every=", 0) == 0) dump_every = std::atoi(s.c_str() + 11);
-    else if (s.rfind("paths=", 0) == 0) num_paths = std::atoi(s.c_str() + 6);
+    else if (s.rfind("paths=", 0) == 0) {
+      num_paths = std::atoi(s.c_str() + 6);
+      const size_t c1 = s.find(',');
+      if (c1 != std::string::npos) {
+        path_el = std::atoi(s.c_str() + c1 + 1);
+        const size_t c2 = s.find(',', c1 + 1);
+        if (c2 != std::string::npos) path_rf = std::atoi(s.c_str() + c2 + 1);
+      }
+    }
     else graph_path = argv[a];
   }
   ot::Timer timer;
@@ -364,7 +374,14 @@ int main(int argc, char** argv) {
     }
   }
   if (num_paths > 0) {
-    const std::vector<ot::Path> paths = timer.report_timing((size_t)num_paths);
+    const size_t K = (size_t)num_paths;
+    const ot::Split el = path_el == 1 ? ot::MAX : ot::MIN;
+    const ot::Tran rf = path_rf == 1 ? ot::FALL : ot::RISE;
+    const std::vector<ot::Path> paths =
+        path_el >= 0 && path_rf >= 0 ? timer.report_timing(K, el, rf)
+        : path_el >= 0              ? timer.report_timing(K, el)
+        : path_rf >= 0              ? timer.report_timing(K, rf)
+                                    : timer.report_timing(K);
     for (size_t k = 0; k < paths.size(); ++k) {
       const ot::Path& p = paths[k];
       std::fprintf(f, "T %zu %.9g %d %zu\n", k, p.slack, (int)p.endpoint->_el, p.size());

@@ -50,6 +50,7 @@ def parse(out, graph):
 
 def run_ref(d, K, extra=()):
     out, graph = os.path.join(d, f"ref_paths{K}.txt"), os.path.join(d, f"graph{K}.txt")
+    # a paths= argument in `extra` overrides this one (the harness keeps the last)
     p = subprocess.run([EXE_REF, d, "cpu", out, graph, f"paths={K}", *extra],
                        capture_output=True, text=True, timeout=600)
     assert p.returncode == 0, p.stderr[-2000:]
@@ -102,6 +103,23 @@ def test_paths_equal_reference_on_its_values(design, K):
         # the worst endpoint's path, reported with the endpoint's slack
         assert float(ours[0].slack) == float(ref[0]["slack"])
     same_paths(ours, ref)
+
+
+@pytest.mark.parametrize("el,rf", [(1, None), (0, None), (None, 1), (1, 0)])
+def test_split_and_transition_forms(design, el, rf):
+    """report_timing(K, el), (K, rf) and (K, el, rf) against the
+    reference's forms of the same name."""
+    d, _ = design
+    K = 8
+    arg = f"paths={K},{-1 if el is None else el}" + ("" if rf is None else f",{rf}")
+    pins, ref, *rest = run_ref(d, K, extra=(arg,))
+    g = path_graph(pins, *rest)
+    ours = g.report_timing(K, el, rf)
+    assert len(ref) > 0
+    same_paths(ours, ref)
+    for p in ours:
+        assert el is None or p.endpoint[1] == el
+        assert rf is None or p.endpoint[2] == rf
 
 
 def test_worst_endpoints_follow_slack_order(design):
