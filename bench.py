@@ -372,11 +372,16 @@ def run_ours(args, world, rank, local):
 
     # ---- end to end through the host C ABI (pinned host buffers)
     e2e = None
+    SECTION_WALL_S["headline"] = round(time.perf_counter() - T_START, 2)
+    t0 = time.perf_counter()
     if not args.no_e2e:
         e2e = run_e2e(args, world, g, ns_np, N, V, S, dev, batch)
+    SECTION_WALL_S["run_e2e"] = round(time.perf_counter() - t0, 2)
 
     # ---- levelization (5M pins, 12M edges, 200 levels)
+    t0 = time.perf_counter()
     lv = run_levelize(args, world, dev) if not args.no_levelize else None
+    SECTION_WALL_S["run_levelize"] = round(time.perf_counter() - t0, 2)
 
     line = {
         "metric": METRIC, "value": value, "unit": "nodes/s", "n_gpus": world,
@@ -433,6 +438,7 @@ def run_ours(args, world, rank, local):
         line["full_update"] = _section(run_full_update, baseline=base if rank == 0 else None)
     if world == 1 and not args.no_huge:
         line["huge_nets"] = _section(run_huge)
+    line["section_wall_s"] = dict(SECTION_WALL_S, total=round(time.perf_counter() - T_START, 1))
     return line
 
 
@@ -540,16 +546,23 @@ def check_headline_outputs(batch, ns_np, seed):
     return out
 
 
+SECTION_WALL_S = {}  # host wall seconds of every section, for the line
+
+
 def _section(fn, *args, **kw):
     """Runs a section after the headline measurement: a failure is reported
     in the line ({"error": ...}, traceback on stderr) instead of losing the
-    headline numbers."""
+    headline numbers.  Its wall time goes to SECTION_WALL_S."""
+    t0 = time.perf_counter()
     try:
         return fn(*args, **kw)
     except Exception as e:  # noqa: BLE001 -- reported, not swallowed
         import traceback
         traceback.print_exc()
         return {"error": f"{type(e).__name__}: {e}"}
+    finally:
+        name = fn.__name__
+        SECTION_WALL_S[name] = round(SECTION_WALL_S.get(name, 0.0) + time.perf_counter() - t0, 2)
 
 
 def run_e2e(args, world, g, ns_np, N, V, S, dev, batch):
@@ -1321,6 +1334,9 @@ def cpu_baseline(g, ns_np):
     dt, kind, cores = time_reference_cpu(f, threads)
     return {"value": f.total_nodes / dt, "unit": "nodes/s", "cores": cores, "kind": kind,
             "sample": f"first {k} of {NUM_NETS} nets ({f.total_nodes} nodes), one pass"}
+
+
+T_START = time.perf_counter()
 
 
 def main():
