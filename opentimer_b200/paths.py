@@ -204,16 +204,23 @@ class PathGraph:
         return Point(self.names[s >> 1], s & 1, self.at[s >> 1, 2 * sf.el + (s & 1)])
 
     def _recover_node(self, sf, node, v, pts):
-        if node is None:
-            return
-        self._recover_node(sf, node.parent, node.frm, pts)
-        u = node.to
-        if node.frm == SUPER:
-            pts.append(self._source_point(sf, u))
-        else:
-            d = self.delay[node.arc, sf.el, pts[-1].transition, u & 1]
-            pts.append(Point(self.names[u >> 1], u & 1, F32(pts[-1].at + d)))
-        self._recover(sf, u, v, pts)
+        """The path of prefix-tree node `node` up to v: its ancestors'
+        segments from the source on, each up to where the next deviates
+        (iterative: a chain of deviations can be K long)."""
+        chain = []
+        while node is not None:
+            chain.append(node)
+            node = node.parent
+        for k in range(len(chain) - 1, -1, -1):
+            nd = chain[k]
+            end = chain[k - 1].frm if k > 0 else v
+            u = nd.to
+            if nd.frm == SUPER:
+                pts.append(self._source_point(sf, u))
+            else:
+                d = self.delay[nd.arc, sf.el, pts[-1].transition, u & 1]
+                pts.append(Point(self.names[u >> 1], u & 1, F32(pts[-1].at + d)))
+            self._recover(sf, u, end, pts)
 
     def _spur(self, sf, pf, pfx, seq):
         u = pfx.to

@@ -92,7 +92,7 @@ def design(tmp_path_factory):
     return d, keep
 
 
-@pytest.mark.parametrize("K", [1, 5, 60])
+@pytest.mark.parametrize("K", [1, 5, 60, 400])
 def test_paths_equal_reference_on_its_values(design, K):
     d, _ = design
     pins, ref, *rest = run_ref(d, K)
