@@ -447,6 +447,43 @@ otg_status otg_prop_status(const void* workspace, otg_stream_t stream);
  * reports (Timer::report_timing, ot/timer/path.cpp:365-420) walk these. */
 otg_status otg_prop_arc_delays(const void* workspace, size_t workspace_bytes, int32_t num_arcs,
                                const float** arc_delay);
+
+/* ---- path reports (host) -------------------------------------------------
+ * A propagated timing graph for the path search, all HOST arrays: the arcs
+ * (constraint arcs flagged: they carry no delay), the data-path sources
+ * (Pin::is_datapath_source: no fanin, a cell's clock pin, a primary
+ * input), the endpoints (primary outputs and the tests' constrained pins),
+ * every arc's delay [num_arcs][8] by (split << 2 | from tran << 1 | to
+ * tran), NaN where empty (otg_prop_arc_delays, copied to the host), and
+ * at / rat / slack [num_pins][4] (corner = split * 2 + tran). */
+typedef struct otg_path_graph {
+  int32_t num_pins, num_arcs, num_endpoints;
+  const int32_t* arc_from;
+  const int32_t* arc_to;
+  const uint8_t* arc_is_test;
+  const uint8_t* pin_is_source;
+  const int32_t* endpoints;
+  const float* arc_delay;
+  const float* at;
+  const float* rat;
+  const float* slack;
+} otg_path_graph;
+
+/* Timer::report_timing(K[, split][, tran]) (ot/timer/path.cpp:365-537):
+ * the K worst data paths, ascending by slack.  split / tran: -1 for any.
+ * K = 1 gives the worst endpoint's path with the endpoint's slack; larger
+ * K the paths of negative slack only (the reference's prefix-tree
+ * search).  Writes num_paths (<= K), path_slack [K], path_endpoint [K][3]
+ * (pin, split, tran), path_start [K + 1] (offsets into the points) and,
+ * up to max_points, point_pin / point_tran / point_at; points_needed gets
+ * the total, and a result that does not fit returns OTG_ERR_WORKSPACE
+ * (call again with a larger max_points).  float32 arithmetic in the
+ * reference's order: on the reference's own graph values the paths are
+ * the reference's, bit for bit. */
+otg_status otg_report_paths(const otg_path_graph* graph, int32_t K, int32_t split, int32_t tran,
+                            int32_t* num_paths, float* path_slack, int32_t* path_endpoint,
+                            int32_t* path_start, int32_t max_points, int32_t* point_pin,
+                            int32_t* point_tran, float* point_at, int32_t* points_needed);
 /* The same over a graph that is the union of independent designs (no arc
  * between two of them): pin_group [P] gives each pin its design, and only
  * the pins whose group_active[design] is nonzero are propagated (and

@@ -33,7 +33,7 @@ C_SYMBOLS = [
     "otg_prop_status", "otg_rc_move_nets", "otg_spef_names", "otg_apply_updates",
     "otg_worst_slack", "otg_spef_write", "otg_fanin_csr_workspace_size", "otg_fanin_csr",
     "otg_fanin_csr_status", "otg_propagate_groups", "otg_worst_slack_groups",
-    "otg_propagate_items", "otg_prop_arc_delays",
+    "otg_propagate_items", "otg_prop_arc_delays", "otg_report_paths",
 ]
 # The reference-compatible C++ entry points (include/otg_compat.hpp), by
 # their Itanium-mangled names.
@@ -61,6 +61,16 @@ class RcForest(ctypes.Structure):
         ("sinks_start", ctypes.c_void_p), ("sink_nodes", ctypes.c_void_p),
         ("driver_slew", ctypes.c_void_p), ("sink_slew", ctypes.c_void_p),
     ]
+
+
+class PathGraph(ctypes.Structure):
+    """otg_path_graph: a propagated timing graph for otg_report_paths."""
+    _fields_ = [("num_pins", ctypes.c_int32), ("num_arcs", ctypes.c_int32),
+                ("num_endpoints", ctypes.c_int32), ("arc_from", ctypes.c_void_p),
+                ("arc_to", ctypes.c_void_p), ("arc_is_test", ctypes.c_void_p),
+                ("pin_is_source", ctypes.c_void_p), ("endpoints", ctypes.c_void_p),
+                ("arc_delay", ctypes.c_void_p), ("at", ctypes.c_void_p), ("rat", ctypes.c_void_p),
+                ("slack", ctypes.c_void_p)]
 
 
 class RcTuning(ctypes.Structure):
@@ -149,6 +159,8 @@ def lib():
         L.otg_propagate_groups.argtypes = [P, P, P, P, P, P, P, P, P, P, P, S, P]
         L.otg_propagate_items.argtypes = [P, P, P, I32, P, P, P, P, P, S, P]
         L.otg_prop_arc_delays.argtypes = [P, S, I32, ctypes.POINTER(P)]
+        L.otg_report_paths.argtypes = [ctypes.POINTER(PathGraph), I32, I32, I32, P, P, P, P, I32,
+                                       P, P, P, P]
         L.otg_worst_slack_groups.argtypes = [P, I32, P, P, I32, P, P, P]
         L.otg_spef_names.argtypes = [P, P, PS]
         L.otg_spef_free.restype = None
@@ -165,7 +177,8 @@ def lib():
                      "otg_rc_move_nets", "otg_spef_names", "otg_apply_updates",
                      "otg_worst_slack", "otg_spef_write", "otg_fanin_csr_workspace_size",
                      "otg_fanin_csr", "otg_fanin_csr_status", "otg_propagate_groups",
-                     "otg_worst_slack_groups", "otg_propagate_items", "otg_prop_arc_delays"]:
+                     "otg_worst_slack_groups", "otg_propagate_items", "otg_prop_arc_delays",
+                     "otg_report_paths"]:
             getattr(L, name).restype = ctypes.c_int
         _lib = L
     return _lib

@@ -15,7 +15,7 @@ BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libotg.so")
 SOURCES = ["otg_rc.cu", "otg_levelize.cu", "otg_synth.cu", "otg_host.cu", "otg_noalloc.cu",
            "otg_serve.cu", "otg_spef.cpp", "otg_prop.cu", "otg_move.cu", "otg_sizing.cu", "otg_spef_write.cpp",
-           "otg_csr.cu"]
+           "otg_csr.cu", "otg_paths.cpp"]
 CXX = os.environ.get("CXX", "g++")
 CXXFLAGS = ["-O3", "-std=c++17", "-fPIC", "-pthread", "-Wall"]
 
