@@ -132,3 +132,50 @@ def test_worst_endpoints_follow_slack_order(design):
     # per split / transition the lists are restricted to that corner
     assert all(el == 1 for _, el, _ in g.worst_endpoints(10, el=1))
     assert all((el, rf) == (0, 1) for _, el, rf in g.worst_endpoints(10, el=0, rf=1))
+
+
+def test_native_search_on_a_hand_built_graph():
+    """0 (a primary input, a source) -> 1 -> 2 (an endpoint): a net arc
+    (rise->rise 1, fall->fall 2) then a negative-unate cell arc (rise->fall
+    3, fall->rise 4), late split only.  The worst late path ends at 2 rising:
+    from 0 falling, 5 + 2 + 4 = 11 against a required time of 10."""
+    import ctypes
+    from opentimer_b200 import _lib
+    nan = np.nan
+    delay = np.full((2, 2, 2, 2), nan, np.float32)  # [arc][el][frf][trf]
+    delay[0, 1, 0, 0], delay[0, 1, 1, 1] = 1.0, 2.0
+    delay[1, 1, 0, 1], delay[1, 1, 1, 0] = 3.0, 4.0
+    at = np.full((3, 4), nan, np.float32)
+    at[0, 2:] = [4.0, 5.0]
+    at[1, 2:] = [5.0, 7.0]
+    at[2, 2:] = [11.0, 8.0]
+    rat = np.full((3, 4), nan, np.float32)
+    rat[2, 2:] = 10.0
+    slack = np.full((3, 4), nan, np.float32)
+    slack[2, 2:] = rat[2, 2:] - at[2, 2:]
+    g = PathGraph(["i", "u:A", "u:ZN"], [0, 1], [1, 2], [], [True, False, False], [2])
+    g.values(delay, at, rat, slack)
+    (p,) = g.report_timing(1)
+    assert p.slack == -1.0 and p.endpoint == ("u:ZN", 1, 0)
+    assert [(q.pin, q.transition, float(q.at)) for q in p.points] == \
+        [("i", 1, 5.0), ("u:A", 1, 7.0), ("u:ZN", 0, 11.0)]
+    # K > 1: only the negative-slack path (the other ends at 8 <= 10)
+    assert [x.slack for x in g.report_timing(5)] == [-1.0]
+    assert g.report_timing(0) == [] and g.report_timing(3, el=0) == []
+    # the C ABI: a result larger than max_points, then bad arguments
+    L = _lib.lib()
+    ptr = lambda a: a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
+    cg = _lib.PathGraph(3, 2, 1, ptr(g._from32), ptr(g._to32), ptr(g._test8), ptr(g._src8),
+                        ptr(g._ends32), ptr(g._delay8), ptr(g.at), ptr(g.rat), ptr(g.slack))
+    n, need = ctypes.c_int32(), ctypes.c_int32()
+    sl, ep, st = np.zeros(1, np.float32), np.zeros(3, np.int32), np.zeros(2, np.int32)
+    pin, tr, pa = np.zeros(1, np.int32), np.zeros(1, np.int32), np.zeros(1, np.float32)
+    code = L.otg_report_paths(ctypes.byref(cg), 1, -1, -1, ctypes.byref(n), ptr(sl), ptr(ep),
+                              ptr(st), 1, ptr(pin), ptr(tr), ptr(pa), ctypes.byref(need))
+    assert code == 8 and need.value == 3 and n.value == 1  # OTG_ERR_WORKSPACE
+    assert L.otg_report_paths(ctypes.byref(cg), 1, 2, -1, ctypes.byref(n), ptr(sl), ptr(ep),
+                              ptr(st), 1, ptr(pin), ptr(tr), ptr(pa), ctypes.byref(need)) == 1
+    bad = np.array([0, 7], np.int32)  # an arc to a pin that does not exist
+    cg.arc_to = ptr(bad)
+    assert L.otg_report_paths(ctypes.byref(cg), 1, -1, -1, ctypes.byref(n), ptr(sl), ptr(ep),
+                              ptr(st), 1, ptr(pin), ptr(tr), ptr(pa), ctypes.byref(need)) == 1
